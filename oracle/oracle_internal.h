@@ -1,0 +1,79 @@
+// Shared helpers of the CPU oracle (test infrastructure only).
+#ifndef GSPLAT_ORACLE_INTERNAL_H
+#define GSPLAT_ORACLE_INTERNAL_H
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+
+#include "gsplat_oracle.h"
+
+namespace orc {
+
+void quat_normalize(const float q[4], float out[4]);
+void quat_inverse(const float q[4], float out[4]);
+void quat_to_mat3(const float q[4], float m[9]);
+void frame_params(const OrcCamera &cam, uint32_t width, uint32_t height, uint32_t tile,
+                  uint32_t sh_degree, OrcFrameParams &p);
+void radix_sort_desc_u64_passes(uint64_t *values, uint64_t *scratch, uint64_t n, uint32_t lo,
+                                uint32_t hi);
+
+// f32::clamp / WGSL clamp for finite inputs.
+inline float clamp_f(float x, float lo, float hi) { return std::fmin(std::fmax(x, lo), hi); }
+
+inline float bits_to_float(uint32_t b) {
+  float f;
+  std::memcpy(&f, &b, 4);
+  return f;
+}
+inline uint32_t float_to_bits(float f) {
+  uint32_t b;
+  std::memcpy(&b, &f, 4);
+  return b;
+}
+
+// e^x for x in [-4.5, 0]: Cody-Waite reduction to base 2 (t = x*log2(e),
+// n = rint(t), f = t - n in [-0.5, 0.5]) and the degree-6 Taylor polynomial of
+// 2^f = e^(f ln 2), coefficients ln(2)^k / k!. Relative error about 2e-7.
+// The CUDA raster uses the same operation sequence, so CPU and GPU agree bit
+// for bit.
+inline float exp_neg(float x) {
+  float t = x * 1.44269504088896341f;
+  float n = std::nearbyint(t);
+  float f = t - n;
+  float p = std::fma(1.54035304e-4f, f, 1.33335581e-3f);
+  p = std::fma(p, f, 9.61812911e-3f);
+  p = std::fma(p, f, 5.55041087e-2f);
+  p = std::fma(p, f, 2.40226507e-1f);
+  p = std::fma(p, f, 6.93147181e-1f);
+  p = std::fma(p, f, 1.0f);
+  int32_t e = (int32_t)n;
+  return bits_to_float(float_to_bits(p) + (uint32_t)(e * (1 << 23)));
+}
+
+// Round-to-nearest-even UNORM8 conversion of a value clamped to [0, 1].
+inline uint8_t to_unorm8(float x) {
+  float c = std::fmin(std::fmax(x, 0.0f), 1.0f);
+  return (uint8_t)std::nearbyint(c * 255.0f);
+}
+
+// Per-pixel coverage and weight of one splat at integer pixel (px, py):
+// fs_main (splat_surface_direct.wgsl:356-369) on the local quad coordinate,
+// with the quad clip |lx|,|ly| <= s from vs_main (wgsl:336-354). Returns false
+// when the fragment is discarded.
+inline bool pixel_weight(const OrcRecord &r, int px, int py, float &g, float &w) {
+  float dpx = (float)px - r.cx;
+  float dpy = (float)py - r.cy;
+  float lx = std::fma(r.ax, dpx, r.ay * dpy);
+  float ly = std::fma(r.bx, dpx, r.by * dpy);
+  if (!(std::fabs(lx) <= r.s && std::fabs(ly) <= r.s)) return false;
+  float r2 = std::fma(lx, lx, ly * ly);
+  if (!(r2 <= 1.0f)) return false;
+  g = exp_neg(-4.5f * r2);
+  w = r.alpha * g;
+  return w > (1.0f / 256.0f);
+}
+
+}  // namespace orc
+
+#endif
