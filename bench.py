@@ -1,0 +1,310 @@
+"""Benchmark of the B200 SortedAlpha renderer: 1080p frames/s of the plain
+one-frame path on the 279,199-splat SH-degree-3 synthetic scene.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+
+Under torchrun each rank renders its own replica of the workload on its GPU
+(the per-frame path does not shard; no collective is used) and the reported
+value is the whole-job frames/s from the max-over-ranks device time.
+
+value: frames/s with the scene resident in HBM, device time of K frames
+  measured with CUDA events on the renderer's stream; L2 is flushed (a
+  256 MiB write) between frames, outside the timed spans.
+e2e: the same frames through the public C ABI from host memory: camera upload,
+  gsplat_context_render_frame and an RGBA8 readback into pinned host memory
+  every step, host wall clock.
+--impl reference: the reference's SortedAlpha frame restated on the host CPU
+  (depth preprocess and 8-bit LSD radix sort on one thread, vertex stage and
+  UNORM8 blending on every host thread), on the same workload.
+"""
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gsplat-rs_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import numpy as np  # noqa: E402
+
+import gsplat_scenes  # noqa: E402
+
+METRIC = "1080p frames/s @279k SH3"
+WORKLOAD = "plain SortedAlpha frame: 279,199 synthetic splats, SH degree 3, 1920x1080, 16x16 tiles"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.out.flush()
+        with open(self.out.name) as f:
+            rows = [r.split(",") for r in f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.out.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(phase, counts, n, planes, width, height, tile_passes):
+    """Bytes each phase must move at minimum (reads + writes), per frame."""
+    v, d, k = counts.visible, counts.drawn, counts.tile_keys
+    if phase == "preprocess":
+        return n * 16 + v * 32 + d * 16 * planes + v * 16 + d * 48
+    if phase == "depth_sort":
+        return v * 4 + 3 * v * 16  # histogram read + three non-trivial passes
+    if phase == "emit":
+        return v * 4 + v * 8 + k * 8
+    if phase == "tile_sort":
+        return k * 4 + tile_passes * k * 16
+    if phase == "ranges":
+        return k * 4
+    if phase == "raster":
+        return k * 52 + width * height * 4
+    return 0
+
+
+def cpu_baseline(scene, cam, w, h, budget_s=15.0, steps=None):
+    import oracle_py
+
+    threads = os.cpu_count() or 1
+    sv = oracle_py.SceneView(scene)
+    oracle_py.render_reference_frame(sv, cam, w, h, threads)  # warm caches
+    t0 = time.perf_counter()
+    frames = 0
+    phases = []
+    while True:
+        _, t = oracle_py.render_reference_frame(sv, cam, w, h, threads)
+        phases.append((t.preprocess_ms, t.sort_ms, t.project_ms, t.raster_ms))
+        frames += 1
+        el = time.perf_counter() - t0
+        if (steps is not None and frames >= steps) or (steps is None and el >= budget_s):
+            break
+    el = time.perf_counter() - t0
+    ph = np.mean(np.array(phases), axis=0)
+    return {"value": frames / el, "unit": "frames/s", "cores": threads, "kind": "port",
+            "sample": f"{frames} full frames of the workload; depth preprocess and radix sort on "
+                      f"1 thread, vertex stage and UNORM8 blend on {threads} threads "
+                      f"(mean ms: preprocess {ph[0]:.1f}, sort {ph[1]:.1f}, vertex {ph[2]:.1f}, "
+                      f"raster {ph[3]:.1f})"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    scene, cam, w, h = gsplat_scenes.config2()
+    import oracle_py
+
+    sv = oracle_py.SceneView(scene)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        oracle_py.render_reference_frame(sv, cam, w, h, threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle_py.render_reference_frame(sv, cam, w, h, threads)
+    el = time.perf_counter() - t0
+    value = args.steps / el
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "frames/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": "frames/s", "cores": threads, "kind": "port",
+                             "sample": "one full frame per step: the reference SortedAlpha path "
+                                       "restated in C++ (oracle/), host CPU"},
+            "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_cuda(args, world, rank, local):
+    import torch
+
+    import gsplat_ffi as ffi
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    scene, cam, w, h = gsplat_scenes.config2()
+    ctx = ffi.Context(w, h)
+    ctx.load_scene(scene)
+    ctx.set_camera(cam)
+    for _ in range(max(args.warmup, 3)):
+        ctx.render_frame()
+    counts = ctx.frame_counts()
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
+
+    # Per-phase device times (separate untimed loop, L2 flushed before each frame).
+    phase_acc = {}
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(i)
+        ctx.render_frame()
+        for k, v in ctx.phase_times().items():
+            phase_acc[k] = phase_acc.get(k, 0.0) + v
+    phases = {k: v / args.steps for k, v in phase_acc.items()}
+
+    clocks = ClockSampler(local)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(i + 1)
+            starts[i].record(stream)
+        ctx.render_frame_async()
+        with torch.cuda.stream(stream):
+            ends[i].record(stream)
+    ctx.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    device_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    if world > 1:
+        t = torch.tensor([device_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        device_ms = float(t.item())
+        torch.distributed.barrier()
+    ms_per_frame = device_ms / args.steps
+    value = world * args.steps / (device_ms / 1000.0)
+
+    # End to end through the C ABI: camera in, frame, RGBA8 readback to pinned memory.
+    pinned = torch.empty(w * h * 4, dtype=torch.uint8, pin_memory=True)
+    out = pinned.numpy()
+    cams = []
+    rng = np.random.default_rng(5)
+    for i in range(args.steps):
+        yaw = 0.7 + 0.002 * i
+        cams.append(ffi.GsplatCamera.from_dict(gsplat_scenes.camera(
+            (4.0 * math.sin(yaw), 0.5, -4.0 * math.cos(yaw)), (0, 0, 0), 45.0)))
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        ctx.set_camera(cams[i])
+        ctx.render_frame()
+        ctx.readback_rgba8(out)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * args.steps / e2e_s, "unit": "frames/s",
+           "h2d_bytes_per_step": 40, "d2h_bytes_per_step": w * h * 4 + 64}
+
+    tiles = ((w + 15) // 16) * ((h + 15) // 16)
+    tile_passes = 2 if tiles > 256 else 1
+    planes = 12
+    dominant = max(phases, key=phases.get)
+    peaks = {}
+    if os.path.exists(PEAKS_FILE):
+        with open(PEAKS_FILE) as f:
+            peaks = json.load(f)
+    hbm = peaks.get("hbm_gbs")
+    bytes_dom = algorithmic_bytes(dominant, counts, scene["positions"].shape[0], planes, w, h,
+                                  tile_passes)
+    achieved = bytes_dom / (phases[dominant] * 1e-3) / 1e9
+    peak = hbm if hbm else FALLBACK_HBM_GBS
+    roofline = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": "measured" if hbm else "fallback",
+                "algorithmic_bytes": bytes_dom}
+    phase_rooflines = {}
+    for k, ms in phases.items():
+        b = algorithmic_bytes(k, counts, scene["positions"].shape[0], planes, w, h, tile_passes)
+        phase_rooflines[k] = {"ms": ms, "bytes": b, "gbs": b / (ms * 1e-3) / 1e9 if ms > 0 else None}
+
+    launches_per_frame = 1 + (2 + 4) + 1 + (2 + tile_passes) + 1 + 1
+    line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_frame,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "l2": "flushed between frames (256 MiB write)",
+                       "parallelism": f"replicas x{world}", "visible": int(counts.visible),
+                       "tile_pairs": int(counts.tile_keys)},
+            "e2e": e2e, "gpu_launches": launches_per_frame * args.steps, "clocks": clk,
+            "roofline": roofline, "phases": phase_rooflines}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(scene, cam, w, h, budget_s=args.cpu_budget)
+    ctx.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_cuda(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,112 @@
+// Device-side structures and helpers shared by the kernels of the renderer.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device_types.h"
+#include "gsr_host.h"
+
+namespace gsr {
+// Bound on look-back spins: predecessors always run ahead (tiles are taken
+// from an atomic ticket in launch order), so this only guards against a
+// fault; on expiry the kernel records kErrLookbackTimeout and moves on.
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u32(uint32_t *p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Single-value decoupled look-back (one warp). Status words hold a 2-bit
+// flag (1 = aggregate, 2 = inclusive prefix) in the top bits and the value in
+// the low 62 bits. Returns the exclusive prefix of `block`.
+constexpr unsigned long long kFlagAgg = 1ull << 62;
+constexpr unsigned long long kFlagInc = 2ull << 62;
+constexpr unsigned long long kValueMask = (1ull << 62) - 1;
+
+__device__ __forceinline__ unsigned long long lookback_warp(unsigned long long *status,
+                                                            uint32_t block,
+                                                            unsigned long long aggregate,
+                                                            uint32_t *error) {
+  const uint32_t lane = threadIdx.x & 31;
+  if (block == 0) {
+    if (lane == 0) st_relaxed_u64(&status[0], kFlagInc | aggregate);
+    return 0;
+  }
+  if (lane == 0) st_relaxed_u64(&status[block], kFlagAgg | aggregate);
+  unsigned long long exclusive = 0;
+  int64_t base = (int64_t)block - 1;
+  uint32_t spins = 0;
+  while (true) {
+    int64_t idx = base - (int64_t)lane;
+    unsigned long long s = idx >= 0 ? ld_relaxed_u64(&status[idx]) : kFlagInc;
+    if (__any_sync(0xffffffffu, (s >> 62) == 0)) {
+      if (++spins > kSpinLimit) {
+        if (lane == 0) atomicOr(error, kErrLookbackTimeout);
+        break;
+      }
+      __nanosleep(32);
+      continue;
+    }
+    uint32_t inc = __ballot_sync(0xffffffffu, (s >> 62) == 2);
+    if (inc) {
+      uint32_t first = __ffs(inc) - 1;
+      exclusive += warp_sum<unsigned long long>(lane <= first ? (s & kValueMask) : 0ull);
+      break;
+    }
+    exclusive += warp_sum<unsigned long long>(s & kValueMask);
+    base -= 32;
+  }
+  if (lane == 0) st_relaxed_u64(&status[block], kFlagInc | (exclusive + aggregate));
+  return exclusive;
+}
+
+// e^x for x in [-4.5, 0]: Cody-Waite reduction to base 2 and the degree-6
+// Taylor polynomial of 2^f (coefficients ln(2)^k / k!), explicit fmaf, so the
+// result is reproducible bit for bit by a C++ restatement. Relative error
+// about 2e-7.
+__device__ __forceinline__ float exp_neg(float x) {
+  float t = x * 1.44269504088896341f;
+  float n = rintf(t);
+  float f = t - n;
+  float p = fmaf(1.54035304e-4f, f, 1.33335581e-3f);
+  p = fmaf(p, f, 9.61812911e-3f);
+  p = fmaf(p, f, 5.55041087e-2f);
+  p = fmaf(p, f, 2.40226507e-1f);
+  p = fmaf(p, f, 6.93147181e-1f);
+  p = fmaf(p, f, 1.0f);
+  int e = __float2int_rn(n);
+  return __int_as_float(__float_as_int(p) + e * (1 << 23));
+}
+
+__device__ __forceinline__ uint32_t to_unorm8(float x) {
+  return __float2uint_rn(fminf(fmaxf(x, 0.0f), 1.0f) * 255.0f);
+}
+
+}  // namespace gsr

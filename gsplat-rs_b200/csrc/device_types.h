@@ -1,0 +1,78 @@
+// Plain data structures shared by the kernels and the host orchestration.
+#pragma once
+
+#include <cstdint>
+#include <vector_types.h>
+
+namespace gsr {
+
+// Scene resident in HBM, structure of arrays of float4 planes (16-byte
+// aligned, one 128-bit load per plane and splat):
+//   pos_alpha[i] = (x, y, z, alpha)         alpha = clamp(sigmoid(opacity))
+//   cov_a[i]     = (xx, xy, xz, yy)         world covariance
+//   cov_b[i]     = (yz, zz, extent_scale, 0)
+//   color[p*n+i] = floats 4p..4p+3 of (DC rgb, rest coefficient 1 rgb, ...)
+struct SceneDev {
+  const float4 *pos_alpha;
+  const float4 *cov_a;
+  const float4 *cov_b;
+  const float4 *color;
+  uint32_t n;
+  uint32_t planes;
+};
+
+// Pixel-space raster record of a drawn splat (48 bytes):
+//   a = (cx, cy, ax, ay)  centre in pixel-centre coordinates, first row of
+//                         the inverse axis matrix (local x = ax*dx + ay*dy)
+//   b = (bx, by, s, alpha) second row, quad extent scale, opacity
+//   c = (r*alpha, g*alpha, b*alpha, 0) premultiplied colour
+struct Record {
+  float4 a, b, c;
+};
+
+// Same layout as GsplatProjectedSplat.
+struct ProjectedDev {
+  float center_ndc[2];
+  float axis_u[2];
+  float axis_v[2];
+  float color[4];
+  float extent_scale;
+  float depth;
+  uint32_t flags;
+  uint16_t tile_x0, tile_y0, tile_x1, tile_y1;
+  uint32_t reserved;
+};
+static_assert(sizeof(ProjectedDev) == 64, "projected splat layout");
+
+// Error bits reported through FrameCounters::error.
+enum : uint32_t {
+  kErrLookbackTimeout = 1u,  // a decoupled look-back wait hit its iteration limit
+  kErrSortTooLarge = 2u,
+};
+
+// Per-frame device counters; zeroed before each frame.
+struct FrameCounters {
+  uint32_t k1_ticket;
+  uint32_t emit_ticket;
+  uint32_t visible;
+  uint32_t drawn;
+  uint32_t error;
+  uint32_t overflow;
+  uint32_t pairs;  // pairs written: min(keys, capacity)
+  uint32_t pad0;
+  unsigned long long keys;  // pairs emitted (may exceed the capacity)
+  uint32_t sort_tickets[16];
+};
+
+// Plan of one radix sort, computed on the device from the global histogram.
+struct SortPlan {
+  uint32_t n;
+  uint32_t passes;
+  uint32_t final_buffer;  // 0: the input buffers, 1: the alternate buffers
+  uint32_t pad;
+  uint32_t skip[8];
+  uint32_t src[8];
+  uint32_t digit_offset[8][256];
+};
+
+}  // namespace gsr

@@ -1,0 +1,346 @@
+// K1: per-splat preprocess. Built with --fmad=false: every f32 expression
+// rounds after each operation, as the reference's f32 code does, so depth
+// keys, projected records and tile rects match the CPU restatement bit for
+// bit (division and sqrt are IEEE-rounded; there are no transcendental calls
+// per frame — alpha, extent scale and covariance are precomputed at load).
+//
+// One thread per splat:
+//   1. depth = row2 . (p - cam); visible iff near <= depth <= far
+//      (preprocess_visible_into, crates/gsplat-render-wgpu/src/lib.rs:1263-1296);
+//   2. visible splats are compacted in id order with a block scan and a
+//      decoupled look-back, emitting (~bits(max(depth, 0)), id) so that an
+//      ascending stable sort yields the reference's descending-depth order;
+//   3. project_splat + eval_color (splat_surface_direct.wgsl:131-217, 233-334);
+//   4. tile rect of the ellipse |local| <= s and the pixel-space record.
+
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace gsr {
+
+namespace {
+
+__device__ __forceinline__ float clampf(float x, float lo, float hi) {
+  return fminf(fmaxf(x, lo), hi);
+}
+
+struct Cov6 {
+  float xx, xy, xz, yy, yz, zz;
+};
+
+// splat_surface_direct.wgsl:96-103
+__device__ __forceinline__ float cov_quadratic(const Cov6 &c, float r0, float r1, float r2) {
+  return r0 * r0 * c.xx + 2.0f * r0 * r1 * c.xy + 2.0f * r0 * r2 * c.xz + r1 * r1 * c.yy +
+         2.0f * r1 * r2 * c.yz + r2 * r2 * c.zz;
+}
+
+// splat_surface_direct.wgsl:105-110
+__device__ __forceinline__ float cov_bilinear(const Cov6 &c, const float *a, const float *b) {
+  float bx = c.xx * b[0] + c.xy * b[1] + c.xz * b[2];
+  float by = c.xy * b[0] + c.yy * b[1] + c.yz * b[2];
+  float bz = c.xz * b[0] + c.yz * b[1] + c.zz * b[2];
+  return a[0] * bx + a[1] * by + a[2] * bz;
+}
+
+__device__ __forceinline__ float plane_float(const float4 *planes, int k) {
+  const float4 v = planes[k >> 2];
+  switch (k & 3) {
+    case 0: return v.x;
+    case 1: return v.y;
+    case 2: return v.z;
+    default: return v.w;
+  }
+}
+
+// eval_sh_rgb (splat_surface_direct.wgsl:233-326): the basis scalars are the
+// left-associated prefixes of each WGSL term, so each channel accumulates
+// exactly the WGSL sequence. `f` holds (DC rgb, rest 1 rgb, rest 2 rgb, ...).
+template <int kPlanes>
+__device__ __forceinline__ void eval_sh(const float4 *f, uint32_t degree, float x, float y,
+                                        float z, float rgb[3]) {
+  const float c0 = 0.28209479177387814f;
+  const float c1 = 0.4886025119029199f;
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) rgb[ch] = c0 * plane_float(f, ch);
+  if (degree == 0) return;
+  {
+    float b0 = c1 * y, b1 = c1 * z, b2 = c1 * x;
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch)
+      rgb[ch] = rgb[ch] - b0 * plane_float(f, 3 + ch) + b1 * plane_float(f, 6 + ch) -
+                b2 * plane_float(f, 9 + ch);
+  }
+  if (degree == 1 || kPlanes < 7) return;
+  float xx = x * x, yy = y * y, zz = z * z;
+  float xy = x * y, yz = y * z, xz = x * z;
+  {
+    float b[5] = {1.0925484305920792f * xy, -1.0925484305920792f * yz,
+                  0.31539156525252005f * (2.0f * zz - xx - yy), -1.0925484305920792f * xz,
+                  0.5462742152960396f * (xx - yy)};
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+      float r = rgb[ch];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) r = r + b[k] * plane_float(f, 3 * (4 + k) + ch);
+      rgb[ch] = r;
+    }
+  }
+  if (degree == 2 || kPlanes < 12) return;
+  {
+    float b[7] = {-0.5900435899266435f * y * (3.0f * xx - yy),
+                  2.890611442640554f * xy * z,
+                  -0.4570457994644658f * y * (4.0f * zz - xx - yy),
+                  0.3731763325901154f * z * (2.0f * zz - 3.0f * xx - 3.0f * yy),
+                  -0.4570457994644658f * x * (4.0f * zz - xx - yy),
+                  1.445305721320277f * z * (xx - yy),
+                  -0.5900435899266435f * x * (xx - 3.0f * yy)};
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+      float r = rgb[ch];
+#pragma unroll
+      for (int k = 0; k < 7; ++k) r = r + b[k] * plane_float(f, 3 * (9 + k) + ch);
+      rgb[ch] = r;
+    }
+  }
+  if (degree == 3 || kPlanes < 19) return;
+  {
+    float b[9] = {2.5033429417967046f * xy * (xx - yy),
+                  -1.7701307697799304f * yz * (3.0f * xx - yy),
+                  0.9461746957575601f * xy * (7.0f * zz - 1.0f),
+                  -0.6690465435572892f * yz * (7.0f * zz - 3.0f),
+                  0.10578554691520431f * (zz * (35.0f * zz - 30.0f) + 3.0f),
+                  -0.6690465435572892f * xz * (7.0f * zz - 3.0f),
+                  0.47308734787878004f * (xx - yy) * (7.0f * zz - 1.0f),
+                  -1.7701307697799304f * xz * (xx - 3.0f * yy),
+                  0.6258357354491761f * (xx * (xx - 3.0f * yy) - yy * (3.0f * xx - yy))};
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+      float r = rgb[ch];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) r = r + b[k] * plane_float(f, 3 * (16 + k) + ch);
+      rgb[ch] = r;
+    }
+  }
+}
+
+// The per-splat vertex stage for a depth-visible splat. Returns false when
+// project_splat marks the splat invalid (behind near, beyond far, or outside
+// the frustum by its axis extents).
+template <int kPlanes>
+__device__ __forceinline__ bool project(const SceneDev &sc, const FrameParams &p, uint32_t i,
+                                        const float4 &pa, const float rel[3], float depth,
+                                        Record &rec, uint2 &rect, ProjectedDev *dbg) {
+  float px = p.r0[0] * rel[0] + p.r0[1] * rel[1] + p.r0[2] * rel[2];
+  float py = p.r1[0] * rel[0] + p.r1[1] * rel[1] + p.r1[2] * rel[2];
+  float z = depth;
+  if (z < p.near_plane || z > p.far_plane || z <= 1e-6f) return false;
+  float inv_z = 1.0f / z;
+  float x_ndc = (px * p.f) * inv_z / p.aspect;
+  float y_ndc = (py * p.f) * inv_z;
+
+  const float4 ca = sc.cov_a[i];
+  const float4 cb = sc.cov_b[i];
+  Cov6 wc{ca.x, ca.y, ca.z, ca.w, cb.x, cb.y};
+  Cov6 cc{cov_quadratic(wc, p.r0[0], p.r0[1], p.r0[2]), cov_bilinear(wc, p.r0, p.r1),
+          cov_bilinear(wc, p.r0, p.r2),                 cov_quadratic(wc, p.r1[0], p.r1[1], p.r1[2]),
+          cov_bilinear(wc, p.r1, p.r2),                 cov_quadratic(wc, p.r2[0], p.r2[1], p.r2[2])};
+  float x_cl = clampf(px / z, -p.lim_x, p.lim_x) * z;
+  float y_cl = clampf(py / z, -p.lim_y, p.lim_y) * z;
+  float inv_z2 = inv_z * inv_z;
+  float j00 = p.fx * inv_z;
+  float j02 = -p.fx * x_cl * inv_z2;
+  float j11 = p.fy * inv_z;
+  float j12 = -p.fy * y_cl * inv_z2;
+  float cov01 = j00 * j11 * cc.xy + j00 * j12 * cc.xz + j02 * j11 * cc.yz + j02 * j12 * cc.zz;
+  float a = j00 * j00 * cc.xx + 2.0f * j00 * j02 * cc.xz + j02 * j02 * cc.zz;
+  float b = cov01;
+  float c = j11 * j11 * cc.yy + 2.0f * j11 * j12 * cc.yz + j12 * j12 * cc.zz;
+  a = a + p.blur_x;
+  c = c + p.blur_y;
+  float apco2 = (a + c) * 0.5f;
+  float amco2 = (a - c) * 0.5f;
+  float term = sqrtf(fmaxf(amco2 * amco2 + b * b, 0.0f));
+  float major = fmaxf(apco2 + term, 1e-10f);
+  float minor = fmaxf(apco2 - term, 1e-10f);
+  float ux = 1.0f, uy = 0.0f;
+  if (fabsf(b) > 1e-8f) {
+    float vx = b, vy = major - a;
+    float len2 = vx * vx + vy * vy;
+    if (!(len2 <= 1e-20f)) {
+      float inv = 1.0f / sqrtf(len2);
+      ux = vx * inv;
+      uy = vy * inv;
+    }
+  } else if (a < c) {
+    ux = 0.0f;
+    uy = 1.0f;
+  }
+  float major_r = clampf(sqrtf(major) * 3.0f, 1e-4f, 2.0f);
+  float minor_r = clampf(sqrtf(minor) * 3.0f, 1e-4f, 2.0f);
+  major_r = fminf(major_r, minor_r * 64.0f);
+  float au0 = ux * major_r, au1 = uy * major_r;
+  float av0 = -uy * minor_r, av1 = ux * minor_r;
+  float ext_x = fabsf(au0) + fabsf(av0);
+  float ext_y = fabsf(au1) + fabsf(av1);
+  if (x_ndc + ext_x < -1.0f || x_ndc - ext_x > 1.0f || y_ndc + ext_y < -1.0f ||
+      y_ndc - ext_y > 1.0f)
+    return false;
+
+  const float al = pa.w;
+  const float s = cb.z;
+  // eval_color: dir = normalize3_or_default(pos - cam, (0,0,1))
+  float len2 = rel[0] * rel[0] + rel[1] * rel[1] + rel[2] * rel[2];
+  float dx = 0.0f, dy = 0.0f, dz = 1.0f;
+  if (!(len2 <= 1e-20f)) {
+    float inv = 1.0f / sqrtf(len2);
+    dx = rel[0] * inv;
+    dy = rel[1] * inv;
+    dz = rel[2] * inv;
+  }
+  float4 fbuf[kPlanes];
+#pragma unroll
+  for (int k = 0; k < kPlanes; ++k) fbuf[k] = sc.color[(size_t)k * sc.n + i];
+  float rgb[3];
+  eval_sh<kPlanes>(fbuf, p.sh_degree, dx, dy, dz, rgb);
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) rgb[ch] = clampf(rgb[ch] + 0.5f, 0.0f, 1.0f);
+  float pr = rgb[0] * al, pg = rgb[1] * al, pb = rgb[2] * al;
+
+  float cxp = (x_ndc + 1.0f) * p.half_w - 0.5f;
+  float cyp = (1.0f - y_ndc) * p.half_h - 0.5f;
+  float uu = au0 * au0 + au1 * au1;
+  float vv = av0 * av0 + av1 * av1;
+  rec.a = make_float4(cxp, cyp, (au0 * p.sx) / uu, (au1 * p.sy) / uu);
+  rec.b = make_float4((av0 * p.sx) / vv, (av1 * p.sy) / vv, s, al);
+  rec.c = make_float4(pr, pg, pb, 0.0f);
+
+  rect = make_uint2(0u, 0u);
+  if (al > 1.0f / 256.0f) {
+    float ex = s * sqrtf(au0 * au0 + av0 * av0) * p.half_w;
+    float ey = s * sqrtf(au1 * au1 + av1 * av1) * p.half_h;
+    ex = ex * 1.00001f + 0.001f;
+    ey = ey * 1.00001f + 0.001f;
+    float fx0 = fmaxf(ceilf(cxp - ex), 0.0f);
+    float fx1 = fminf(floorf(cxp + ex), (float)(p.width - 1));
+    float fy0 = fmaxf(ceilf(cyp - ey), 0.0f);
+    float fy1 = fminf(floorf(cyp + ey), (float)(p.height - 1));
+    if (fx0 <= fx1 && fy0 <= fy1) {
+      uint32_t tx0 = (uint32_t)fx0 / p.tile, tx1 = (uint32_t)fx1 / p.tile + 1;
+      uint32_t ty0 = (uint32_t)fy0 / p.tile, ty1 = (uint32_t)fy1 / p.tile + 1;
+      rect = make_uint2(tx0 | (ty0 << 16), tx1 | (ty1 << 16));
+    }
+  }
+  if (dbg) {
+    dbg->center_ndc[0] = x_ndc;
+    dbg->center_ndc[1] = y_ndc;
+    dbg->axis_u[0] = au0;
+    dbg->axis_u[1] = au1;
+    dbg->axis_v[0] = av0;
+    dbg->axis_v[1] = av1;
+    dbg->color[0] = pr;
+    dbg->color[1] = pg;
+    dbg->color[2] = pb;
+    dbg->color[3] = al;
+    dbg->extent_scale = s;
+    dbg->flags |= 2u;
+    dbg->tile_x0 = (uint16_t)(rect.x & 0xffffu);
+    dbg->tile_y0 = (uint16_t)(rect.x >> 16);
+    dbg->tile_x1 = (uint16_t)(rect.y & 0xffffu);
+    dbg->tile_y1 = (uint16_t)(rect.y >> 16);
+  }
+  return true;
+}
+
+constexpr int kK1Threads = 256;
+
+template <int kPlanes, bool kDebug>
+__global__ void __launch_bounds__(kK1Threads) preprocess_kernel(
+    SceneDev sc, FrameParams p, uint32_t *__restrict__ vis_keys, uint32_t *__restrict__ vis_ids,
+    uint2 *__restrict__ rects, Record *__restrict__ records, unsigned long long *status,
+    FrameCounters *counters, ProjectedDev *__restrict__ dbg_out) {
+  __shared__ uint32_t s_block;
+  __shared__ uint32_t s_warp[kK1Threads / 32];
+  __shared__ uint32_t s_prefix;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_block = atomicAdd(&counters->k1_ticket, 1u);
+  __syncthreads();
+  const uint32_t block = s_block;
+  const uint32_t i = block * kK1Threads + threadIdx.x;
+  const bool valid = i < sc.n;
+
+  float4 pa = valid ? sc.pos_alpha[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  float rel[3] = {pa.x - p.cam[0], pa.y - p.cam[1], pa.z - p.cam[2]};
+  float depth = p.r2[0] * rel[0] + p.r2[1] * rel[1] + p.r2[2] * rel[2];
+  const bool vis = valid && depth >= p.near_plane && depth <= p.far_plane;
+
+  // Block-wide compaction of the visible flags, warp ballots first.
+  const uint32_t ballot = __ballot_sync(0xffffffffu, vis);
+  const uint32_t rank = __popc(ballot & lanemask_lt());
+  if (lane == 0) s_warp[warp] = __popc(ballot);
+  __syncthreads();
+  uint32_t warp_prefix = 0, block_total = 0;
+#pragma unroll
+  for (int w = 0; w < kK1Threads / 32; ++w) {
+    uint32_t c = s_warp[w];
+    warp_prefix += (w < (int)warp) ? c : 0u;
+    block_total += c;
+  }
+  if (warp == 0) {
+    unsigned long long ex = lookback_warp(status, block, block_total, &counters->error);
+    if (lane == 0) s_prefix = (uint32_t)ex;
+  }
+  __syncthreads();
+  const uint32_t prefix = s_prefix;
+  if (threadIdx.x == 0 && block == (sc.n - 1) / kK1Threads) counters->visible = prefix + block_total;
+
+  ProjectedDev *dbg = nullptr;
+  if (kDebug && valid) {
+    dbg = &dbg_out[i];
+    ProjectedDev z = {};
+    z.depth = depth;
+    z.flags = vis ? 1u : 0u;
+    *dbg = z;
+  }
+  if (!vis) return;
+  const uint32_t slot = prefix + warp_prefix + rank;
+  vis_keys[slot] = ~__float_as_uint(fmaxf(depth, 0.0f));
+  vis_ids[slot] = i;
+
+  Record rec;
+  uint2 rect = make_uint2(0u, 0u);
+  bool drawn = project<kPlanes>(sc, p, i, pa, rel, depth, rec, rect, dbg);
+  rects[i] = rect;
+  if (drawn) {
+    records[i] = rec;
+    uint32_t dmask = __ballot_sync(__activemask(), true);
+    if (lane == __ffs(dmask) - 1) atomicAdd(&counters->drawn, __popc(dmask));
+  }
+}
+
+template <int kPlanes>
+void launch_k1(const SceneDev &sc, const FrameParams &p, const K1Buffers &b, bool debug,
+               cudaStream_t stream) {
+  uint32_t blocks = (sc.n + kK1Threads - 1) / kK1Threads;
+  if (blocks == 0) return;
+  if (debug)
+    preprocess_kernel<kPlanes, true><<<blocks, kK1Threads, 0, stream>>>(
+        sc, p, b.vis_keys, b.vis_ids, b.rects, b.records, b.status, b.counters, b.projected);
+  else
+    preprocess_kernel<kPlanes, false><<<blocks, kK1Threads, 0, stream>>>(
+        sc, p, b.vis_keys, b.vis_ids, b.rects, b.records, b.status, b.counters, nullptr);
+}
+
+}  // namespace
+
+void launch_preprocess(const SceneDev &sc, const FrameParams &p, const K1Buffers &b, bool debug,
+                       cudaStream_t stream) {
+  switch (sc.planes) {
+    case 1: launch_k1<1>(sc, p, b, debug, stream); break;
+    case 3: launch_k1<3>(sc, p, b, debug, stream); break;
+    case 7: launch_k1<7>(sc, p, b, debug, stream); break;
+    case 12: launch_k1<12>(sc, p, b, debug, stream); break;
+    default: launch_k1<19>(sc, p, b, debug, stream); break;
+  }
+}
+
+}  // namespace gsr

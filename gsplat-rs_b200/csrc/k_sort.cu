@@ -1,0 +1,271 @@
+// K3: onesweep LSD radix sort of (u32 key, u32 value) pairs, ascending and
+// stable, 8-bit digits.
+//
+//   1. histogram kernel: one read of the keys builds the digit histograms of
+//      every pass (shared-memory histograms, one global add per bin and block);
+//   2. plan kernel (one block): exclusive digit offsets per pass; a pass whose
+//      keys all share one digit is marked skipped, and the ping-pong buffer of
+//      every remaining pass is fixed on the device, so no host round trip is
+//      needed between passes;
+//   3. one kernel per pass: each block takes the next tile of 256*IPT keys
+//      from an atomic ticket (launch order, so look-back never waits on a
+//      block that has not started), ranks its keys stably per digit with warp
+//      match votes, publishes its digit counts, resolves its global digit
+//      offsets by decoupled look-back over the predecessor tiles (bounded
+//      waits), reorders the tile in shared memory and writes digit runs
+//      contiguously.
+//
+// Stability over equal keys is what reproduces the reference's tie order
+// (crates/gsplat-sort/src/radix.rs:11-58: stable LSD passes, equal keys keep
+// their input order).
+
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace gsr {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr uint32_t kFlagA = 1u << 30;
+constexpr uint32_t kFlagP = 2u << 30;
+constexpr uint32_t kMask = (1u << 30) - 1;
+
+template <int kIpt>
+__global__ void __launch_bounds__(kThreads) hist_kernel(const uint32_t *__restrict__ keys,
+                                                        const uint32_t *__restrict__ count,
+                                                        uint32_t begin_bit, uint32_t passes,
+                                                        uint32_t *__restrict__ hist) {
+  constexpr uint32_t kTile = kThreads * kIpt;
+  __shared__ uint32_t s_hist[4][256];
+  const uint32_t n = *count;
+  const uint32_t base = blockIdx.x * kTile;
+  if (base >= n) return;
+  for (uint32_t k = threadIdx.x; k < 4 * 256; k += kThreads) (&s_hist[0][0])[k] = 0;
+  __syncthreads();
+  const uint32_t end = min(n, base + kTile);
+  for (uint32_t idx = base + threadIdx.x; idx < end; idx += kThreads) {
+    uint32_t key = keys[idx];
+    for (uint32_t p = 0; p < passes; ++p) atomicAdd(&s_hist[p][(key >> (begin_bit + 8 * p)) & 255u], 1u);
+  }
+  __syncthreads();
+  for (uint32_t p = 0; p < passes; ++p) {
+    uint32_t c = s_hist[p][threadIdx.x];
+    if (c) atomicAdd(&hist[p * 256 + threadIdx.x], c);
+  }
+}
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s_wsum,
+                                                         uint32_t &total) {
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= (uint32_t)o) inc += t;
+  }
+  if (lane == 31) s_wsum[warp] = inc;
+  __syncthreads();
+  uint32_t before = 0;
+  total = 0;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) {
+    uint32_t c = s_wsum[w];
+    before += (w < (int)warp) ? c : 0u;
+    total += c;
+  }
+  __syncthreads();
+  return before + inc - v;
+}
+
+__global__ void __launch_bounds__(kThreads) plan_kernel(const uint32_t *__restrict__ count,
+                                                        const uint32_t *__restrict__ hist,
+                                                        uint32_t passes, SortPlan *plan) {
+  __shared__ uint32_t s_wsum[kWarps];
+  __shared__ uint32_t s_trivial[4];
+  const uint32_t n = *count;
+  const uint32_t d = threadIdx.x;
+  if (d < 4) s_trivial[d] = 0;
+  __syncthreads();
+  for (uint32_t p = 0; p < passes; ++p) {
+    uint32_t c = hist[p * 256 + d];
+    uint32_t total;
+    uint32_t ex = block_exclusive_scan(c, s_wsum, total);
+    plan->digit_offset[p][d] = ex;
+    if (c == n) s_trivial[p] = 1;  // n == 0 marks every pass trivial
+  }
+  __syncthreads();
+  if (d == 0) {
+    uint32_t buf = 0;
+    for (uint32_t p = 0; p < 8; ++p) {
+      uint32_t skip = p < passes ? s_trivial[p] : 1u;
+      plan->skip[p] = skip;
+      plan->src[p] = buf;
+      if (!skip) buf ^= 1u;
+    }
+    plan->final_buffer = buf;
+    plan->n = n;
+    plan->passes = passes;
+  }
+}
+
+template <int kIpt>
+__global__ void __launch_bounds__(kThreads) pass_kernel(const SortPlan *__restrict__ plan,
+                                                        uint32_t pass, uint32_t shift,
+                                                        uint32_t *k0, uint32_t *v0, uint32_t *k1,
+                                                        uint32_t *v1, uint32_t *status,
+                                                        uint32_t *ticket, uint32_t *error) {
+  constexpr uint32_t kTile = kThreads * kIpt;
+  __shared__ uint32_t s_warp_hist[kWarps][256];
+  __shared__ uint32_t s_keys[kTile];
+  __shared__ uint32_t s_vals[kTile];
+  __shared__ uint32_t s_block_start[256];
+  __shared__ uint32_t s_global[256];
+  __shared__ uint32_t s_wsum[kWarps];
+  __shared__ uint32_t s_tile;
+
+  if (plan->skip[pass]) return;
+  const uint32_t n = plan->n;
+  const bool from0 = plan->src[pass] == 0;
+  const uint32_t *__restrict__ in_k = from0 ? k0 : k1;
+  const uint32_t *__restrict__ in_v = from0 ? v0 : v1;
+  uint32_t *__restrict__ out_k = from0 ? k1 : k0;
+  uint32_t *__restrict__ out_v = from0 ? v1 : v0;
+
+  if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+  for (uint32_t k = threadIdx.x; k < kWarps * 256; k += kThreads) (&s_warp_hist[0][0])[k] = 0;
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint32_t base = tile * kTile;
+  if (base >= n) return;
+
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t warp_base = base + warp * 32 * kIpt;
+  uint32_t key[kIpt], val[kIpt], rank[kIpt];
+#pragma unroll
+  for (int i = 0; i < kIpt; ++i) {
+    uint32_t idx = warp_base + i * 32 + lane;
+    if (idx < n) {
+      key[i] = in_k[idx];
+      val[i] = in_v[idx];
+    } else {
+      key[i] = 0xffffffffu;  // ranks after every real key of digit 255
+      val[i] = 0;
+    }
+  }
+  // Stable per-warp ranking: items are visited in position order
+  // (i outer, lane inner), peers with the same digit are found by match vote.
+  uint32_t *wh = s_warp_hist[warp];
+  const uint32_t lt = lanemask_lt();
+#pragma unroll
+  for (int i = 0; i < kIpt; ++i) {
+    uint32_t d = (key[i] >> shift) & 255u;
+    uint32_t peers = __match_any_sync(0xffffffffu, d);
+    uint32_t before = wh[d];
+    rank[i] = before + __popc(peers & lt);
+    __syncwarp();
+    if (lane == (uint32_t)(__ffs(peers) - 1)) wh[d] = before + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // Per digit: exclusive prefix over warps, block count, publish, look back.
+  const uint32_t d = threadIdx.x;
+  uint32_t block_count = 0;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) {
+    uint32_t c = s_warp_hist[w][d];
+    s_warp_hist[w][d] = block_count;
+    block_count += c;
+  }
+  uint32_t *my_status = &status[(size_t)tile * 256];
+  st_relaxed_u32(&my_status[d], (tile == 0 ? kFlagP : kFlagA) | block_count);
+  uint32_t total;
+  s_block_start[d] = block_exclusive_scan(block_count, s_wsum, total);
+
+  uint32_t exclusive = 0;
+  if (tile > 0) {
+    int32_t t = (int32_t)tile - 1;
+    uint32_t spins = 0;
+    while (t >= 0) {
+      uint32_t s = ld_relaxed_u32(&status[(size_t)t * 256 + d]);
+      uint32_t flag = s & ~kMask;
+      if (flag == 0) {
+        if (++spins > kSpinLimit) {
+          atomicOr(error, kErrLookbackTimeout);
+          break;
+        }
+        __nanosleep(20);
+        continue;
+      }
+      exclusive += s & kMask;
+      if (flag == kFlagP) break;
+      --t;
+    }
+    st_relaxed_u32(&my_status[d], kFlagP | (exclusive + block_count));
+  }
+  s_global[d] = plan->digit_offset[pass][d] + exclusive;
+  __syncthreads();
+
+  // Reorder the tile by digit in shared memory.
+#pragma unroll
+  for (int i = 0; i < kIpt; ++i) {
+    uint32_t dg = (key[i] >> shift) & 255u;
+    uint32_t pos = s_block_start[dg] + s_warp_hist[warp][dg] + rank[i];
+    s_keys[pos] = key[i];
+    s_vals[pos] = val[i];
+  }
+  __syncthreads();
+  // Each digit run lands contiguously in the output.
+#pragma unroll 4
+  for (uint32_t s = threadIdx.x; s < kTile; s += kThreads) {
+    uint32_t k = s_keys[s];
+    uint32_t dg = (k >> shift) & 255u;
+    uint32_t g = s_global[dg] + (s - s_block_start[dg]);
+    if (g < n) {
+      out_k[g] = k;
+      out_v[g] = s_vals[s];
+    }
+  }
+}
+
+inline uint32_t ipt_for(uint32_t capacity) { return capacity <= (1u << 21) ? 8u : 16u; }
+inline uint32_t tiles_for(uint32_t capacity) {
+  uint32_t tile = kThreads * ipt_for(capacity);
+  return (capacity + tile - 1) / tile;
+}
+
+}  // namespace
+
+// Scratch layout: [tickets: 64 words][hist: 4*256][status: passes*tiles*256].
+uint64_t sort_work_words(uint32_t capacity, uint32_t passes) {
+  return 64ull + 4ull * 256ull + (uint64_t)passes * tiles_for(capacity) * 256ull;
+}
+
+void launch_sort(const SortBuffers &b, cudaStream_t stream) {
+  const uint32_t tiles = tiles_for(b.capacity);
+  const uint64_t words = sort_work_words(b.capacity, b.passes);
+  cudaMemsetAsync(b.work, 0, words * sizeof(uint32_t), stream);
+  uint32_t *tickets = b.work;
+  uint32_t *hist = b.work + 64;
+  uint32_t *status = b.work + 64 + 4 * 256;
+  const uint32_t grid = tiles ? tiles : 1;
+  if (ipt_for(b.capacity) == 8)
+    hist_kernel<8><<<grid, kThreads, 0, stream>>>(b.keys0, b.count, b.begin_bit, b.passes, hist);
+  else
+    hist_kernel<16><<<grid, kThreads, 0, stream>>>(b.keys0, b.count, b.begin_bit, b.passes, hist);
+  plan_kernel<<<1, kThreads, 0, stream>>>(b.count, hist, b.passes, b.plan);
+  for (uint32_t p = 0; p < b.passes; ++p) {
+    uint32_t *st = status + (size_t)p * tiles * 256;
+    if (ipt_for(b.capacity) == 8)
+      pass_kernel<8><<<grid, kThreads, 0, stream>>>(b.plan, p, b.begin_bit + 8 * p, b.keys0,
+                                                    b.vals0, b.keys1, b.vals1, st, tickets + p,
+                                                    b.error);
+    else
+      pass_kernel<16><<<grid, kThreads, 0, stream>>>(b.plan, p, b.begin_bit + 8 * p, b.keys0,
+                                                     b.vals0, b.keys1, b.vals1, st, tickets + p,
+                                                     b.error);
+  }
+}
+
+}  // namespace gsr

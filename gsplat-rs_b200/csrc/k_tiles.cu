@@ -1,0 +1,154 @@
+// K2: (tile, splat) pair emission, and the tile-range build.
+//
+// Emission walks the depth-sorted visible ids. Each block takes the next
+// 1024 sorted positions from an atomic ticket, sums their tile counts (area
+// of each splat's tile rect), and gets its global pair offset from a
+// decoupled look-back, so pairs land in exactly the order a sequential walk
+// would write them: depth order, then rect rows, then rect columns. The
+// block then writes its pairs cooperatively — thread t writes pairs t,
+// t+256, ... and finds the owning splat by binary search over the block's
+// inclusive counts — so a splat covering thousands of tiles does not leave
+// one thread doing all the work.
+
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace gsr {
+namespace {
+
+constexpr int kEmitThreads = 256;
+constexpr int kEmitIpt = 4;
+constexpr int kEmitItems = kEmitThreads * kEmitIpt;
+
+__global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b, uint32_t tiles_x) {
+  __shared__ uint32_t s_incl[kEmitItems];
+  __shared__ uint32_t s_id[kEmitItems];
+  __shared__ uint2 s_rect[kEmitItems];
+  __shared__ uint32_t s_wsum[kEmitThreads / 32];
+  __shared__ uint32_t s_block;
+  __shared__ unsigned long long s_prefix;
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_block = atomicAdd(&b.counters->emit_ticket, 1u);
+  __syncthreads();
+  const uint32_t V = b.counters->visible;
+  const uint32_t block = s_block;
+  const uint32_t start = block * kEmitItems;
+  if (start >= V) return;
+  const uint32_t *ids = b.depth_plan->final_buffer == 0 ? b.ids0 : b.ids1;
+
+  uint32_t cnt[kEmitIpt];
+  uint32_t local = 0;
+#pragma unroll
+  for (int k = 0; k < kEmitIpt; ++k) {
+    uint32_t slot = tid * kEmitIpt + k;
+    uint32_t j = start + slot;
+    uint32_t id = 0, c = 0;
+    uint2 r = make_uint2(0u, 0u);
+    if (j < V) {
+      id = ids[j];
+      r = b.rects[id];
+      uint32_t w = (r.y & 0xffffu) - (r.x & 0xffffu);
+      uint32_t h = (r.y >> 16) - (r.x >> 16);
+      c = w * h;
+    }
+    s_id[slot] = id;
+    s_rect[slot] = r;
+    cnt[k] = c;
+    local += c;
+  }
+  // Block exclusive scan of the per-thread sums.
+  uint32_t inc = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= (uint32_t)o) inc += t;
+  }
+  if (lane == 31) s_wsum[warp] = inc;
+  __syncthreads();
+  uint32_t before = 0, total = 0;
+#pragma unroll
+  for (int w = 0; w < kEmitThreads / 32; ++w) {
+    uint32_t c = s_wsum[w];
+    before += (w < (int)warp) ? c : 0u;
+    total += c;
+  }
+  uint32_t run = before + inc - local;
+#pragma unroll
+  for (int k = 0; k < kEmitIpt; ++k) {
+    run += cnt[k];
+    s_incl[tid * kEmitIpt + k] = run;
+  }
+  if (warp == 0) {
+    unsigned long long ex = lookback_warp(b.status, block, total, &b.counters->error);
+    if (lane == 0) s_prefix = ex;
+  }
+  __syncthreads();
+  const unsigned long long prefix = s_prefix;
+  if (tid == 0 && block == (V - 1) / kEmitItems) {
+    unsigned long long all = prefix + total;
+    b.counters->keys = all;
+    b.counters->pairs = (uint32_t)(all < b.capacity ? all : b.capacity);
+    if (all > b.capacity) b.counters->overflow = 1u;
+  }
+  for (uint32_t k = tid; k < total; k += kEmitThreads) {
+    unsigned long long g = prefix + k;
+    if (g >= b.capacity) break;
+    uint32_t lo = 0, hi = kEmitItems - 1;
+    while (lo < hi) {
+      uint32_t mid = (lo + hi) >> 1;
+      if (s_incl[mid] > k) hi = mid;
+      else lo = mid + 1;
+    }
+    uint32_t first = lo ? s_incl[lo - 1] : 0u;
+    uint32_t off = k - first;
+    uint2 r = s_rect[lo];
+    uint32_t x0 = r.x & 0xffffu, y0 = r.x >> 16;
+    uint32_t w = (r.y & 0xffffu) - x0;
+    uint32_t ty = y0 + off / w, tx = x0 + off % w;
+    b.tile_keys[g] = ty * tiles_x + tx;
+    b.tile_vals[g] = s_id[lo];
+  }
+}
+
+__global__ void ranges_kernel(const SortPlan *__restrict__ plan, const uint32_t *k0,
+                              const uint32_t *k1, const FrameCounters *__restrict__ counters,
+                              uint2 *__restrict__ ranges) {
+  const uint32_t K = counters->pairs;
+  const uint32_t *keys = plan->final_buffer == 0 ? k0 : k1;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < K; i += gridDim.x * blockDim.x) {
+    uint32_t t = keys[i];
+    if (i == 0 || keys[i - 1] != t) ranges[t].x = i;
+    if (i + 1 == K || keys[i + 1] != t) ranges[t].y = i + 1;
+  }
+}
+
+__global__ void fill_kernel(uint32_t *dst, uint32_t value, uint64_t count) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    dst[i] = value;
+}
+
+}  // namespace
+
+void launch_emit(const EmitBuffers &b, const FrameParams &p, cudaStream_t stream) {
+  uint32_t blocks = (b.n + kEmitItems - 1) / kEmitItems;
+  if (blocks == 0) return;
+  emit_kernel<<<blocks, kEmitThreads, 0, stream>>>(b, p.tiles_x);
+}
+
+void launch_ranges(const SortPlan *tile_plan, const uint32_t *keys0, const uint32_t *keys1,
+                   const FrameCounters *counters, uint32_t capacity, uint2 *ranges,
+                   cudaStream_t stream) {
+  uint32_t blocks = (capacity + 255) / 256;
+  blocks = blocks < 148 * 8 ? (blocks ? blocks : 1) : 148 * 8;
+  ranges_kernel<<<blocks, 256, 0, stream>>>(tile_plan, keys0, keys1, counters, ranges);
+}
+
+void launch_fill_u32(uint32_t *dst, uint32_t value, uint64_t count, cudaStream_t stream) {
+  if (count == 0) return;
+  uint64_t blocks = (count + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  fill_kernel<<<(uint32_t)blocks, 256, 0, stream>>>(dst, value, count);
+}
+
+}  // namespace gsr

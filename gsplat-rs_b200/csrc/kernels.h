@@ -1,0 +1,77 @@
+// Launch interface of the CUDA kernels (host-callable, plain pointers).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gsr_host.h"
+
+namespace gsr {
+
+struct SceneDev;
+struct Record;
+struct ProjectedDev;
+struct FrameCounters;
+struct SortPlan;
+
+// ---- K1: preprocess -------------------------------------------------------
+struct K1Buffers {
+  uint32_t *vis_keys;          // [n] ~depth bits of visible splats, compacted
+  uint32_t *vis_ids;           // [n] their ids, ascending
+  uint2 *rects;                // [n] tile rect per visible splat
+  Record *records;             // [n] raster record per drawn splat
+  unsigned long long *status;  // [ceil(n/256)] look-back words, zeroed
+  FrameCounters *counters;
+  ProjectedDev *projected;     // [n] debug tap, or null
+};
+void launch_preprocess(const SceneDev &sc, const FrameParams &p, const K1Buffers &b, bool debug,
+                       cudaStream_t stream);
+
+// ---- K3: onesweep LSD radix sort of (u32 key, u32 value) pairs -----------
+// Sorts ascending and stably over bits [begin_bit, begin_bit + 8*passes) of
+// the key. The item count is read from device memory (*count), the grids are
+// sized from `capacity`. The result ends in (keys0, vals0) or (keys1, vals1)
+// as plan->final_buffer says.
+struct SortBuffers {
+  uint32_t *keys0, *vals0, *keys1, *vals1;
+  const uint32_t *count;
+  uint32_t capacity;
+  uint32_t begin_bit;
+  uint32_t passes;  // 1..4
+  SortPlan *plan;
+  uint32_t *work;   // sort_work_words(capacity, passes) words of scratch
+  uint32_t *error;
+};
+uint64_t sort_work_words(uint32_t capacity, uint32_t passes);
+// Zeroes the scratch (one memset) and launches the histogram, plan and pass
+// kernels on `stream`.
+void launch_sort(const SortBuffers &b, cudaStream_t stream);
+
+// ---- K2: tile-pair emission over the depth-sorted visible ids ------------
+struct EmitBuffers {
+  const SortPlan *depth_plan;      // selects the buffer holding the sorted ids
+  const uint32_t *ids0, *ids1;     // depth-sorted ids, [visible]
+  const uint2 *rects;
+  uint32_t *tile_keys, *tile_vals; // [capacity] output pairs
+  uint64_t capacity;
+  unsigned long long *status;      // [ceil(n/1024)] look-back words, zeroed
+  FrameCounters *counters;
+  uint32_t n;                      // splat count (upper bound of visible)
+};
+void launch_emit(const EmitBuffers &b, const FrameParams &p, cudaStream_t stream);
+
+// ---- tile ranges from the tile-sorted keys -------------------------------
+void launch_ranges(const SortPlan *tile_plan, const uint32_t *keys0, const uint32_t *keys1,
+                   const FrameCounters *counters, uint32_t capacity, uint2 *ranges,
+                   cudaStream_t stream);
+
+// ---- K4: tile raster ------------------------------------------------------
+void launch_raster(const FrameParams &p, const uint2 *ranges, const SortPlan *tile_plan,
+                   const uint32_t *ids0, const uint32_t *ids1, const Record *records,
+                   uint32_t *image, uint32_t blend_mode, const FrameCounters *counters,
+                   uint32_t *sticky, cudaStream_t stream);
+
+// ---- small helpers ----------------------------------------------------------
+void launch_fill_u32(uint32_t *dst, uint32_t value, uint64_t count, cudaStream_t stream);
+
+}  // namespace gsr

@@ -1,0 +1,170 @@
+/*
+ * gsplat_cuda.h — additive exports of the B200 CUDA SortedAlpha renderer.
+ *
+ * Nothing here changes the v0.1 ABI in gsplat.h; these entry points add what
+ * the reference's ABI lacks (reference gsplat.h:105-111 has no pixel readback
+ * and no load from memory) plus the debug taps the parity tests read, the
+ * standalone GPU sort that replaces gsplat-sort's backends, and batched
+ * rendering. Error convention as in gsplat.h: int32_t GsplatErrorCode plus a
+ * thread-local gsplat_last_error_message().
+ */
+#ifndef GSPLAT_CUDA_H
+#define GSPLAT_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "gsplat.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Compositing of the per-tile splat lists. */
+typedef enum GsplatBlendMode {
+  /* Default. FP32 front-to-back: C += (rgb*a*g)*T, T *= (1 - a*g); a pixel
+   * stops once T < 1e-4 (after adding the splat that crossed it) and a warp
+   * stops when all its pixels have. One UNORM8 rounding at the end. */
+  GSPLAT_BLEND_FP32_FRONT_TO_BACK = 0,
+  /* Parity mode with the reference's Rgba8Unorm target: back-to-front,
+   * dst = src + dst*(1 - src.a) rounded to UNORM8 after every splat, as the
+   * reference's premultiplied-alpha blend state does
+   * (crates/gsplat-render-wgpu/src/draw_pass.rs:75, lib.rs:53). */
+  GSPLAT_BLEND_UNORM8_BACK_TO_FRONT = 1,
+} GsplatBlendMode;
+
+/* A scene in the reference's SceneBuffers layout
+ * (crates/gsplat-core/src/lib.rs:201-213): RUF positions, opacity logits,
+ * log-scales, xyzw rotations, DC coefficients and, for sh_degree > 0,
+ * channel-major sh_rest ([R c1..cK, G c1..cK, B c1..cK] per splat,
+ * K = (sh_degree+1)^2 - 1). Host pointers; the library copies the data. */
+typedef struct GsplatSceneDesc {
+  uint64_t count;
+  uint32_t sh_degree;
+  uint32_t reserved;
+  const float *positions;     /* 3*count */
+  const float *opacity;       /* count */
+  const float *scale_xyz;     /* 3*count */
+  const float *rotation_xyzw; /* 4*count */
+  const float *color_dc;      /* 3*count */
+  const float *sh_rest;       /* count*3*K, or NULL when sh_degree == 0 */
+} GsplatSceneDesc;
+
+/* One splat after the vertex stage of the reference shader
+ * (crates/gsplat-render-wgpu/shaders/splat_surface_direct.wgsl:131-217,
+ * 328-334); 64 bytes. Written for every splat id by the debug tap. */
+typedef struct GsplatProjectedSplat {
+  float center_ndc[2];
+  float axis_u[2];
+  float axis_v[2];
+  float color[4]; /* premultiplied rgb, alpha */
+  float extent_scale;
+  float depth;
+  uint32_t flags; /* bit0 depth-visible, bit1 drawn (inside the frustum) */
+  uint16_t tile_x0, tile_y0, tile_x1, tile_y1; /* tile rect, ends exclusive */
+  uint32_t reserved;
+} GsplatProjectedSplat;
+
+/* Counters and device timings of the last frame of a context. */
+typedef struct GsplatFrameCounts {
+  uint64_t visible;      /* depth-visible splats (= GsplatStats.visible_count) */
+  uint64_t drawn;        /* visible splats inside the frustum */
+  uint64_t tile_keys;    /* (tile, splat) pairs emitted */
+  uint64_t key_capacity; /* pair capacity of the context's workspace */
+  uint32_t tiles_x, tiles_y, tile_size, blend_mode;
+  float preprocess_ms, sort_ms, raster_ms, frame_ms;
+  uint32_t frame_reruns; /* frames re-run after growing the pair buffers */
+  uint32_t reserved;
+} GsplatFrameCounts;
+
+/* ---- context extensions ---- */
+
+/* Renderer::set_size (crates/gsplat-render-wgpu/src/lib.rs:383-399). */
+int32_t gsplat_context_set_size(GsplatContext *ctx, uint32_t width, uint32_t height);
+int32_t gsplat_context_get_config(const GsplatContext *ctx, GsplatConfig *out_config);
+int32_t gsplat_context_get_camera(const GsplatContext *ctx, GsplatCamera *out_camera);
+int32_t gsplat_context_set_blend_mode(GsplatContext *ctx, uint32_t mode);
+/* Tile edge in pixels: 8 or 16 (default 16). Images do not depend on it. */
+int32_t gsplat_context_set_tile_size(GsplatContext *ctx, uint32_t tile);
+/* When enabled, render_frame also keeps the per-splat projected records for
+ * gsplat_context_debug_projected. Off by default. */
+int32_t gsplat_context_set_debug_taps(GsplatContext *ctx, uint32_t enabled);
+
+/* Load a scene from host memory (validated like SceneBuffers::validate,
+ * crates/gsplat-core/src/lib.rs:224-276). Replaces any loaded scene. */
+int32_t gsplat_context_load_scene_buffers(GsplatContext *ctx, const GsplatSceneDesc *scene);
+
+/* Copy the last frame's RGBA8 image (row 0 = top, tight rows of width*4
+ * bytes) into `out`, which must hold width*height*4 bytes. Stands in for
+ * Renderer::readback_rgba8 (lib.rs:779-795). */
+int32_t gsplat_context_readback_rgba8(GsplatContext *ctx, uint8_t *out, uint64_t out_len);
+
+int32_t gsplat_context_get_frame_counts(const GsplatContext *ctx, GsplatFrameCounts *out);
+
+/* Device time of each phase of the last frame, in this order: preprocess,
+ * depth sort, pair emission, tile sort, tile ranges, raster. Writes up to
+ * `capacity` values and the phase count to *out_count. */
+int32_t gsplat_context_get_phase_times(const GsplatContext *ctx, float *out, uint32_t capacity,
+                                       uint32_t *out_count);
+
+/* Enqueue one frame on the context's stream without waiting for it (the
+ * tile-pair buffers keep the size of the last synchronous frame). Errors of
+ * enqueued frames, including a pair-buffer overflow, are reported by the next
+ * gsplat_context_sync, after which stats describe the last enqueued frame. */
+int32_t gsplat_context_render_frame_async(GsplatContext *ctx);
+int32_t gsplat_context_sync(GsplatContext *ctx);
+
+/* The context's cudaStream_t, for callers that order their own device work
+ * (events, copies) with the renderer's frames. */
+int32_t gsplat_context_get_stream(const GsplatContext *ctx, void **out_stream);
+
+/* ---- debug taps of the last frame (copies to host memory) ---- */
+
+/* Depth-sorted visible splat ids: back-to-front, ties by ascending id — the
+ * order Renderer::current_sorted_indices returns after a CPU sort
+ * (lib.rs:605-607). */
+int32_t gsplat_context_debug_order(GsplatContext *ctx, uint32_t *out, uint64_t capacity,
+                                   uint64_t *out_len);
+/* Per splat id (needs gsplat_context_set_debug_taps(ctx, 1) before the frame). */
+int32_t gsplat_context_debug_projected(GsplatContext *ctx, GsplatProjectedSplat *out,
+                                       uint64_t capacity, uint64_t *out_len);
+/* (tile, splat id) pairs in emission order (depth order, rect rows outer). */
+int32_t gsplat_context_debug_tile_pairs(GsplatContext *ctx, uint32_t *tiles, uint32_t *ids,
+                                        uint64_t capacity, uint64_t *out_len);
+/* Per-tile [start, end) ranges (2 words per tile) and the tile-sorted ids. */
+int32_t gsplat_context_debug_tile_ranges(GsplatContext *ctx, uint32_t *ranges,
+                                         uint64_t ranges_capacity, uint32_t *ids,
+                                         uint64_t ids_capacity, uint64_t *out_keys);
+
+/* ---- standalone GPU sort (replaces gsplat-sort's CPU and GPU backends) ---- */
+
+/* CpuSortBackend::sort_values_by_keys (crates/gsplat-sort/src/lib.rs:36-61):
+ * permute `values` so that keys are descending; equal keys keep their input
+ * order. `keys` is not modified. Host pointers; len < 2^30. */
+int32_t gsplat_cuda_sort_values_by_keys(const uint32_t *keys, uint32_t *values, uint64_t len);
+/* CpuSortBackend::sort_pairs (lib.rs:81-101): keys descending, equal keys by
+ * ascending value; both arrays are permuted. */
+int32_t gsplat_cuda_sort_pairs(uint32_t *keys, uint32_t *values, uint64_t len);
+
+/* ---- host utilities ---- */
+
+/* Parsed PLY scene owned by the library (crates/gsplat-io-ply/src/lib.rs:178-235). */
+typedef struct GsplatHostScene GsplatHostScene;
+int32_t gsplat_ply_load(const char *path, GsplatHostScene **out_scene);
+void gsplat_host_scene_destroy(GsplatHostScene *scene);
+int32_t gsplat_host_scene_view(const GsplatHostScene *scene, GsplatSceneDesc *out_desc);
+
+/* camera_rotation_looking_at (crates/gsplat-ffi-c/src/lib.rs:1677-1733). */
+int32_t gsplat_camera_look_at(const float position[3], const float target[3],
+                              float vertical_fov_radians, float near_plane, float far_plane,
+                              GsplatCamera *out_camera);
+
+/* Name, SM count and compute capability of the current CUDA device. */
+int32_t gsplat_cuda_device_info(char *name, uint64_t name_capacity, int32_t *sm_count,
+                                int32_t *cc_major, int32_t *cc_minor);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GSPLAT_CUDA_H */

@@ -1,0 +1,304 @@
+"""GPU parity of the CUDA SortedAlpha path against the CPU oracle, through the
+C ABI. Integer and index work (visible order, tile pairs, tile ranges) must be
+bit-exact; the projected records and both compositing modes are also expected
+bit-exact because the kernels and the oracle run the same f32 operation
+sequence; the FP32 image is additionally held to the reference's own image
+parity gate against the UNORM8 reference model and to <= 2/255 against the
+FP64 evaluation."""
+
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import gsplat_ffi as ffi
+import gsplat_scenes
+from conftest import GOLDEN, ROOT, lcg_seq
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(w, h):
+    return ffi.Context(w, h)
+
+
+def _render(scene, cam, w, h, blend=0, tile=16, debug=True):
+    ctx = _ctx(w, h)
+    ctx.set_debug_taps(debug)
+    ctx.set_blend_mode(blend)
+    ctx.set_tile_size(tile)
+    ctx.load_scene(scene)
+    ctx.set_camera(cam)
+    ctx.render_frame()
+    return ctx
+
+
+def _compare_stages(ctx, fr, sv):
+    order = ctx.debug_order()
+    assert np.array_equal(order, fr.order), "depth order"
+    proj = ctx.debug_projected()
+    assert proj.shape[0] == sv.n
+    vis = (fr.proj["flags"] & 1) != 0
+    assert np.array_equal(proj["flags"], fr.proj["flags"])
+    assert np.array_equal(proj["depth"][vis].view(np.uint32), fr.proj["depth"][vis].view(np.uint32))
+    drawn = (fr.proj["flags"] & 2) != 0
+    for f in ("center_ndc", "axis_u", "axis_v", "color", "extent_scale"):
+        a = proj[f][drawn].view(np.uint32)
+        b = fr.proj[f][drawn].view(np.uint32)
+        assert np.array_equal(a, b), f
+    for f in ("tile_x0", "tile_y0", "tile_x1", "tile_y1"):
+        assert np.array_equal(proj[f][drawn], fr.proj[f][drawn]), f
+    tiles, ids = ctx.debug_tile_pairs()
+    assert np.array_equal(tiles, fr.pair_tiles) and np.array_equal(ids, fr.pair_ids), "pairs"
+    ranges, sorted_ids = ctx.debug_tile_ranges(fr.num_tiles)
+    assert np.array_equal(ranges, fr.ranges), "ranges"
+    assert np.array_equal(sorted_ids, fr.tile_ids), "tile lists"
+    counts = ctx.frame_counts()
+    assert counts.visible == fr.visible and counts.drawn == fr.drawn
+    assert counts.tile_keys == len(fr.pair_tiles)
+
+
+def _image_metrics(img, ref8, ref64):
+    d8 = np.abs(img.astype(np.int32) - ref8.astype(np.int32))
+    d64 = np.abs(img.astype(np.int32) - ref64.astype(np.int32))
+    rgb = d8[..., :3] / 255.0
+    return {"mean_abs_rgb_vs_unorm8": float(rgb.mean()),
+            "frac_over_3_255_vs_unorm8": float((rgb > 3.0 / 255.0).any(axis=-1).mean()),
+            "max_vs_unorm8": int(d8.max()), "max_vs_f64": int(d64.max()),
+            "mean_vs_f64": float(d64.mean() / 255.0)}
+
+
+@pytest.mark.parametrize("cfg", ["config1", "config2_small"])
+def test_frame_parity_stages_and_images(oracle, cfg):
+    if cfg == "config1":
+        scene, cam, w, h = gsplat_scenes.config1(seed=0)
+    else:
+        scene, cam, w, h = gsplat_scenes.config2(seed=11, n=40000)
+        w, h = 960, 540
+    sv = oracle.SceneView(scene)
+    fr = oracle.Frame(sv, cam, w, h)
+    ctx = _render(scene, cam, w, h, blend=0)
+    _compare_stages(ctx, fr, sv)
+    img32 = ctx.readback_rgba8()
+    assert np.array_equal(img32, fr.raster_tiles_fp32()), "fp32 image vs restatement"
+    ref8 = fr.raster_unorm8()
+    ref64, _ = fr.raster_f64()
+    m = _image_metrics(img32, ref8, ref64)
+    print(cfg, m)
+    assert m["mean_abs_rgb_vs_unorm8"] <= 1.0 / 255.0
+    assert m["frac_over_3_255_vs_unorm8"] <= 0.001
+    assert m["max_vs_f64"] <= 2
+    ctx.set_blend_mode(1)
+    ctx.render_frame()
+    img8 = ctx.readback_rgba8()
+    assert np.array_equal(img8, ref8), "unorm8 parity image vs reference model"
+    ctx.close()
+
+
+def test_full_config2_parity(oracle):
+    """279,199 splats, SH3, 1920x1080: every stage bit-exact at full size."""
+    scene, cam, w, h = gsplat_scenes.config2()
+    sv = oracle.SceneView(scene)
+    fr = oracle.Frame(sv, cam, w, h)
+    ctx = _render(scene, cam, w, h)
+    _compare_stages(ctx, fr, sv)
+    img = ctx.readback_rgba8()
+    assert np.array_equal(img, fr.raster_tiles_fp32())
+    ref8 = fr.raster_unorm8()
+    ref64, _ = fr.raster_f64()
+    m = _image_metrics(img, ref8, ref64)
+    print("config2", m, "visible", fr.visible, "pairs", len(fr.pair_tiles))
+    assert m["mean_abs_rgb_vs_unorm8"] <= 1.0 / 255.0
+    assert m["frac_over_3_255_vs_unorm8"] <= 0.001
+    assert m["max_vs_f64"] <= 2
+    st = ctx.stats()
+    assert st.visible_count == fr.visible and st.drawn_count == fr.visible
+    ctx.close()
+
+
+def test_conformance_minimal_ascii(kats):
+    k = kats["conformance"]
+    w, h = k["size"]
+    for blend in (0, 1):
+        ctx = _ctx(w, h)
+        ctx.set_blend_mode(blend)
+        ctx.load_scene_path(os.path.join(GOLDEN, "minimal_ascii.ply"))
+        ctx.set_camera(ffi.lib().gsplat_camera_default())
+        ctx.render_frame()
+        st = ctx.stats()
+        assert st.visible_count == k["visible"] and st.drawn_count == k["drawn"]
+        assert st.frame_ms >= 0
+        img = ctx.readback_rgba8()
+        assert (img[..., 3] > 0).any()
+        means = img.reshape(-1, 4).astype(np.float64).sum(0) / (w * h * 255.0)
+        for c in range(4):
+            assert abs(means[c] - k["channel_means"][c]) <= k["tolerance"], (blend, means)
+        ctx.close()
+
+
+def test_back_to_front_order_kat(kats):
+    k = kats["back_to_front"]
+    n = len(k["positions"])
+    scene = {"positions": np.array(k["positions"], np.float32), "opacity": np.ones(n, np.float32),
+             "scale_xyz": np.zeros((n, 3), np.float32),
+             "rotation_xyzw": np.tile(np.float32([0, 0, 0, 1]), (n, 1)),
+             "color_dc": np.tile(np.float32([0.2, 0.3, 0.4]), (n, 1)), "sh_degree": 0,
+             "sh_rest": None}
+    ctx = _render(scene, gsplat_scenes.default_camera(), 1280, 720)
+    assert ctx.debug_order().tolist() == k["order"]
+    assert ctx.stats().visible_count == k["visible"]
+
+
+def test_sort_kats_and_lcg(kats, oracle):
+    k = kats["sort_values_immutable"]
+    assert ffi.sort_values_by_keys(k["keys"], k["values"]).tolist() == k["values_out"]
+    for name in ("sort_pairs_small", "sort_gpu_small"):
+        k = kats[name]
+        keys, values = ffi.sort_pairs(k["keys"], k["values"])
+        assert keys.tolist() == k["keys_out"] and values.tolist() == k["values_out"]
+    k = kats["sort_lcg"]
+    for n, seed in [(k["large_len"], k["large_seed"])] + [(m, k["edge_seed_base"] + m)
+                                                          for m in k["edge_lengths"]]:
+        keys = np.array(lcg_seq(seed, n), np.uint32)
+        vals = np.arange(n, dtype=np.uint32)
+        assert np.array_equal(ffi.sort_values_by_keys(keys, vals),
+                              oracle.sort_values_by_keys(keys, vals)), n
+        gk, gv = ffi.sort_pairs(keys, vals)
+        ok_, ov = oracle.sort_pairs(keys, vals)
+        assert np.array_equal(gk, ok_) and np.array_equal(gv, ov), n
+
+
+def test_sort_gpu_radix_cases(kats, oracle):
+    k = kats["gpu_radix_cases"]
+    for count in k["counts"]:
+        idx = np.arange(count, dtype=np.uint64)
+        keys = ((idx * np.uint64(k["hash_multiplier"])) & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+        keys &= np.uint32(k["key_mask"])
+        keys[idx % 11 == 0] = 0
+        keys[idx % 11 == 1] = 0xFFFFFFFF
+        ids = (count - idx).astype(np.uint32)
+        assert np.array_equal(ffi.sort_values_by_keys(keys, ids),
+                              oracle.sort_values_by_keys(keys, ids)), count
+    eq = k["equal_keys"]
+    ids = np.arange(eq["count"], dtype=np.uint32)
+    assert np.array_equal(ffi.sort_values_by_keys(np.full(eq["count"], eq["key"], np.uint32), ids), ids)
+
+
+@pytest.mark.parametrize("n", [3_000_000, 5_000_001])
+def test_sort_large_with_ties(oracle, n):
+    rng = np.random.default_rng(n)
+    keys = rng.integers(0, 1 << 20, n, dtype=np.uint32)  # heavy ties, top byte constant
+    vals = rng.permutation(n).astype(np.uint32)
+    assert np.array_equal(ffi.sort_values_by_keys(keys, vals), oracle.sort_values_by_keys(keys, vals))
+
+
+def test_tile_size_does_not_change_the_image(oracle):
+    scene, cam, w, h = gsplat_scenes.config1(seed=3)
+    a = _render(scene, cam, w, h, tile=16).readback_rgba8()
+    b = _render(scene, cam, w, h, tile=8).readback_rgba8()
+    assert np.array_equal(a, b)
+    sv = oracle.SceneView(scene)
+    fr = oracle.Frame(sv, cam, w, h, tile=8)
+    ctx = _render(scene, cam, w, h, tile=8)
+    _compare_stages(ctx, fr, sv)
+
+
+@pytest.mark.parametrize("degree", [1, 2, 4])
+def test_sh_degrees(oracle, degree):
+    rng = np.random.default_rng(degree)
+    n = 5000
+    scene = gsplat_scenes.make_scene(rng, gsplat_scenes.gmm_means(rng, n), -4.0, 0.6, 0.5, 1.5,
+                                     degree)
+    cam = gsplat_scenes.camera((2.5, 0.8, -3.0), (0, 0, 0), 55.0)
+    sv = oracle.SceneView(scene)
+    fr = oracle.Frame(sv, cam, 400, 300)
+    ctx = _render(scene, cam, 400, 300)
+    _compare_stages(ctx, fr, sv)
+    assert np.array_equal(ctx.readback_rgba8(), fr.raster_tiles_fp32())
+
+
+def test_edge_cases(oracle):
+    empty = {"positions": np.zeros((0, 3), np.float32), "opacity": np.zeros(0, np.float32),
+             "scale_xyz": np.zeros((0, 3), np.float32), "rotation_xyzw": np.zeros((0, 4), np.float32),
+             "color_dc": np.zeros((0, 3), np.float32), "sh_degree": 0, "sh_rest": None}
+    ctx = _render(empty, gsplat_scenes.default_camera(), 64, 48)
+    assert ctx.stats().visible_count == 0
+    assert not ctx.readback_rgba8().any()
+    assert ctx.debug_order().size == 0
+    # everything behind the camera
+    scene, cam, w, h = gsplat_scenes.config1(seed=1)
+    back = dict(cam, rotation_xyzw=gsplat_scenes.look_at(cam["position"], (0, 0, -20)))
+    ctx = _render(scene, back, w, h)
+    fr = oracle.Frame(oracle.SceneView(scene), back, w, h)
+    assert ctx.stats().visible_count == fr.visible
+    assert np.array_equal(ctx.readback_rgba8(), fr.raster_tiles_fp32())
+    # odd image sizes (partial edge tiles)
+    for (w2, h2) in ((1, 1), (17, 33), (255, 1)):
+        ctx = _render(scene, cam, w2, h2)
+        fr = oracle.Frame(oracle.SceneView(scene), cam, w2, h2)
+        assert np.array_equal(ctx.readback_rgba8(), fr.raster_tiles_fp32()), (w2, h2)
+
+
+def test_large_splats_grow_pair_buffers(oracle):
+    """Large splats near the camera overflow the initial pair capacity; the
+    frame is re-run with larger buffers and stays exact."""
+    rng = np.random.default_rng(9)
+    n = 3000
+    means = rng.uniform(-2, 2, (n, 3)).astype(np.float32)
+    scene = gsplat_scenes.make_scene(rng, means, -0.5, 0.3, 2.0, 0.5, 0)
+    cam = gsplat_scenes.camera((0.0, 0.0, -3.0), (0, 0, 0), 70.0)
+    sv = oracle.SceneView(scene)
+    fr = oracle.Frame(sv, cam, 640, 480, tile=8)
+    ctx = _render(scene, cam, 640, 480, tile=8)
+    counts = ctx.frame_counts()
+    assert counts.tile_keys == len(fr.pair_tiles) > 16 * n
+    assert counts.frame_reruns >= 1
+    _compare_stages(ctx, fr, sv)
+    assert np.array_equal(ctx.readback_rgba8(), fr.raster_tiles_fp32())
+
+
+def test_repeat_frames_are_identical_and_camera_errors():
+    scene, cam, w, h = gsplat_scenes.config1(seed=4)
+    ctx = _render(scene, cam, w, h, debug=False)
+    a = ctx.readback_rgba8().copy()
+    ctx.render_frame()
+    assert np.array_equal(a, ctx.readback_rgba8())
+    bad = dict(cam, near_plane=10.0, far_plane=1.0)
+    with pytest.raises(ffi.GsplatError) as e:
+        ctx.set_camera(bad)
+    assert e.value.code == ffi.INVALID_ARGUMENT
+    ctx2 = _ctx(32, 32)
+    with pytest.raises(ffi.GsplatError) as e:
+        ctx2.render_frame()
+    assert e.value.code == ffi.SCENE_NOT_LOADED
+    with pytest.raises(ffi.GsplatError) as e:
+        ctx2.set_auto_camera()
+    assert e.value.code == ffi.SCENE_NOT_LOADED
+    ctx2.load_scene(scene)
+    ctx2.set_auto_camera()
+    ctx2.render_frame()
+    assert ctx2.stats().visible_count > 0
+    ctx2.set_size(48, 40)
+    ctx2.render_frame()
+    assert ctx2.readback_rgba8().shape == (40, 48, 4)
+
+
+def test_c_smoke_programs_run():
+    exe = os.path.join(ROOT, "tests", "ffi", "_build_smoke")
+    subprocess.run(["gcc", "-O2", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "ffi", "ffi_smoke_cuda.c"), "-o", exe,
+                    "-L", os.path.dirname(ffi.LIB_PATH), "-lgsplat_ffi_c",
+                    "-Wl,-rpath," + os.path.dirname(ffi.LIB_PATH)], check=True)
+    try:
+        r = subprocess.run([exe], cwd=ROOT, capture_output=True, text=True)
+        assert r.returncode == 0, r.stdout + r.stderr
+        assert "ffi smoke ok" in r.stdout
+    finally:
+        os.remove(exe)
+    ref = os.path.join(ROOT, "oracle", "_ref", "ffi_smoke")
+    if os.path.exists(ref):
+        r = subprocess.run([ref, os.path.join(GOLDEN, "minimal_ascii.ply")], cwd=ROOT,
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stdout + r.stderr
+        assert "ffi smoke ok" in r.stdout
