@@ -315,6 +315,15 @@ static void cpu_sh_color(const OrcScene &sc, uint64_t i, const float dir[3], flo
   for (int ch = 0; ch < 3; ++ch) rgb[ch] = std::fmax(rgb[ch] + 0.5f, 0.0f);
 }
 
+// Exact f32 quotients d / 255 for d in 0..255 (the same correctly rounded
+// values a division produces).
+static float g_inv255[256];
+static bool init_inv255() {
+  for (int d = 0; d < 256; ++d) g_inv255[d] = (float)d / 255.0f;
+  return true;
+}
+static const bool g_inv255_ready = init_inv255();
+
 static void parallel_rows(uint32_t height, int threads,
                           const std::function<void(uint32_t, uint32_t)> &fn) {
   if (threads <= 1 || height < 2) {
@@ -342,6 +351,59 @@ static inline void quad_pixel_bbox(const OrcProjected &p, const OrcRecord &r, ui
   x1 = (int)std::min((double)w - 1, std::ceil(r.cx + rx));
   y0 = (int)std::max(0.0, std::floor(r.cy - ry));
   y1 = (int)std::min((double)h - 1, std::ceil(r.cy + ry));
+}
+
+// Band workers of the compositors. target_clones builds an FMA version
+// (explicit fmaf becomes one instruction) and a portable one, picked at load
+// time; both compute identical values.
+__attribute__((target_clones("fma", "default"))) static void unorm8_band(
+    const OrcRecord *records, const OrcProjected *proj, const uint32_t *order, uint64_t v,
+    uint32_t width, uint32_t height, uint8_t *rgba, uint32_t ya, uint32_t yb) {
+  for (uint64_t j = 0; j < v; ++j) {
+    uint32_t s = order[j];
+    const OrcProjected &p = proj[s];
+    if (!(p.flags & 2u)) continue;
+    const OrcRecord &r = records[s];
+    int x0, x1, y0, y1;
+    quad_pixel_bbox(p, r, width, height, x0, x1, y0, y1);
+    y0 = std::max<int>(y0, (int)ya);
+    y1 = std::min<int>(y1, (int)yb - 1);
+    for (int py = y0; py <= y1; ++py)
+      for (int px = x0; px <= x1; ++px) {
+        float g, w;
+        if (!pixel_weight(r, px, py, g, w)) continue;
+        uint8_t *d = &rgba[((size_t)py * width + px) * 4];
+        float one_minus = 1.0f - w;
+        float src[3] = {r.pr * g, r.pg * g, r.pb * g};
+        for (int ch = 0; ch < 3; ++ch) d[ch] = to_unorm8(std::fma(g_inv255[d[ch]], one_minus, src[ch]));
+        d[3] = to_unorm8(std::fma(g_inv255[d[3]], one_minus, w));
+      }
+  }
+}
+
+__attribute__((target_clones("fma", "default"))) static void tiles_fp32_band(
+    const OrcRecord *records, const uint32_t *ranges, const uint32_t *sorted_ids, uint32_t width,
+    uint32_t tile, uint32_t tiles_x, uint8_t *rgba, uint32_t ya, uint32_t yb) {
+  for (uint32_t py = ya; py < yb; ++py)
+    for (uint32_t px = 0; px < width; ++px) {
+      uint32_t t = (py / tile) * tiles_x + (px / tile);
+      uint32_t start = ranges[2 * t], end = ranges[2 * t + 1];
+      float T = 1.0f, c[3] = {0.0f, 0.0f, 0.0f};
+      for (uint32_t k = end; k > start; --k) {
+        const OrcRecord &r = records[sorted_ids[k - 1]];
+        float g, w;
+        if (!pixel_weight(r, (int)px, (int)py, g, w)) continue;
+        float tn = T * (1.0f - w);
+        c[0] = std::fma(r.pr * g, T, c[0]);
+        c[1] = std::fma(r.pg * g, T, c[1]);
+        c[2] = std::fma(r.pb * g, T, c[2]);
+        T = tn;
+        if (T < 1e-4f) break;
+      }
+      uint8_t *d = &rgba[((size_t)py * width + px) * 4];
+      d[0] = to_unorm8(c[0]); d[1] = to_unorm8(c[1]); d[2] = to_unorm8(c[2]);
+      d[3] = to_unorm8(1.0f - T);
+    }
 }
 
 }  // namespace orc
@@ -489,30 +551,7 @@ void orc_raster_unorm8(const OrcRecord *records, const OrcProjected *proj,
                        uint8_t *rgba, int32_t threads) {
   std::memset(rgba, 0, (size_t)width * height * 4);
   parallel_rows(height, threads, [&](uint32_t ya, uint32_t yb) {
-    for (uint64_t j = 0; j < v; ++j) {
-      uint32_t s = order[j];
-      const OrcProjected &p = proj[s];
-      if (!(p.flags & 2u)) continue;
-      const OrcRecord &r = records[s];
-      int x0, x1, y0, y1;
-      quad_pixel_bbox(p, r, width, height, x0, x1, y0, y1);
-      y0 = std::max<int>(y0, (int)ya);
-      y1 = std::min<int>(y1, (int)yb - 1);
-      for (int py = y0; py <= y1; ++py)
-        for (int px = x0; px <= x1; ++px) {
-          float g, w;
-          if (!pixel_weight(r, px, py, g, w)) continue;
-          uint8_t *d = &rgba[((size_t)py * width + px) * 4];
-          float one_minus = 1.0f - w;
-          float src[3] = {r.pr * g, r.pg * g, r.pb * g};
-          for (int ch = 0; ch < 3; ++ch) {
-            float dst = (float)d[ch] / 255.0f;
-            d[ch] = to_unorm8(std::fma(dst, one_minus, src[ch]));
-          }
-          float dst_a = (float)d[3] / 255.0f;
-          d[3] = to_unorm8(std::fma(dst_a, one_minus, w));
-        }
-    }
+    unorm8_band(records, proj, order, v, width, height, rgba, ya, yb);
   });
 }
 
@@ -568,26 +607,7 @@ void orc_raster_tiles_fp32(const OrcRecord *records, const uint32_t *ranges,
                            const uint32_t *sorted_ids, uint32_t width, uint32_t height,
                            uint32_t tile, uint32_t tiles_x, uint8_t *rgba, int32_t threads) {
   parallel_rows(height, threads, [&](uint32_t ya, uint32_t yb) {
-    for (uint32_t py = ya; py < yb; ++py)
-      for (uint32_t px = 0; px < width; ++px) {
-        uint32_t t = (py / tile) * tiles_x + (px / tile);
-        uint32_t start = ranges[2 * t], end = ranges[2 * t + 1];
-        float T = 1.0f, c[3] = {0.0f, 0.0f, 0.0f};
-        for (uint32_t k = end; k > start; --k) {
-          const OrcRecord &r = records[sorted_ids[k - 1]];
-          float g, w;
-          if (!pixel_weight(r, (int)px, (int)py, g, w)) continue;
-          float tn = T * (1.0f - w);
-          c[0] = std::fma(r.pr * g, T, c[0]);
-          c[1] = std::fma(r.pg * g, T, c[1]);
-          c[2] = std::fma(r.pb * g, T, c[2]);
-          T = tn;
-          if (T < 1e-4f) break;
-        }
-        uint8_t *d = &rgba[((size_t)py * width + px) * 4];
-        d[0] = to_unorm8(c[0]); d[1] = to_unorm8(c[1]); d[2] = to_unorm8(c[2]);
-        d[3] = to_unorm8(1.0f - T);
-      }
+    tiles_fp32_band(records, ranges, sorted_ids, width, tile, tiles_x, rgba, ya, yb);
   });
 }
 
