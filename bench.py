@@ -50,49 +50,72 @@ def dist_setup():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons, sampled every 100 ms from before
+    the warm-up until after the timed region; stop() keeps the samples whose
+    timestamps fall inside the timed window (widened by one sampling period),
+    or the nearest ones when the window is shorter than a period."""
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    QUERY = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
+        self.window = None
         self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.out,
                 stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
 
+    def mark(self, t0, t1):
+        self.window = (t0, t1)
+
     def stop(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.3)
         self.proc.terminate()
         self.proc.wait()
         self.out.flush()
         with open(self.out.name) as f:
-            rows = [r.split(",") for r in f.read().strip().splitlines() if r.strip()]
+            lines = [r for r in f.read().strip().splitlines() if r.strip()]
         os.unlink(self.out.name)
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            r = [x.strip() for x in r]
+        import datetime
+
+        samples = []
+        for line in lines:
+            r = [x.strip() for x in line.split(",")]
             try:
-                sm.append(float(r[1]))
-                smax = float(r[2])
+                ts = datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                samples.append((ts, float(r[2]), float(r[3]), r[6:10]))
             except (ValueError, IndexError):
                 continue
-            for k, name in enumerate(names):
-                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+        if not samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sel, how = samples, "whole run"
+        if self.window:
+            t0, t1 = self.window
+            sel = [x for x in samples if t0 - 0.1 <= x[0] <= t1 + 0.1]
+            how = "timed window"
+            if not sel:
+                mid = 0.5 * (t0 + t1)
+                sel = sorted(samples, key=lambda x: abs(x[0] - mid))[:3]
+                how = "nearest to the timed window"
+        reasons = set()
+        for x in sel:
+            for k, name in enumerate(self.REASONS):
+                if k < len(x[3]) and x[3][k].lower().startswith("active"):
                     reasons.add(name)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": float(np.median([x[1] for x in sel])), "sm_max_mhz": sel[0][2],
+                "reasons": sorted(reasons), "samples": len(sel), "selection": how}
 
 
 def algorithmic_bytes(phase, counts, n, planes, width, height, tile_passes):
@@ -138,7 +161,10 @@ def cpu_baseline(scene, cam, w, h, budget_s=15.0, steps=None):
                       f"raster {ph[3]:.1f})"}
 
 
-def run_reference(args, world, rank):
+def run_reference(args, world, rank, budget_s=150.0):
+    """Reference arm on rank 0: the CPU restatement of the reference frame.
+    Each step is one frame; when K full frames would exceed the time budget,
+    each step rasterises a band of rows and the frame time is scaled from it."""
     if rank != 0:
         return
     scene, cam, w, h = gsplat_scenes.config2()
@@ -146,21 +172,30 @@ def run_reference(args, world, rank):
 
     sv = oracle_py.SceneView(scene)
     threads = os.cpu_count() or 1
+    _, t = oracle_py.render_reference_frame(sv, cam, w, h, threads)
+    frac = min(1.0, budget_s / max(1e-9, (args.steps + args.warmup) * t.total_ms / 1000.0))
+    rows = max(1, int(h * frac))
     for _ in range(args.warmup):
-        oracle_py.render_reference_frame(sv, cam, w, h, threads)
+        oracle_py.render_reference_frame(sv, cam, w, h, threads, rows=rows)
+    frame_ms = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        oracle_py.render_reference_frame(sv, cam, w, h, threads)
+        _, t = oracle_py.render_reference_frame(sv, cam, w, h, threads, rows=rows)
+        frame_ms.append(t.preprocess_ms + t.sort_ms + t.project_ms + t.raster_ms * h / rows)
     el = time.perf_counter() - t0
-    value = args.steps / el
+    value = 1000.0 * len(frame_ms) / sum(frame_ms)
+    sample = ("one frame per step: the reference SortedAlpha path restated in C++ (oracle/): "
+              f"depth preprocess and radix sort on 1 thread, vertex stage and UNORM8 blend on "
+              f"{threads} threads")
+    if rows < h:
+        sample += f"; raster of rows 0-{rows} per step, frame time scaled by {h}/{rows}"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "frames/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "parallelism": "host threads"},
             "cpu_baseline": {"value": value, "unit": "frames/s", "cores": threads, "kind": "port",
-                             "sample": "one full frame per step: the reference SortedAlpha path "
-                                       "restated in C++ (oracle/), host CPU"},
+                             "sample": sample},
             "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -180,6 +215,8 @@ def run_cuda(args, world, rank, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     scene, cam, w, h = gsplat_scenes.config2()
+    clocks = ClockSampler(local)
+    clocks.start()
     ctx = ffi.Context(w, h)
     ctx.load_scene(scene)
     ctx.set_camera(cam)
@@ -199,13 +236,12 @@ def run_cuda(args, world, rank, local):
             phase_acc[k] = phase_acc.get(k, 0.0) + v
     phases = {k: v / args.steps for k, v in phase_acc.items()}
 
-    clocks = ClockSampler(local)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    clocks.start()
+    t_begin = time.time()
     for i in range(args.steps):
         with torch.cuda.stream(stream):
             flush.fill_(i + 1)
@@ -215,7 +251,7 @@ def run_cuda(args, world, rank, local):
             ends[i].record(stream)
     ctx.sync()
     torch.cuda.synchronize()
-    clk = clocks.stop()
+    clocks.mark(t_begin, time.time())
     device_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     if world > 1:
         t = torch.tensor([device_ms], device="cuda", dtype=torch.float64)
@@ -246,6 +282,7 @@ def run_cuda(args, world, rank, local):
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
+    clk = clocks.stop()
     e2e = {"value": world * args.steps / e2e_s, "unit": "frames/s",
            "h2d_bytes_per_step": 40, "d2h_bytes_per_step": w * h * 4 + 64}
 
@@ -293,7 +330,7 @@ def run_cuda(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
     ap.add_argument("--cpu-budget", type=float, default=15.0)

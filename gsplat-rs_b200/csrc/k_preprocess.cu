@@ -7,11 +7,12 @@
 // One thread per splat:
 //   1. depth = row2 . (p - cam); visible iff near <= depth <= far
 //      (preprocess_visible_into, crates/gsplat-render-wgpu/src/lib.rs:1263-1296);
-//   2. visible splats are compacted in id order with a block scan and a
+//   2. project_splat + eval_color (splat_surface_direct.wgsl:131-217, 233-334),
+//      tile rect of the ellipse |local| <= s and the pixel-space record;
+//   3. digit histograms of the depth keys for the radix sort;
+//   4. visible splats are compacted in id order with a block scan and a
 //      decoupled look-back, emitting (~bits(max(depth, 0)), id) so that an
-//      ascending stable sort yields the reference's descending-depth order;
-//   3. project_splat + eval_color (splat_surface_direct.wgsl:131-217, 233-334);
-//   4. tile rect of the ellipse |local| <= s and the pixel-space record.
+//      ascending stable sort yields the reference's descending-depth order.
 
 #include "device_common.cuh"
 #include "kernels.h"
@@ -257,12 +258,14 @@ template <int kPlanes, bool kDebug>
 __global__ void __launch_bounds__(kK1Threads) preprocess_kernel(
     SceneDev sc, FrameParams p, uint32_t *__restrict__ vis_keys, uint32_t *__restrict__ vis_ids,
     uint2 *__restrict__ rects, Record *__restrict__ records, unsigned long long *status,
-    FrameCounters *counters, ProjectedDev *__restrict__ dbg_out) {
+    FrameCounters *counters, uint32_t *__restrict__ key_hist, ProjectedDev *__restrict__ dbg_out) {
   __shared__ uint32_t s_block;
   __shared__ uint32_t s_warp[kK1Threads / 32];
   __shared__ uint32_t s_prefix;
+  __shared__ uint32_t s_hist[4][256];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) s_block = atomicAdd(&counters->k1_ticket, 1u);
+  for (uint32_t k = threadIdx.x; k < 4 * 256; k += kK1Threads) (&s_hist[0][0])[k] = 0;
   __syncthreads();
   const uint32_t block = s_block;
   const uint32_t i = block * kK1Threads + threadIdx.x;
@@ -273,11 +276,41 @@ __global__ void __launch_bounds__(kK1Threads) preprocess_kernel(
   float depth = p.r2[0] * rel[0] + p.r2[1] * rel[1] + p.r2[2] * rel[2];
   const bool vis = valid && depth >= p.near_plane && depth <= p.far_plane;
 
-  // Block-wide compaction of the visible flags, warp ballots first.
+  // The vertex stage first (it does not depend on the compaction), so that
+  // the look-back below waits on predecessors that have long published.
+  ProjectedDev *dbg = nullptr;
+  if (kDebug && valid) {
+    dbg = &dbg_out[i];
+    ProjectedDev z = {};
+    z.depth = depth;
+    z.flags = vis ? 1u : 0u;
+    *dbg = z;
+  }
+  const uint32_t key = ~__float_as_uint(fmaxf(depth, 0.0f));
+  if (vis) {
+    Record rec;
+    uint2 rect = make_uint2(0u, 0u);
+    bool drawn = project<kPlanes>(sc, p, i, pa, rel, depth, rec, rect, dbg);
+    rects[i] = rect;
+    if (drawn) {
+      records[i] = rec;
+      uint32_t dmask = __ballot_sync(__activemask(), true);
+      if (lane == __ffs(dmask) - 1) atomicAdd(&counters->drawn, __popc(dmask));
+    }
+    // Digit histograms of the depth keys for every radix pass.
+#pragma unroll
+    for (int d = 0; d < 4; ++d) atomicAdd(&s_hist[d][(key >> (8 * d)) & 255u], 1u);
+  }
+
+  // Block-wide compaction of the visible flags, then the global offset.
   const uint32_t ballot = __ballot_sync(0xffffffffu, vis);
   const uint32_t rank = __popc(ballot & lanemask_lt());
   if (lane == 0) s_warp[warp] = __popc(ballot);
   __syncthreads();
+  for (uint32_t k = threadIdx.x; k < 4 * 256; k += kK1Threads) {
+    uint32_t c = (&s_hist[0][0])[k];
+    if (c) atomicAdd(&key_hist[k], c);
+  }
   uint32_t warp_prefix = 0, block_total = 0;
 #pragma unroll
   for (int w = 0; w < kK1Threads / 32; ++w) {
@@ -292,29 +325,10 @@ __global__ void __launch_bounds__(kK1Threads) preprocess_kernel(
   __syncthreads();
   const uint32_t prefix = s_prefix;
   if (threadIdx.x == 0 && block == (sc.n - 1) / kK1Threads) counters->visible = prefix + block_total;
-
-  ProjectedDev *dbg = nullptr;
-  if (kDebug && valid) {
-    dbg = &dbg_out[i];
-    ProjectedDev z = {};
-    z.depth = depth;
-    z.flags = vis ? 1u : 0u;
-    *dbg = z;
-  }
   if (!vis) return;
   const uint32_t slot = prefix + warp_prefix + rank;
-  vis_keys[slot] = ~__float_as_uint(fmaxf(depth, 0.0f));
+  vis_keys[slot] = key;
   vis_ids[slot] = i;
-
-  Record rec;
-  uint2 rect = make_uint2(0u, 0u);
-  bool drawn = project<kPlanes>(sc, p, i, pa, rel, depth, rec, rect, dbg);
-  rects[i] = rect;
-  if (drawn) {
-    records[i] = rec;
-    uint32_t dmask = __ballot_sync(__activemask(), true);
-    if (lane == __ffs(dmask) - 1) atomicAdd(&counters->drawn, __popc(dmask));
-  }
 }
 
 template <int kPlanes>
@@ -324,10 +338,12 @@ void launch_k1(const SceneDev &sc, const FrameParams &p, const K1Buffers &b, boo
   if (blocks == 0) return;
   if (debug)
     preprocess_kernel<kPlanes, true><<<blocks, kK1Threads, 0, stream>>>(
-        sc, p, b.vis_keys, b.vis_ids, b.rects, b.records, b.status, b.counters, b.projected);
+        sc, p, b.vis_keys, b.vis_ids, b.rects, b.records, b.status, b.counters, b.key_hist,
+        b.projected);
   else
     preprocess_kernel<kPlanes, false><<<blocks, kK1Threads, 0, stream>>>(
-        sc, p, b.vis_keys, b.vis_ids, b.rects, b.records, b.status, b.counters, nullptr);
+        sc, p, b.vis_keys, b.vis_ids, b.rects, b.records, b.status, b.counters, b.key_hist,
+        nullptr);
 }
 
 }  // namespace

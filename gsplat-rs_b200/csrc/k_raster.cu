@@ -12,9 +12,11 @@
 // local = inverse axis matrix * (pixel - centre); discard unless
 // |local.x|, |local.y| <= s (the quad), r^2 = |local|^2 <= 1, and
 // w = alpha * exp(-4.5 r^2) > 1/256; the source is (premult rgb * g, w).
-//   FP32 mode: front to back (walks the list from its end); C += src * T,
-//     T *= 1 - w; a pixel finishes once T < 1e-4, a warp leaves the chunk
-//     when all its pixels have, the block stops loading once all are done.
+//   FP32 mode: front to back (walks the list from its end); coverage is
+//     r^2 <= s^2 and w > 1/256 (in exact arithmetic the same set as the quad
+//     clip, r^2 <= 1 and the alpha threshold); C += premult * (g T),
+//     T *= 1 - w; a pixel finishes once T < 1e-4, a warp when all its pixels
+//     have, the block stops loading once all are done.
 //   UNORM8 mode: back to front, dst = src + dst * (1 - w) rounded to UNORM8
 //     after every splat (the reference's Rgba8Unorm premultiplied blend).
 
@@ -32,15 +34,15 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-template <int kTile, bool kUnorm8>
-__global__ void __launch_bounds__(kTile *kTile) raster_kernel(
+// UNORM8 parity mode: back to front over the tile list, the reference
+// fragment rule with the quad clip, rounding to UNORM8 after every blend.
+template <int kTile>
+__global__ void __launch_bounds__(kTile *kTile) raster_unorm8_kernel(
     FrameParams p, const uint2 *__restrict__ ranges, const SortPlan *__restrict__ plan,
     const uint32_t *__restrict__ ids0, const uint32_t *__restrict__ ids1,
     const Record *__restrict__ records, uint32_t *__restrict__ image,
     const FrameCounters *__restrict__ counters, uint32_t *sticky) {
   constexpr int kN = kTile * kTile;
-  // The raster is the last kernel of a frame: fold the frame's error and
-  // overflow flags into the word a deferred sync reads.
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     uint32_t bits = counters->error | (counters->overflow ? 0x80000000u : 0u);
     if (bits) atomicOr(sticky, bits);
@@ -48,7 +50,6 @@ __global__ void __launch_bounds__(kTile *kTile) raster_kernel(
   __shared__ float4 s_a[2][kN];
   __shared__ float4 s_b[2][kN];
   __shared__ float4 s_c[2][kN];
-
   const uint32_t tile = blockIdx.x;
   const uint32_t tx = tile % p.tiles_x, ty = tile / p.tiles_x;
   const uint32_t tid = threadIdx.x;
@@ -60,23 +61,17 @@ __global__ void __launch_bounds__(kTile *kTile) raster_kernel(
   const uint2 range = ranges[tile];
   const uint32_t count = range.y - range.x;
   const uint32_t chunks = (count + kN - 1) / kN;
-
-  // Chunk c holds list positions (in processing order) c*kN .. c*kN+kN-1.
   auto issue = [&](uint32_t c, int buf) {
     uint32_t k = c * kN + tid;
     if (k < count) {
-      uint32_t pos = kUnorm8 ? range.x + k : range.y - 1 - k;
-      const Record *r = &records[ids[pos]];
+      const Record *r = &records[ids[range.x + k]];
       cp_async16(&s_a[buf][tid], &r->a);
       cp_async16(&s_b[buf][tid], &r->b);
       cp_async16(&s_c[buf][tid], &r->c);
     }
     cp_async_commit();
   };
-
-  float T = 1.0f, c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
   uint32_t d0 = 0, d1 = 0, d2 = 0, d3 = 0;
-  bool done = !inside;
   if (chunks > 0) issue(0, 0);
   for (uint32_t c = 0; c < chunks; ++c) {
     const int buf = c & 1;
@@ -85,32 +80,9 @@ __global__ void __launch_bounds__(kTile *kTile) raster_kernel(
     cp_async_wait_1();
     __syncthreads();
     const uint32_t n_in = min((uint32_t)kN, count - c * kN);
-    if (kUnorm8) {
-      if (inside) {
-        for (uint32_t j = 0; j < n_in; ++j) {
-          const float4 a = s_a[buf][j], b = s_b[buf][j], col = s_c[buf][j];
-          float dpx = fpx - a.x, dpy = fpy - a.y;
-          float lx = fmaf(a.z, dpx, a.w * dpy);
-          float ly = fmaf(b.x, dpx, b.y * dpy);
-          if (!(fabsf(lx) <= b.z && fabsf(ly) <= b.z)) continue;
-          float r2 = fmaf(lx, lx, ly * ly);
-          if (!(r2 <= 1.0f)) continue;
-          float g = exp_neg(-4.5f * r2);
-          float w = b.w * g;
-          if (!(w > 1.0f / 256.0f)) continue;
-          float om = 1.0f - w;
-          d0 = to_unorm8(fmaf((float)d0 / 255.0f, om, col.x * g));
-          d1 = to_unorm8(fmaf((float)d1 / 255.0f, om, col.y * g));
-          d2 = to_unorm8(fmaf((float)d2 / 255.0f, om, col.z * g));
-          d3 = to_unorm8(fmaf((float)d3 / 255.0f, om, w));
-        }
-      }
-      __syncthreads();
-    } else {
+    if (inside) {
       for (uint32_t j = 0; j < n_in; ++j) {
-        if (__all_sync(0xffffffffu, done)) break;
-        if (done) continue;
-        const float4 a = s_a[buf][j], b = s_b[buf][j];
+        const float4 a = s_a[buf][j], b = s_b[buf][j], col = s_c[buf][j];
         float dpx = fpx - a.x, dpy = fpy - a.y;
         float lx = fmaf(a.z, dpx, a.w * dpy);
         float ly = fmaf(b.x, dpx, b.y * dpy);
@@ -120,27 +92,150 @@ __global__ void __launch_bounds__(kTile *kTile) raster_kernel(
         float g = exp_neg(-4.5f * r2);
         float w = b.w * g;
         if (!(w > 1.0f / 256.0f)) continue;
-        const float4 col = s_c[buf][j];
-        float tn = T * (1.0f - w);
-        c0 = fmaf(col.x * g, T, c0);
-        c1 = fmaf(col.y * g, T, c1);
-        c2 = fmaf(col.z * g, T, c2);
-        T = tn;
-        if (T < 1e-4f) done = true;
+        float om = 1.0f - w;
+        d0 = to_unorm8(fmaf((float)d0 / 255.0f, om, col.x * g));
+        d1 = to_unorm8(fmaf((float)d1 / 255.0f, om, col.y * g));
+        d2 = to_unorm8(fmaf((float)d2 / 255.0f, om, col.z * g));
+        d3 = to_unorm8(fmaf((float)d3 / 255.0f, om, w));
       }
-      if (__syncthreads_count(done) == kN) break;
     }
+    __syncthreads();
   }
   cp_async_wait_all();
-  if (!inside) return;
-  uint32_t out;
-  if (kUnorm8) {
-    out = d0 | (d1 << 8) | (d2 << 16) | (d3 << 24);
-  } else {
-    out = to_unorm8(c0) | (to_unorm8(c1) << 8) | (to_unorm8(c2) << 16) |
-          (to_unorm8(1.0f - T) << 24);
+  if (inside) image[(size_t)py * p.width + px] = d0 | (d1 << 8) | (d2 << 16) | (d3 << 24);
+}
+
+// FP32 front-to-back mode. Threads map to 8x4-pixel warp blocks (lane l of
+// warp w covers column (w % (kTile/8))*8 + (l & 7), row (w / (kTile/8))*4 +
+// (l >> 3)). Per chunk of kN list entries:
+//   1. raw records arrive by cp.async (double-buffered, next chunk in flight);
+//   2. each thread derives, for its entry and this tile, the tile-local
+//      offsets ox, oy (local = (ax*lx + ay*ly + ox, bx*lx + by*ly + oy) for
+//      tile-local pixel coordinates), s^2, and a bit mask of the warp blocks
+//      the splat's ellipse bounding box (plus one pixel) touches;
+//   3. each warp compacts the entries whose mask has its bit (ballots keep the
+//      list order) and blends only those; a pixel stops at T < 1e-4, a warp
+//      when all 32 pixels have, the block when all pixels have.
+// Culling is conservative, so results equal the unculled per-pixel walk.
+template <int kTile>
+__global__ void __launch_bounds__(kTile *kTile) raster_fp32_kernel(
+    FrameParams p, const uint2 *__restrict__ ranges, const SortPlan *__restrict__ plan,
+    const uint32_t *__restrict__ ids0, const uint32_t *__restrict__ ids1,
+    const Record *__restrict__ records, uint32_t *__restrict__ image,
+    const FrameCounters *__restrict__ counters, uint32_t *sticky) {
+  constexpr int kN = kTile * kTile;
+  constexpr int kWarps = kN / 32;
+  constexpr int kBlocksX = kTile / 8;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    uint32_t bits = counters->error | (counters->overflow ? 0x80000000u : 0u);
+    if (bits) atomicOr(sticky, bits);
   }
-  image[(size_t)py * p.width + px] = out;
+  __shared__ float4 s_raw[2][3][kN];
+  __shared__ float4 s_d0[kN];  // ax, ay, ox, s2
+  __shared__ float4 s_d1[kN];  // bx, by, oy, alpha
+  __shared__ float4 s_d2[kN];  // r*alpha, g*alpha, b*alpha, -
+  __shared__ uint8_t s_mask[kN];
+  __shared__ uint16_t s_list[kWarps][kN];
+
+  const uint32_t tile = blockIdx.x;
+  const uint32_t tx = tile % p.tiles_x, ty = tile / p.tiles_x;
+  const uint32_t x0 = tx * kTile, y0 = ty * kTile;
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t bx0 = (warp % kBlocksX) * 8, by0 = (warp / kBlocksX) * 4;
+  const uint32_t lxp = bx0 + (lane & 7), lyp = by0 + (lane >> 3);
+  const uint32_t px = x0 + lxp, py = y0 + lyp;
+  const bool inside = px < p.width && py < p.height;
+  // Local coordinates are taken from the 16-pixel grid corner at or before
+  // the tile, so 8x8 and 16x16 tiles evaluate every pixel identically.
+  const uint32_t ax0 = x0 & ~15u, ay0 = y0 & ~15u;
+  const float fx = (float)(px - ax0), fy = (float)(py - ay0);
+  const float fax = (float)ax0, fay = (float)ay0;
+  const float ftx = (float)x0, fty = (float)y0;
+  const uint32_t *__restrict__ ids = plan->final_buffer == 0 ? ids0 : ids1;
+  const uint2 range = ranges[tile];
+  const uint32_t count = range.y - range.x;
+  const uint32_t chunks = (count + kN - 1) / kN;
+
+  auto issue = [&](uint32_t c, int buf) {
+    uint32_t k = c * kN + tid;
+    if (k < count) {
+      const Record *r = &records[ids[range.y - 1 - k]];
+      cp_async16(&s_raw[buf][0][tid], &r->a);
+      cp_async16(&s_raw[buf][1][tid], &r->b);
+      cp_async16(&s_raw[buf][2][tid], &r->c);
+    }
+    cp_async_commit();
+  };
+
+  float T = 1.0f, c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
+  bool done = !inside;
+  if (chunks > 0) issue(0, 0);
+  for (uint32_t c = 0; c < chunks; ++c) {
+    const int buf = c & 1;
+    if (c + 1 < chunks) issue(c + 1, buf ^ 1);
+    else cp_async_commit();
+    cp_async_wait_1();
+    const uint32_t n_in = min((uint32_t)kN, count - c * kN);
+    if (tid < n_in) {
+      const float4 a = s_raw[buf][0][tid], b = s_raw[buf][1][tid], col = s_raw[buf][2][tid];
+      float cxa = a.x - fax, cya = a.y - fay;
+      float ox = -fmaf(a.z, cxa, a.w * cya);
+      float oy = -fmaf(b.x, cxa, b.y * cya);
+      float cxl = a.x - ftx, cyl = a.y - fty;
+      s_d0[tid] = make_float4(a.z, a.w, ox, b.z * b.z);
+      s_d1[tid] = make_float4(b.x, b.y, oy, b.w);
+      s_d2[tid] = col;
+      // Bounding box of |local| <= s: half extents s*|row of M| / |det M^-1|.
+      float inv_det = 1.0f / fabsf(a.z * b.y - a.w * b.x);
+      float hx = b.z * sqrtf(b.y * b.y + a.w * a.w) * inv_det + 1.0f;
+      float hy = b.z * sqrtf(b.x * b.x + a.z * a.z) * inv_det + 1.0f;
+      uint32_t mask = 0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) {
+        float bxl = (float)((w % kBlocksX) * 8), byl = (float)((w / kBlocksX) * 4);
+        bool hit = cxl + hx >= bxl && cxl - hx <= bxl + 7.0f && cyl + hy >= byl &&
+                   cyl - hy <= byl + 3.0f;
+        mask |= hit ? (1u << w) : 0u;
+      }
+      s_mask[tid] = (uint8_t)mask;
+    }
+    __syncthreads();
+    // Ordered compaction of this warp's entries.
+    uint32_t n_w = 0;
+    for (uint32_t k0 = 0; k0 < n_in; k0 += 32) {
+      uint32_t k = k0 + lane;
+      bool hit = k < n_in && ((s_mask[k] >> warp) & 1u);
+      uint32_t bal = __ballot_sync(0xffffffffu, hit);
+      if (hit) s_list[warp][n_w + __popc(bal & lanemask_lt())] = (uint16_t)k;
+      n_w += __popc(bal);
+    }
+    __syncwarp();
+    for (uint32_t i = 0; i < n_w; ++i) {
+      if (__all_sync(0xffffffffu, done)) break;
+      const uint32_t j = s_list[warp][i];
+      const float4 d0 = s_d0[j];
+      const float4 d1 = s_d1[j];
+      float lx = fmaf(d0.x, fx, fmaf(d0.y, fy, d0.z));
+      float ly = fmaf(d1.x, fx, fmaf(d1.y, fy, d1.z));
+      float r2 = fmaf(lx, lx, ly * ly);
+      if (done || !(r2 <= d0.w)) continue;
+      float g = gauss_weight(r2);
+      float w = d1.w * g;
+      if (!(w > 1.0f / 256.0f)) continue;
+      const float4 col = s_d2[j];
+      float gT = g * T;
+      c0 = fmaf(col.x, gT, c0);
+      c1 = fmaf(col.y, gT, c1);
+      c2 = fmaf(col.z, gT, c2);
+      T = T * (1.0f - w);
+      if (T < 1e-4f) done = true;
+    }
+    if (__syncthreads_count(done) == kN) break;
+  }
+  cp_async_wait_all();
+  if (inside)
+    image[(size_t)py * p.width + px] = to_unorm8(c0) | (to_unorm8(c1) << 8) |
+                                       (to_unorm8(c2) << 16) | (to_unorm8(1.0f - T) << 24);
 }
 
 }  // namespace
@@ -153,14 +248,14 @@ void launch_raster(const FrameParams &p, const uint2 *ranges, const SortPlan *ti
   if (blocks == 0) return;
   if (p.tile == 16) {
     if (blend_mode == 1)
-      raster_kernel<16, true><<<blocks, 256, 0, stream>>>(p, ranges, tile_plan, ids0, ids1, records, image, counters, sticky);
+      raster_unorm8_kernel<16><<<blocks, 256, 0, stream>>>(p, ranges, tile_plan, ids0, ids1, records, image, counters, sticky);
     else
-      raster_kernel<16, false><<<blocks, 256, 0, stream>>>(p, ranges, tile_plan, ids0, ids1, records, image, counters, sticky);
+      raster_fp32_kernel<16><<<blocks, 256, 0, stream>>>(p, ranges, tile_plan, ids0, ids1, records, image, counters, sticky);
   } else {
     if (blend_mode == 1)
-      raster_kernel<8, true><<<blocks, 64, 0, stream>>>(p, ranges, tile_plan, ids0, ids1, records, image, counters, sticky);
+      raster_unorm8_kernel<8><<<blocks, 64, 0, stream>>>(p, ranges, tile_plan, ids0, ids1, records, image, counters, sticky);
     else
-      raster_kernel<8, false><<<blocks, 64, 0, stream>>>(p, ranges, tile_plan, ids0, ids1, records, image, counters, sticky);
+      raster_fp32_kernel<8><<<blocks, 64, 0, stream>>>(p, ranges, tile_plan, ids0, ids1, records, image, counters, sticky);
   }
 }
 

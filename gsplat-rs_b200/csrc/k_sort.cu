@@ -250,11 +250,13 @@ void launch_sort(const SortBuffers &b, cudaStream_t stream) {
   uint32_t *hist = b.work + 64;
   uint32_t *status = b.work + 64 + 4 * 256;
   const uint32_t grid = tiles ? tiles : 1;
-  if (ipt_for(b.capacity) == 8)
-    hist_kernel<8><<<grid, kThreads, 0, stream>>>(b.keys0, b.count, b.begin_bit, b.passes, hist);
-  else
-    hist_kernel<16><<<grid, kThreads, 0, stream>>>(b.keys0, b.count, b.begin_bit, b.passes, hist);
-  plan_kernel<<<1, kThreads, 0, stream>>>(b.count, hist, b.passes, b.plan);
+  if (!b.hist) {
+    if (ipt_for(b.capacity) == 8)
+      hist_kernel<8><<<grid, kThreads, 0, stream>>>(b.keys0, b.count, b.begin_bit, b.passes, hist);
+    else
+      hist_kernel<16><<<grid, kThreads, 0, stream>>>(b.keys0, b.count, b.begin_bit, b.passes, hist);
+  }
+  plan_kernel<<<1, kThreads, 0, stream>>>(b.count, b.hist ? b.hist : hist, b.passes, b.plan);
   for (uint32_t p = 0; p < b.passes; ++p) {
     uint32_t *st = status + (size_t)p * tiles * 256;
     if (ipt_for(b.capacity) == 8)

@@ -5,10 +5,11 @@
 // of each splat's tile rect), and gets its global pair offset from a
 // decoupled look-back, so pairs land in exactly the order a sequential walk
 // would write them: depth order, then rect rows, then rect columns. The
-// block then writes its pairs cooperatively — thread t writes pairs t,
-// t+256, ... and finds the owning splat by binary search over the block's
-// inclusive counts — so a splat covering thousands of tiles does not leave
-// one thread doing all the work.
+// block then writes its pairs cooperatively: each warp walks the pairs of
+// its 128 items 32 at a time, every lane finding its splat with a shuffle
+// search over the items' inclusive pair counts, so a splat covering thousands
+// of tiles is spread over the lanes. The digit histograms the tile sort needs
+// are accumulated while the pairs are written.
 
 #include "device_common.cuh"
 #include "kernels.h"
@@ -19,16 +20,19 @@ namespace {
 constexpr int kEmitThreads = 256;
 constexpr int kEmitIpt = 4;
 constexpr int kEmitItems = kEmitThreads * kEmitIpt;
+constexpr int kEmitWarps = kEmitThreads / 32;
 
 __global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b, uint32_t tiles_x) {
   __shared__ uint32_t s_incl[kEmitItems];
   __shared__ uint32_t s_id[kEmitItems];
   __shared__ uint2 s_rect[kEmitItems];
   __shared__ uint32_t s_wsum[kEmitThreads / 32];
+  __shared__ uint32_t s_hist[3][256];
   __shared__ uint32_t s_block;
   __shared__ unsigned long long s_prefix;
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_block = atomicAdd(&b.counters->emit_ticket, 1u);
+  for (uint32_t k = tid; k < 3 * 256; k += kEmitThreads) (&s_hist[0][0])[k] = 0;
   __syncthreads();
   const uint32_t V = b.counters->visible;
   const uint32_t block = s_block;
@@ -90,23 +94,52 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b, uint3
     b.counters->pairs = (uint32_t)(all < b.capacity ? all : b.capacity);
     if (all > b.capacity) b.counters->overflow = 1u;
   }
-  for (uint32_t k = tid; k < total; k += kEmitThreads) {
-    unsigned long long g = prefix + k;
-    if (g >= b.capacity) break;
-    uint32_t lo = 0, hi = kEmitItems - 1;
-    while (lo < hi) {
-      uint32_t mid = (lo + hi) >> 1;
-      if (s_incl[mid] > k) hi = mid;
-      else lo = mid + 1;
+
+  // Each warp writes the pairs of its own 128 items, 32 pairs per round. For
+  // pair `my` a lane finds its item by a 5-step shuffle search over the
+  // inclusive ends of a 32-item window starting at the round's first item.
+  const uint32_t ib = warp * (kEmitItems / kEmitWarps);
+  const uint32_t il = ib + kEmitItems / kEmitWarps - 1;
+  uint32_t k = ib ? s_incl[ib - 1] : 0u;
+  const uint32_t kend = s_incl[il];
+  uint32_t it = ib;
+  while (k < kend) {
+    const uint32_t inc_w = s_incl[min(it + lane, il)];
+    const uint32_t win_start = it ? s_incl[it - 1] : 0u;
+    const uint32_t win_end = __shfl_sync(0xffffffffu, inc_w, 31);
+    const uint32_t round_end = min(k + 32u, win_end);
+    const uint32_t my = k + lane;
+    uint32_t c = 0;
+#pragma unroll
+    for (uint32_t step = 16; step >= 1; step >>= 1) {
+      uint32_t v = __shfl_sync(0xffffffffu, inc_w, c + step - 1);
+      if (v <= my) c += step;
     }
-    uint32_t first = lo ? s_incl[lo - 1] : 0u;
-    uint32_t off = k - first;
-    uint2 r = s_rect[lo];
-    uint32_t x0 = r.x & 0xffffu, y0 = r.x >> 16;
-    uint32_t w = (r.y & 0xffffu) - x0;
-    uint32_t ty = y0 + off / w, tx = x0 + off % w;
-    b.tile_keys[g] = ty * tiles_x + tx;
-    b.tile_vals[g] = s_id[lo];
+    const uint32_t prev = __shfl_sync(0xffffffffu, inc_w, c ? c - 1 : 0);
+    const unsigned long long g = prefix + my;
+    if (my < round_end && g < b.capacity) {
+      const uint32_t item = it + c;
+      const uint32_t off = my - (c ? prev : win_start);
+      const uint2 r = s_rect[item];
+      const uint32_t x0 = r.x & 0xffffu, y0 = r.x >> 16;
+      const uint32_t w = (r.y & 0xffffu) - x0;
+      uint32_t row = (uint32_t)((float)off * (1.0f / (float)w));
+      if (row * w > off) --row;
+      else if ((row + 1) * w <= off) ++row;
+      const uint32_t tile = (y0 + row) * tiles_x + x0 + (off - row * w);
+      b.tile_keys[g] = tile;
+      b.tile_vals[g] = s_id[item];
+      atomicAdd(&s_hist[0][tile & 255u], 1u);
+      if (b.tile_passes > 1) atomicAdd(&s_hist[1][(tile >> 8) & 255u], 1u);
+      if (b.tile_passes > 2) atomicAdd(&s_hist[2][(tile >> 16) & 255u], 1u);
+    }
+    it += __popc(__ballot_sync(0xffffffffu, inc_w <= round_end));
+    k = round_end;
+  }
+  __syncthreads();
+  for (uint32_t q = tid; q < b.tile_passes * 256; q += kEmitThreads) {
+    uint32_t c = (&s_hist[0][0])[q];
+    if (c) atomicAdd(&b.tile_hist[q], c);
   }
 }
 

@@ -22,6 +22,7 @@ struct K1Buffers {
   Record *records;             // [n] raster record per drawn splat
   unsigned long long *status;  // [ceil(n/256)] look-back words, zeroed
   FrameCounters *counters;
+  uint32_t *key_hist;          // [4][256] digit histograms of the depth keys, zeroed
   ProjectedDev *projected;     // [n] debug tap, or null
 };
 void launch_preprocess(const SceneDev &sc, const FrameParams &p, const K1Buffers &b, bool debug,
@@ -41,10 +42,13 @@ struct SortBuffers {
   SortPlan *plan;
   uint32_t *work;   // sort_work_words(capacity, passes) words of scratch
   uint32_t *error;
+  // Digit histograms [passes][256] already accumulated by the producer of
+  // the keys (then no histogram kernel runs), or null.
+  const uint32_t *hist;
 };
 uint64_t sort_work_words(uint32_t capacity, uint32_t passes);
-// Zeroes the scratch (one memset) and launches the histogram, plan and pass
-// kernels on `stream`.
+// Zeroes the scratch (one memset) and launches the histogram (unless given),
+// plan and pass kernels on `stream`.
 void launch_sort(const SortBuffers &b, cudaStream_t stream);
 
 // ---- K2: tile-pair emission over the depth-sorted visible ids ------------
@@ -56,6 +60,8 @@ struct EmitBuffers {
   uint64_t capacity;
   unsigned long long *status;      // [ceil(n/1024)] look-back words, zeroed
   FrameCounters *counters;
+  uint32_t *tile_hist;             // [passes][256] digit histograms of the tile ids, zeroed
+  uint32_t tile_passes;
   uint32_t n;                      // splat count (upper bound of visible)
 };
 void launch_emit(const EmitBuffers &b, const FrameParams &p, cudaStream_t stream);

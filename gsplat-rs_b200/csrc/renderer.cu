@@ -150,6 +150,8 @@ void Renderer::ensure_scene_workspace() {
   const uint64_t off_counters = off; off += align256(sizeof(FrameCounters));
   const uint64_t off_k1 = off; off += align256(8 * k1_words);
   const uint64_t off_emit = off; off += align256(8 * emit_words);
+  const uint64_t off_khist = off; off += align256(4 * 4 * 256);
+  const uint64_t off_thist = off; off += align256(4 * 4 * 256);
   frame_scratch_zero_bytes_ = off;
   const uint64_t off_dplan = off; off += align256(sizeof(SortPlan));
   const uint64_t off_tplan = off; off += align256(sizeof(SortPlan));
@@ -159,6 +161,8 @@ void Renderer::ensure_scene_workspace() {
   counters_ = frame_scratch_.as<FrameCounters>(off_counters);
   k1_status_ = frame_scratch_.as<unsigned long long>(off_k1);
   emit_status_ = frame_scratch_.as<unsigned long long>(off_emit);
+  key_hist_ = frame_scratch_.as<uint32_t>(off_khist);
+  tile_hist_ = frame_scratch_.as<uint32_t>(off_thist);
   depth_plan_ = frame_scratch_.as<SortPlan>(off_dplan);
   tile_plan_ = frame_scratch_.as<SortPlan>(off_tplan);
   sticky_ = frame_scratch_.as<uint32_t>(off_sticky);
@@ -231,18 +235,20 @@ void Renderer::enqueue_frame(const FrameParams &p) {
   GSR_CUDA(cudaMemsetAsync(ranges_, 0, 8ull * p.num_tiles, stream_));
   GSR_CUDA(cudaEventRecord(ev_[0], stream_));
 
-  K1Buffers k1{vis_keys0_, vis_vals0_, rects_, records_, k1_status_, counters_,
+  K1Buffers k1{vis_keys0_, vis_vals0_, rects_, records_, k1_status_, counters_, key_hist_,
                debug_ ? projected_.as<ProjectedDev>() : nullptr};
   launch_preprocess(scene_->dev, p, k1, debug_, stream_);
   GSR_CUDA(cudaEventRecord(ev_[1], stream_));
 
   SortBuffers ds{vis_keys0_, vis_vals0_, vis_keys1_, vis_vals1_, &counters_->visible,
-                 std::max<uint32_t>(n, 1), 0, 4, depth_plan_, depth_sort_work_, &counters_->error};
+                 std::max<uint32_t>(n, 1), 0, 4, depth_plan_, depth_sort_work_, &counters_->error,
+                 key_hist_};
   launch_sort(ds, stream_);
   GSR_CUDA(cudaEventRecord(ev_[2], stream_));
 
+  const uint32_t tpasses = tile_sort_passes(p.num_tiles);
   EmitBuffers eb{depth_plan_, vis_vals0_, vis_vals1_, rects_, tile_keys0_, tile_vals0_,
-                 key_cap_, emit_status_, counters_, n};
+                 key_cap_, emit_status_, counters_, tile_hist_, tpasses, n};
   launch_emit(eb, p, stream_);
   if (debug_) {
     GSR_CUDA(cudaMemcpyAsync(debug_pairs_.as<uint32_t>(), tile_keys0_, 4 * key_cap_,
@@ -252,8 +258,8 @@ void Renderer::enqueue_frame(const FrameParams &p) {
   }
   GSR_CUDA(cudaEventRecord(ev_[3], stream_));
   SortBuffers ts{tile_keys0_, tile_vals0_, tile_keys1_, tile_vals1_, &counters_->pairs,
-                 (uint32_t)key_cap_, 0, tile_sort_passes(p.num_tiles), tile_plan_,
-                 tile_sort_work_, &counters_->error};
+                 (uint32_t)key_cap_, 0, tpasses, tile_plan_, tile_sort_work_, &counters_->error,
+                 tile_hist_};
   launch_sort(ts, stream_);
   GSR_CUDA(cudaEventRecord(ev_[4], stream_));
   launch_ranges(tile_plan_, tile_keys0_, tile_keys1_, counters_, (uint32_t)key_cap_, ranges_, stream_);

@@ -126,6 +126,8 @@ class Renderer {
   unsigned long long *k1_status_ = nullptr;
   unsigned long long *emit_status_ = nullptr;
   uint32_t *sticky_ = nullptr;  // OR of error bits of every frame since the last sync
+  uint32_t *key_hist_ = nullptr;   // [4][256] depth-key digit histograms (from K1)
+  uint32_t *tile_hist_ = nullptr;  // [4][256] tile-id digit histograms (from K2)
   // Splat-sized workspace.
   DeviceBuffer splat_ws_;
   uint32_t splat_cap_ = 0;

@@ -64,7 +64,7 @@ struct SortScratch {
 // Sorts (k[src], v[src]) ascending; returns the buffer index of the result.
 int run_sort(SortScratch &s, int src, uint32_t n, cudaStream_t st) {
   SortBuffers b{s.k[src], s.v[src], s.k[1 - src], s.v[1 - src], s.count, n, 0, 4, s.plan,
-                s.work, s.error};
+                s.work, s.error, nullptr};
   launch_sort(b, st);
   SortPlan plan;
   uint32_t err = 0;

@@ -148,7 +148,8 @@ typedef struct OrcFrameTiming {
 int32_t orc_render_reference_frame(const OrcScene *scene, const float *alpha,
                                    const float *extent_scale, const float *cov6,
                                    const OrcCamera *camera, uint32_t width, uint32_t height,
-                                   uint8_t *rgba, int32_t threads, OrcFrameTiming *timing);
+                                   uint32_t raster_rows, uint8_t *rgba, int32_t threads,
+                                   OrcFrameTiming *timing);
 
 #ifdef __cplusplus
 }

@@ -51,6 +51,25 @@ inline float exp_neg(float x) {
   return bits_to_float(float_to_bits(p) + (uint32_t)(e * (1 << 23)));
 }
 
+// e^(-4.5 r2) for r2 in [0, 1] as the CUDA FP32 raster computes it: one
+// folded constant (-4.5 log2 e), the 1.5 * 2^23 shifter for the nearest
+// integer n, the same degree-6 Taylor polynomial of 2^f, and n added to the
+// exponent bits.
+inline float gauss_weight(float r2) {
+  const float kShift = 12582912.0f;
+  float t = r2 * -6.49212768f;
+  float tr = t + kShift;
+  float n = tr - kShift;
+  float f = t - n;
+  float p = std::fma(1.54035304e-4f, f, 1.33335581e-3f);
+  p = std::fma(p, f, 9.61812911e-3f);
+  p = std::fma(p, f, 5.55041087e-2f);
+  p = std::fma(p, f, 2.40226507e-1f);
+  p = std::fma(p, f, 6.93147181e-1f);
+  p = std::fma(p, f, 1.0f);
+  return bits_to_float(float_to_bits(p) + (float_to_bits(tr) << 23));
+}
+
 // Round-to-nearest-even UNORM8 conversion of a value clamped to [0, 1].
 inline uint8_t to_unorm8(float x) {
   float c = std::fmin(std::fmax(x, 0.0f), 1.0f);

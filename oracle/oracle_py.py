@@ -115,8 +115,8 @@ def lib():
                                             _u8p, ctypes.c_int32]
         L.orc_render_reference_frame.argtypes = [ctypes.POINTER(OrcScene), _f32p, _f32p, _f32p,
                                                  ctypes.POINTER(OrcCamera), ctypes.c_uint32,
-                                                 ctypes.c_uint32, _u8p, ctypes.c_int32,
-                                                 ctypes.POINTER(OrcFrameTiming)]
+                                                 ctypes.c_uint32, ctypes.c_uint32, _u8p,
+                                                 ctypes.c_int32, ctypes.POINTER(OrcFrameTiming)]
         L.orc_render_reference_frame.restype = ctypes.c_int32
         _lib = L
     return _lib
@@ -311,13 +311,14 @@ def build_instances(sv, cam, width, height, indices):
     return out[:12 * k].reshape(k, 12), out_idx[:k]
 
 
-def render_reference_frame(sv, cam, width, height, threads=8):
-    """The reference SortedAlpha frame on the host CPU; returns (rgba, timing)."""
+def render_reference_frame(sv, cam, width, height, threads=8, rows=0):
+    """The reference SortedAlpha frame on the host CPU; returns (rgba, timing).
+    rows > 0 composites only the top `rows` rows (a bounded sample)."""
     out = np.zeros(width * height * 4, np.uint8)
     t = OrcFrameTiming()
     rc = lib().orc_render_reference_frame(ctypes.byref(sv.c), _p(sv.alpha, _f32p),
                                           _p(sv.extent, _f32p), _p(sv.cov, _f32p),
-                                          ctypes.byref(camera(cam)), width, height,
+                                          ctypes.byref(camera(cam)), width, height, rows,
                                           _p(out, _u8p), threads, ctypes.byref(t))
     if rc != 0:
         raise ValueError("invalid camera")

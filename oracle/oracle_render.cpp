@@ -381,23 +381,42 @@ __attribute__((target_clones("fma", "default"))) static void unorm8_band(
   }
 }
 
+// The CUDA FP32 tile raster, pixel by pixel: per (splat, 16-pixel grid cell)
+// the local offsets ox, oy and s^2; per pixel local = (ax*lx + ay*ly + ox,
+// bx*lx + by*ly + oy) in pixel coordinates relative to the cell corner,
+// coverage r^2 <= s^2 and w > 1/256, C += premult * (g T), T *= 1 - w, stop
+// once T < 1e-4.
 __attribute__((target_clones("fma", "default"))) static void tiles_fp32_band(
     const OrcRecord *records, const uint32_t *ranges, const uint32_t *sorted_ids, uint32_t width,
     uint32_t tile, uint32_t tiles_x, uint8_t *rgba, uint32_t ya, uint32_t yb) {
   for (uint32_t py = ya; py < yb; ++py)
     for (uint32_t px = 0; px < width; ++px) {
-      uint32_t t = (py / tile) * tiles_x + (px / tile);
+      uint32_t tx = px / tile, ty = py / tile;
+      uint32_t t = ty * tiles_x + tx;
+      // local coordinates from the 16-pixel grid corner at or before the tile
+      const uint32_t ax0 = (tx * tile) & ~15u, ay0 = (ty * tile) & ~15u;
+      const float ftx = (float)ax0, fty = (float)ay0;
+      const float fx = (float)(px - ax0), fy = (float)(py - ay0);
       uint32_t start = ranges[2 * t], end = ranges[2 * t + 1];
       float T = 1.0f, c[3] = {0.0f, 0.0f, 0.0f};
       for (uint32_t k = end; k > start; --k) {
         const OrcRecord &r = records[sorted_ids[k - 1]];
-        float g, w;
-        if (!pixel_weight(r, (int)px, (int)py, g, w)) continue;
-        float tn = T * (1.0f - w);
-        c[0] = std::fma(r.pr * g, T, c[0]);
-        c[1] = std::fma(r.pg * g, T, c[1]);
-        c[2] = std::fma(r.pb * g, T, c[2]);
-        T = tn;
+        float cxl = r.cx - ftx, cyl = r.cy - fty;
+        float ox = -std::fma(r.ax, cxl, r.ay * cyl);
+        float oy = -std::fma(r.bx, cxl, r.by * cyl);
+        float s2 = r.s * r.s;
+        float lx = std::fma(r.ax, fx, std::fma(r.ay, fy, ox));
+        float ly = std::fma(r.bx, fx, std::fma(r.by, fy, oy));
+        float r2 = std::fma(lx, lx, ly * ly);
+        if (!(r2 <= s2)) continue;
+        float g = gauss_weight(r2);
+        float w = r.alpha * g;
+        if (!(w > 1.0f / 256.0f)) continue;
+        float gT = g * T;
+        c[0] = std::fma(r.pr, gT, c[0]);
+        c[1] = std::fma(r.pg, gT, c[1]);
+        c[2] = std::fma(r.pb, gT, c[2]);
+        T = T * (1.0f - w);
         if (T < 1e-4f) break;
       }
       uint8_t *d = &rgba[((size_t)py * width + px) * 4];
@@ -600,9 +619,7 @@ void orc_raster_f64(const OrcRecord *records, const OrcProjected *proj, const ui
 }
 
 // Restatement of the CUDA FP32 front-to-back tile raster: each pixel walks its
-// tile's list from the back (nearest) to the front, accumulates
-// C += (premult * g) * T, T *= (1 - w), and stops once T < 1e-4 after adding
-// the splat that crossed the threshold.
+// tile's list from the back (nearest) to the front (see tiles_fp32_band).
 void orc_raster_tiles_fp32(const OrcRecord *records, const uint32_t *ranges,
                            const uint32_t *sorted_ids, uint32_t width, uint32_t height,
                            uint32_t tile, uint32_t tiles_x, uint8_t *rgba, int32_t threads) {
@@ -617,7 +634,8 @@ void orc_raster_tiles_fp32(const OrcRecord *records, const uint32_t *ranges,
 int32_t orc_render_reference_frame(const OrcScene *scene, const float *alpha,
                                    const float *extent_scale, const float *cov6,
                                    const OrcCamera *camera, uint32_t width, uint32_t height,
-                                   uint8_t *rgba, int32_t threads, OrcFrameTiming *timing) {
+                                   uint32_t raster_rows, uint8_t *rgba, int32_t threads,
+                                   OrcFrameTiming *timing) {
   using clk = std::chrono::steady_clock;
   auto ms = [](clk::time_point a, clk::time_point b) {
     return std::chrono::duration<double, std::milli>(b - a).count();
@@ -651,7 +669,12 @@ int32_t orc_render_reference_frame(const OrcScene *scene, const float *alpha,
     for (int t = 0; t < nt; ++t) drawn += drawn_t[t];
   }
   auto t3 = clk::now();
-  orc_raster_unorm8(rec.data(), proj.data(), order.data(), v, width, height, rgba, threads);
+  // raster_rows < height composites only the top rows (a bounded sample).
+  uint32_t rows = raster_rows && raster_rows < height ? raster_rows : height;
+  std::memset(rgba, 0, (size_t)width * height * 4);
+  parallel_rows(rows, threads, [&](uint32_t ya, uint32_t yb) {
+    unorm8_band(rec.data(), proj.data(), order.data(), v, width, height, rgba, ya, yb);
+  });
   auto t4 = clk::now();
   if (timing) {
     timing->preprocess_ms = ms(t0, t1);
