@@ -491,6 +491,16 @@ int32_t gsplat_cuda_sort_pairs(uint32_t *keys, uint32_t *values, uint64_t len) {
   });
 }
 
+int32_t gsplat_cuda_sort_values_by_keys_noalloc(const uint32_t *keys, uint32_t *values,
+                                                uint64_t len, void *stream) {
+  return guarded("gsplat_cuda_sort_values_by_keys_noalloc", [&]() -> int32_t {
+    std::string msg;
+    Code c = gsr::sort_values_by_keys_noalloc(keys, values, len, (cudaStream_t)stream, msg);
+    if (c != Code::Ok) return fail(c, "gsplat_cuda_sort_values_by_keys_noalloc: " + msg);
+    return ok();
+  });
+}
+
 int32_t gsplat_ply_load(const char *path, GsplatHostScene **out_scene) {
   return guarded("gsplat_ply_load", [&]() -> int32_t {
     if (!out_scene) return fail(Code::InvalidArgument, "gsplat_ply_load: out_scene is null");

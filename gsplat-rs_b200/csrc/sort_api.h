@@ -2,6 +2,11 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "gsr_host.h"
 
 namespace gsr {
 
@@ -15,5 +20,13 @@ void sort_pairs_host(uint32_t *keys, uint32_t *values, uint64_t n);
 
 void device_info(char *name, uint64_t name_capacity, int32_t *sm_count, int32_t *cc_major,
                  int32_t *cc_minor);
+
+// The same sort on caller-owned device buffers, with all scratch in a static
+// device array (sort_noalloc.cu); never allocates. Returns Ok or an error code
+// with `msg` set.
+Code sort_values_by_keys_noalloc(const uint32_t *keys, uint32_t *values, uint64_t n,
+                                 cudaStream_t stream, std::string &msg);
+uint64_t noalloc_scratch_bytes();
+uint32_t noalloc_max_items();
 
 }  // namespace gsr

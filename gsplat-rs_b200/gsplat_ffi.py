@@ -169,6 +169,8 @@ _SIGS = [
       ctypes.POINTER(ctypes.c_uint64)]),
     ("gsplat_cuda_sort_values_by_keys", ctypes.c_int32, [_u32p, _u32p, ctypes.c_uint64]),
     ("gsplat_cuda_sort_pairs", ctypes.c_int32, [_u32p, _u32p, ctypes.c_uint64]),
+    ("gsplat_cuda_sort_values_by_keys_noalloc", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
     ("gsplat_ply_load", ctypes.c_int32, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
     ("gsplat_host_scene_destroy", None, [ctypes.c_void_p]),
     ("gsplat_host_scene_view", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(GsplatSceneDesc)]),

@@ -146,6 +146,25 @@ int32_t gsplat_cuda_sort_values_by_keys(const uint32_t *keys, uint32_t *values, 
  * ascending value; both arrays are permuted. */
 int32_t gsplat_cuda_sort_pairs(uint32_t *keys, uint32_t *values, uint64_t len);
 
+/* No counterpart in the reference: an allocation-free form of
+ * gsplat_cuda_sort_values_by_keys for callers that cannot allocate device
+ * memory — hosts that own all GPU memory through their own pool and forbid
+ * libraries to call cudaMalloc, or latency-critical threads where
+ * cudaMalloc/cudaFree (which can synchronise the device) are not allowed.
+ * `keys` and `values` are caller-owned DEVICE pointers of `len` elements;
+ * `values` is permuted in place so that keys descend, equal keys keeping
+ * their input order, and `keys` is left unchanged. `stream` is a
+ * cudaStream_t (NULL for the default stream); the call waits for it before
+ * returning. All scratch lives in one static device array of about 14.7 MB
+ * that every GPU loading the library holds until exit; len above
+ * 1,048,576 (2^20) is rejected with GSPLAT_ERROR_INVALID_ARGUMENT. The first
+ * call on a device looks the array's address up (cudaGetSymbolAddress), so
+ * make it before any stream capture starts on that device. Calls share the
+ * array; overlapping calls would race, so calls are serialised inside the
+ * process. Nothing here calls cudaMalloc or cudaFree. */
+int32_t gsplat_cuda_sort_values_by_keys_noalloc(const uint32_t *keys, uint32_t *values,
+                                                uint64_t len, void *stream);
+
 /* ---- host utilities ---- */
 
 /* Parsed PLY scene owned by the library (crates/gsplat-io-ply/src/lib.rs:178-235). */
