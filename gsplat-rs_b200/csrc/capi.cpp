@@ -339,6 +339,14 @@ int32_t gsplat_context_set_debug_taps(GsplatContext *ctx, uint32_t enabled) {
   });
 }
 
+int32_t gsplat_context_set_cuda_graph(GsplatContext *ctx, uint32_t enabled) {
+  return guarded("gsplat_context_set_cuda_graph", [&]() -> int32_t {
+    if (!ctx) return fail(Code::InvalidArgument, "gsplat_context_set_cuda_graph: ctx is null");
+    ctx->renderer->set_use_graph(enabled != 0);
+    return ok();
+  });
+}
+
 int32_t gsplat_context_load_scene_buffers(GsplatContext *ctx, const GsplatSceneDesc *scene) {
   return guarded("gsplat_context_load_scene_buffers", [&]() -> int32_t {
     if (!ctx || !scene)

@@ -87,6 +87,65 @@ __device__ __forceinline__ unsigned long long lookback_warp(unsigned long long *
   return exclusive;
 }
 
+// Finds the view a block or a global index belongs to: the last v with
+// base(v) <= x, by binary search over the view table.
+template <typename F>
+__device__ __forceinline__ uint32_t find_view(uint32_t num_views, uint32_t x, F base) {
+  uint32_t lo = 0, hi = num_views - 1;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi + 1) >> 1;
+    if (base(mid) <= x) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Split form of the look-back for kernels that learn their block's count
+// early but can use the prefix only later: publish the aggregate as soon as
+// it is known, resolve the exclusive prefix (any warp, read-only) later, and
+// have exactly one warp publish the inclusive prefix afterwards.
+__device__ __forceinline__ void lookback_publish_aggregate(unsigned long long *status,
+                                                           uint32_t block,
+                                                           unsigned long long aggregate) {
+  st_relaxed_u64(&status[block], (block == 0 ? kFlagInc : kFlagAgg) | aggregate);
+}
+
+__device__ __forceinline__ unsigned long long lookback_resolve(unsigned long long *status,
+                                                               uint32_t block, uint32_t *error) {
+  const uint32_t lane = threadIdx.x & 31;
+  if (block == 0) return 0;
+  unsigned long long exclusive = 0;
+  int64_t base = (int64_t)block - 1;
+  uint32_t spins = 0;
+  while (true) {
+    int64_t idx = base - (int64_t)lane;
+    unsigned long long s = idx >= 0 ? ld_relaxed_u64(&status[idx]) : kFlagInc;
+    if (__any_sync(0xffffffffu, (s >> 62) == 0)) {
+      if (++spins > kSpinLimit) {
+        if (lane == 0) atomicOr(error, kErrLookbackTimeout);
+        break;
+      }
+      __nanosleep(32);
+      continue;
+    }
+    uint32_t inc = __ballot_sync(0xffffffffu, (s >> 62) == 2);
+    if (inc) {
+      uint32_t first = __ffs(inc) - 1;
+      exclusive += warp_sum<unsigned long long>(lane <= first ? (s & kValueMask) : 0ull);
+      break;
+    }
+    exclusive += warp_sum<unsigned long long>(s & kValueMask);
+    base -= 32;
+  }
+  return exclusive;
+}
+
+__device__ __forceinline__ void lookback_publish_inclusive(unsigned long long *status,
+                                                           uint32_t block,
+                                                           unsigned long long inclusive) {
+  if (block != 0) st_relaxed_u64(&status[block], kFlagInc | inclusive);
+}
+
 // e^x for x in [-4.5, 0]: Cody-Waite reduction to base 2 and the degree-6
 // Taylor polynomial of 2^f (coefficients ln(2)^k / k!), explicit fmaf, so the
 // result is reproducible bit for bit by a C++ restatement. Relative error

@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <vector_types.h>
 
+#include "gsr_host.h"
+
 namespace gsr {
 
 // Scene resident in HBM, structure of arrays of float4 planes (16-byte
@@ -62,6 +64,26 @@ struct FrameCounters {
   uint32_t pad0;
   unsigned long long keys;  // pairs emitted (may exceed the capacity)
   uint32_t sort_tickets[16];
+};
+
+// One view of a frame batch (a plain frame is a batch of one view). Splats
+// of all views share one index space: view v's splat i is gid = splat_base+i.
+struct ViewDev {
+  FrameParams p;       // per-view uniforms (camera, image size, tile grid)
+  SceneDev sc;         // the view's scene
+  uint32_t splat_base; // first gid of the view
+  uint32_t block_base; // first preprocess block of the view
+  uint32_t tile_base;  // first global tile id of the view
+  uint32_t pad;
+  unsigned long long image_base;  // first pixel of the view's image
+};
+
+// Per-view counters of a batch (zeroed per batch).
+struct ViewCounters {
+  uint32_t visible;
+  uint32_t drawn;
+  uint32_t pairs;
+  uint32_t pad;
 };
 
 // Plan of one radix sort, computed on the device from the global histogram.

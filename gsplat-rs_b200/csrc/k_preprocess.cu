@@ -200,7 +200,8 @@ __device__ __forceinline__ bool project(const SceneDev &sc, const FrameParams &p
   }
   float4 fbuf[kPlanes];
 #pragma unroll
-  for (int k = 0; k < kPlanes; ++k) fbuf[k] = sc.color[(size_t)k * sc.n + i];
+  for (int k = 0; k < kPlanes; ++k)
+    fbuf[k] = k < (int)sc.planes ? sc.color[(size_t)k * sc.n + i] : make_float4(0.f, 0.f, 0.f, 0.f);
   float rgb[3];
   eval_sh<kPlanes>(fbuf, p.sh_degree, dx, dy, dz, rgb);
 #pragma unroll
@@ -255,20 +256,28 @@ __device__ __forceinline__ bool project(const SceneDev &sc, const FrameParams &p
 constexpr int kK1Threads = 256;
 
 template <int kPlanes, bool kDebug>
-__global__ void __launch_bounds__(kK1Threads) preprocess_kernel(
-    SceneDev sc, FrameParams p, uint32_t *__restrict__ vis_keys, uint32_t *__restrict__ vis_ids,
-    uint2 *__restrict__ rects, Record *__restrict__ records, unsigned long long *status,
-    FrameCounters *counters, uint32_t *__restrict__ key_hist, ProjectedDev *__restrict__ dbg_out) {
+__global__ void __launch_bounds__(kK1Threads) preprocess_kernel(const ViewDev *__restrict__ views,
+                                                                uint32_t num_views,
+                                                                uint32_t total_blocks,
+                                                                K1Buffers b) {
   __shared__ uint32_t s_block;
+  __shared__ uint32_t s_view;
   __shared__ uint32_t s_warp[kK1Threads / 32];
-  __shared__ uint32_t s_prefix;
   __shared__ uint32_t s_hist[4][256];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (threadIdx.x == 0) s_block = atomicAdd(&counters->k1_ticket, 1u);
+  if (threadIdx.x == 0) {
+    const uint32_t blk = atomicAdd(&b.counters->k1_ticket, 1u);
+    s_block = blk;
+    s_view = find_view(num_views, blk, [&](uint32_t v) { return views[v].block_base; });
+  }
   for (uint32_t k = threadIdx.x; k < 4 * 256; k += kK1Threads) (&s_hist[0][0])[k] = 0;
   __syncthreads();
   const uint32_t block = s_block;
-  const uint32_t i = block * kK1Threads + threadIdx.x;
+  const uint32_t view = s_view;
+  const FrameParams p = views[view].p;
+  const SceneDev sc = views[view].sc;
+  const uint32_t i = (block - views[view].block_base) * kK1Threads + threadIdx.x;
+  const uint32_t gid = views[view].splat_base + i;
   const bool valid = i < sc.n;
 
   float4 pa = valid ? sc.pos_alpha[i] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -276,11 +285,27 @@ __global__ void __launch_bounds__(kK1Threads) preprocess_kernel(
   float depth = p.r2[0] * rel[0] + p.r2[1] * rel[1] + p.r2[2] * rel[2];
   const bool vis = valid && depth >= p.near_plane && depth <= p.far_plane;
 
-  // The vertex stage first (it does not depend on the compaction), so that
-  // the look-back below waits on predecessors that have long published.
+  // The block's visible count is known right after the depth test: publish
+  // it for the successors' look-back before doing the heavy vertex stage.
+  const uint32_t ballot = __ballot_sync(0xffffffffu, vis);
+  const uint32_t rank = __popc(ballot & lanemask_lt());
+  if (lane == 0) s_warp[warp] = __popc(ballot);
+  __syncthreads();
+  uint32_t warp_prefix = 0, block_total = 0;
+#pragma unroll
+  for (int w = 0; w < kK1Threads / 32; ++w) {
+    uint32_t c = s_warp[w];
+    warp_prefix += (w < (int)warp) ? c : 0u;
+    block_total += c;
+  }
+  if (threadIdx.x == 0) {
+    lookback_publish_aggregate(b.status, block, block_total);
+    if (block_total) atomicAdd(&b.view_counters[view].visible, block_total);
+  }
+
   ProjectedDev *dbg = nullptr;
   if (kDebug && valid) {
-    dbg = &dbg_out[i];
+    dbg = &b.projected[gid];
     ProjectedDev z = {};
     z.depth = depth;
     z.flags = vis ? 1u : 0u;
@@ -291,72 +316,61 @@ __global__ void __launch_bounds__(kK1Threads) preprocess_kernel(
     Record rec;
     uint2 rect = make_uint2(0u, 0u);
     bool drawn = project<kPlanes>(sc, p, i, pa, rel, depth, rec, rect, dbg);
-    rects[i] = rect;
+    b.rects[gid] = rect;
     if (drawn) {
-      records[i] = rec;
+      b.records[gid] = rec;
       uint32_t dmask = __ballot_sync(__activemask(), true);
-      if (lane == __ffs(dmask) - 1) atomicAdd(&counters->drawn, __popc(dmask));
+      if (lane == __ffs(dmask) - 1) {
+        atomicAdd(&b.counters->drawn, __popc(dmask));
+        atomicAdd(&b.view_counters[view].drawn, __popc(dmask));
+      }
     }
     // Digit histograms of the depth keys for every radix pass.
 #pragma unroll
     for (int d = 0; d < 4; ++d) atomicAdd(&s_hist[d][(key >> (8 * d)) & 255u], 1u);
   }
-
-  // Block-wide compaction of the visible flags, then the global offset.
-  const uint32_t ballot = __ballot_sync(0xffffffffu, vis);
-  const uint32_t rank = __popc(ballot & lanemask_lt());
-  if (lane == 0) s_warp[warp] = __popc(ballot);
+  // Every warp resolves the block's offset on its own (no second block
+  // barrier); warp 0 publishes the inclusive prefix.
+  const unsigned long long prefix = lookback_resolve(b.status, block, &b.counters->error);
+  if (warp == 0 && lane == 0) {
+    lookback_publish_inclusive(b.status, block, prefix + block_total);
+    if (block == total_blocks - 1) b.counters->visible = (uint32_t)(prefix + block_total);
+  }
+  if (vis) {
+    const uint32_t slot = (uint32_t)prefix + warp_prefix + rank;
+    b.vis_keys[slot] = key;
+    b.vis_ids[slot] = gid;
+  }
   __syncthreads();
   for (uint32_t k = threadIdx.x; k < 4 * 256; k += kK1Threads) {
     uint32_t c = (&s_hist[0][0])[k];
-    if (c) atomicAdd(&key_hist[k], c);
+    if (c) atomicAdd(&b.key_hist[k], c);
   }
-  uint32_t warp_prefix = 0, block_total = 0;
-#pragma unroll
-  for (int w = 0; w < kK1Threads / 32; ++w) {
-    uint32_t c = s_warp[w];
-    warp_prefix += (w < (int)warp) ? c : 0u;
-    block_total += c;
-  }
-  if (warp == 0) {
-    unsigned long long ex = lookback_warp(status, block, block_total, &counters->error);
-    if (lane == 0) s_prefix = (uint32_t)ex;
-  }
-  __syncthreads();
-  const uint32_t prefix = s_prefix;
-  if (threadIdx.x == 0 && block == (sc.n - 1) / kK1Threads) counters->visible = prefix + block_total;
-  if (!vis) return;
-  const uint32_t slot = prefix + warp_prefix + rank;
-  vis_keys[slot] = key;
-  vis_ids[slot] = i;
 }
 
 template <int kPlanes>
-void launch_k1(const SceneDev &sc, const FrameParams &p, const K1Buffers &b, bool debug,
-               cudaStream_t stream) {
-  uint32_t blocks = (sc.n + kK1Threads - 1) / kK1Threads;
-  if (blocks == 0) return;
+void launch_k1(const ViewDev *views, uint32_t num_views, uint32_t total_blocks, const K1Buffers &b,
+               bool debug, cudaStream_t stream) {
+  if (total_blocks == 0) return;
   if (debug)
-    preprocess_kernel<kPlanes, true><<<blocks, kK1Threads, 0, stream>>>(
-        sc, p, b.vis_keys, b.vis_ids, b.rects, b.records, b.status, b.counters, b.key_hist,
-        b.projected);
+    preprocess_kernel<kPlanes, true><<<total_blocks, kK1Threads, 0, stream>>>(views, num_views,
+                                                                              total_blocks, b);
   else
-    preprocess_kernel<kPlanes, false><<<blocks, kK1Threads, 0, stream>>>(
-        sc, p, b.vis_keys, b.vis_ids, b.rects, b.records, b.status, b.counters, b.key_hist,
-        nullptr);
+    preprocess_kernel<kPlanes, false><<<total_blocks, kK1Threads, 0, stream>>>(views, num_views,
+                                                                               total_blocks, b);
 }
 
 }  // namespace
 
-void launch_preprocess(const SceneDev &sc, const FrameParams &p, const K1Buffers &b, bool debug,
-                       cudaStream_t stream) {
-  switch (sc.planes) {
-    case 1: launch_k1<1>(sc, p, b, debug, stream); break;
-    case 3: launch_k1<3>(sc, p, b, debug, stream); break;
-    case 7: launch_k1<7>(sc, p, b, debug, stream); break;
-    case 12: launch_k1<12>(sc, p, b, debug, stream); break;
-    default: launch_k1<19>(sc, p, b, debug, stream); break;
-  }
+uint32_t preprocess_blocks(uint32_t splats) { return (splats + kK1Threads - 1) / kK1Threads; }
+
+void launch_preprocess(const ViewDev *views, uint32_t num_views, uint32_t total_blocks,
+                       uint32_t max_planes, const K1Buffers &b, bool debug, cudaStream_t stream) {
+  if (max_planes <= 1) launch_k1<1>(views, num_views, total_blocks, b, debug, stream);
+  else if (max_planes <= 3) launch_k1<3>(views, num_views, total_blocks, b, debug, stream);
+  else if (max_planes <= 7) launch_k1<7>(views, num_views, total_blocks, b, debug, stream);
+  else if (max_planes <= 12) launch_k1<12>(views, num_views, total_blocks, b, debug, stream);
+  else launch_k1<19>(views, num_views, total_blocks, b, debug, stream);
 }
 
 }  // namespace gsr

@@ -36,22 +36,40 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // UNORM8 parity mode: back to front over the tile list, the reference
 // fragment rule with the quad clip, rounding to UNORM8 after every blend.
+// Per-block prologue shared by both raster kernels: fold the frame's error
+// bits into the sticky word (block 0) and find the view of this global tile.
+__device__ __forceinline__ uint32_t raster_view(const ViewDev *__restrict__ views,
+                                                uint32_t num_views,
+                                                const FrameCounters *__restrict__ counters,
+                                                uint32_t *sticky, uint32_t *s_view) {
+  if (threadIdx.x == 0) {
+    if (blockIdx.x == 0) {
+      uint32_t bits = counters->error | (counters->overflow ? 0x80000000u : 0u);
+      if (bits) atomicOr(sticky, bits);
+    }
+    *s_view = find_view(num_views, blockIdx.x, [&](uint32_t v) { return views[v].tile_base; });
+  }
+  __syncthreads();
+  return *s_view;
+}
+
 template <int kTile>
 __global__ void __launch_bounds__(kTile *kTile) raster_unorm8_kernel(
-    FrameParams p, const uint2 *__restrict__ ranges, const SortPlan *__restrict__ plan,
-    const uint32_t *__restrict__ ids0, const uint32_t *__restrict__ ids1,
-    const Record *__restrict__ records, uint32_t *__restrict__ image,
-    const FrameCounters *__restrict__ counters, uint32_t *sticky) {
+    const ViewDev *__restrict__ views, uint32_t num_views, const uint2 *__restrict__ ranges,
+    const SortPlan *__restrict__ plan, const uint32_t *__restrict__ ids0,
+    const uint32_t *__restrict__ ids1, const Record *__restrict__ records,
+    uint32_t *__restrict__ images, const FrameCounters *__restrict__ counters, uint32_t *sticky) {
   constexpr int kN = kTile * kTile;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    uint32_t bits = counters->error | (counters->overflow ? 0x80000000u : 0u);
-    if (bits) atomicOr(sticky, bits);
-  }
   __shared__ float4 s_a[2][kN];
   __shared__ float4 s_b[2][kN];
   __shared__ float4 s_c[2][kN];
+  __shared__ uint32_t s_view;
+  const uint32_t view = raster_view(views, num_views, counters, sticky, &s_view);
+  const FrameParams p = views[view].p;
+  uint32_t *__restrict__ image = images + views[view].image_base;
   const uint32_t tile = blockIdx.x;
-  const uint32_t tx = tile % p.tiles_x, ty = tile / p.tiles_x;
+  const uint32_t local_tile = tile - views[view].tile_base;
+  const uint32_t tx = local_tile % p.tiles_x, ty = local_tile / p.tiles_x;
   const uint32_t tid = threadIdx.x;
   const uint32_t px = tx * kTile + (tid % kTile);
   const uint32_t py = ty * kTile + (tid / kTile);
@@ -119,17 +137,14 @@ __global__ void __launch_bounds__(kTile *kTile) raster_unorm8_kernel(
 // Culling is conservative, so results equal the unculled per-pixel walk.
 template <int kTile>
 __global__ void __launch_bounds__(kTile *kTile) raster_fp32_kernel(
-    FrameParams p, const uint2 *__restrict__ ranges, const SortPlan *__restrict__ plan,
-    const uint32_t *__restrict__ ids0, const uint32_t *__restrict__ ids1,
-    const Record *__restrict__ records, uint32_t *__restrict__ image,
-    const FrameCounters *__restrict__ counters, uint32_t *sticky) {
+    const ViewDev *__restrict__ views, uint32_t num_views, const uint2 *__restrict__ ranges,
+    const SortPlan *__restrict__ plan, const uint32_t *__restrict__ ids0,
+    const uint32_t *__restrict__ ids1, const Record *__restrict__ records,
+    uint32_t *__restrict__ images, const FrameCounters *__restrict__ counters, uint32_t *sticky) {
   constexpr int kN = kTile * kTile;
   constexpr int kWarps = kN / 32;
   constexpr int kBlocksX = kTile / 8;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    uint32_t bits = counters->error | (counters->overflow ? 0x80000000u : 0u);
-    if (bits) atomicOr(sticky, bits);
-  }
+  __shared__ uint32_t s_view;
   __shared__ float4 s_raw[2][3][kN];
   __shared__ float4 s_d0[kN];  // ax, ay, ox, s2
   __shared__ float4 s_d1[kN];  // bx, by, oy, alpha
@@ -137,14 +152,19 @@ __global__ void __launch_bounds__(kTile *kTile) raster_fp32_kernel(
   __shared__ uint8_t s_mask[kN];
   __shared__ uint16_t s_list[kWarps][kN];
 
+  const uint32_t view = raster_view(views, num_views, counters, sticky, &s_view);
+  const uint32_t width = views[view].p.width, height = views[view].p.height;
+  const uint32_t tiles_x = views[view].p.tiles_x;
+  uint32_t *__restrict__ image = images + views[view].image_base;
   const uint32_t tile = blockIdx.x;
-  const uint32_t tx = tile % p.tiles_x, ty = tile / p.tiles_x;
+  const uint32_t local_tile = tile - views[view].tile_base;
+  const uint32_t tx = local_tile % tiles_x, ty = local_tile / tiles_x;
   const uint32_t x0 = tx * kTile, y0 = ty * kTile;
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t bx0 = (warp % kBlocksX) * 8, by0 = (warp / kBlocksX) * 4;
   const uint32_t lxp = bx0 + (lane & 7), lyp = by0 + (lane >> 3);
   const uint32_t px = x0 + lxp, py = y0 + lyp;
-  const bool inside = px < p.width && py < p.height;
+  const bool inside = px < width && py < height;
   // Local coordinates are taken from the 16-pixel grid corner at or before
   // the tile, so 8x8 and 16x16 tiles evaluate every pixel identically.
   const uint32_t ax0 = x0 & ~15u, ay0 = y0 & ~15u;
@@ -185,18 +205,41 @@ __global__ void __launch_bounds__(kTile *kTile) raster_fp32_kernel(
       s_d0[tid] = make_float4(a.z, a.w, ox, b.z * b.z);
       s_d1[tid] = make_float4(b.x, b.y, oy, b.w);
       s_d2[tid] = col;
-      // Bounding box of |local| <= s: half extents s*|row of M| / |det M^-1|.
-      float inv_det = 1.0f / fabsf(a.z * b.y - a.w * b.x);
-      float hx = b.z * sqrtf(b.y * b.y + a.w * a.w) * inv_det + 1.0f;
-      float hy = b.z * sqrtf(b.x * b.x + a.z * a.z) * inv_det + 1.0f;
+      // Which 8x4 warp blocks the ellipse |local| <= s reaches: for each
+      // 4-row band, the x-interval the ellipse spans within the band (plus
+      // half a pixel on every side), tested against the two 8-column blocks.
+      // q(dx, dy) = A dx^2 + 2B dx dy + C dy^2 is |local|^2 in pixel units.
+      const float qa = fmaf(a.z, a.z, b.x * b.x);
+      const float qb = fmaf(a.z, a.w, b.x * b.y);
+      const float qc = fmaf(a.w, a.w, b.y * b.y);
+      const float s2 = b.z * b.z;
+      const float det = fmaf(qa, qc, -qb * qb);
+      const float inv_a = 1.0f / qa;
+      const float hx = sqrtf(s2 * qc / det);
+      const float hy = sqrtf(s2 * qa / det);
+      const float dy_left = qb * hx / qc;  // dy of the leftmost point; rightmost at -dy_left
+      const float s2a = s2 * qa;
       uint32_t mask = 0;
 #pragma unroll
-      for (int w = 0; w < kWarps; ++w) {
-        float bxl = (float)((w % kBlocksX) * 8), byl = (float)((w / kBlocksX) * 4);
-        bool hit = cxl + hx >= bxl && cxl - hx <= bxl + 7.0f && cyl + hy >= byl &&
-                   cyl - hy <= byl + 3.0f;
-        mask |= hit ? (1u << w) : 0u;
+      for (int band = 0; band < kTile / 4; ++band) {
+        const float lo = fmaxf((float)(4 * band) - 0.5f - cyl, -hy);
+        const float hi = fminf((float)(4 * band) + 3.5f - cyl, hy);
+        if (!(lo <= hi)) continue;
+        const float r_lo = sqrtf(fmaxf(s2a - det * lo * lo, 0.0f));
+        const float r_hi = sqrtf(fmaxf(s2a - det * hi * hi, 0.0f));
+        float xmin = fminf((-qb * lo - r_lo) * inv_a, (-qb * hi - r_hi) * inv_a);
+        float xmax = fmaxf((-qb * lo + r_lo) * inv_a, (-qb * hi + r_hi) * inv_a);
+        if (dy_left >= lo && dy_left <= hi) xmin = -hx;
+        if (-dy_left >= lo && -dy_left <= hi) xmax = hx;
+        const float x0 = cxl + xmin - 0.5f, x1 = cxl + xmax + 0.5f;
+#pragma unroll
+        for (int col = 0; col < kBlocksX; ++col)
+          if (x1 >= (float)(8 * col) && x0 <= (float)(8 * col + 7))
+            mask |= 1u << (band * kBlocksX + col);
       }
+      // A degenerate conic (never expected: axes are clamped to an
+      // anisotropy of 64) falls back to every block.
+      if (!(det > 0.0f) || !(hx < 3.0e38f) || !(hy < 3.0e38f)) mask = (1u << kWarps) - 1u;
       s_mask[tid] = (uint8_t)mask;
     }
     __syncthreads();
@@ -234,28 +277,28 @@ __global__ void __launch_bounds__(kTile *kTile) raster_fp32_kernel(
   }
   cp_async_wait_all();
   if (inside)
-    image[(size_t)py * p.width + px] = to_unorm8(c0) | (to_unorm8(c1) << 8) |
+    image[(size_t)py * width + px] = to_unorm8(c0) | (to_unorm8(c1) << 8) |
                                        (to_unorm8(c2) << 16) | (to_unorm8(1.0f - T) << 24);
 }
 
 }  // namespace
 
-void launch_raster(const FrameParams &p, const uint2 *ranges, const SortPlan *tile_plan,
-                   const uint32_t *ids0, const uint32_t *ids1, const Record *records,
-                   uint32_t *image, uint32_t blend_mode, const FrameCounters *counters,
-                   uint32_t *sticky, cudaStream_t stream) {
-  const uint32_t blocks = p.num_tiles;
-  if (blocks == 0) return;
-  if (p.tile == 16) {
+void launch_raster(const ViewDev *views, uint32_t num_views, uint32_t total_tiles, uint32_t tile,
+                   const uint2 *ranges, const SortPlan *tile_plan, const uint32_t *ids0,
+                   const uint32_t *ids1, const Record *records, uint32_t *images,
+                   uint32_t blend_mode, const FrameCounters *counters, uint32_t *sticky,
+                   cudaStream_t stream) {
+  if (total_tiles == 0) return;
+  if (tile == 16) {
     if (blend_mode == 1)
-      raster_unorm8_kernel<16><<<blocks, 256, 0, stream>>>(p, ranges, tile_plan, ids0, ids1, records, image, counters, sticky);
+      raster_unorm8_kernel<16><<<total_tiles, 256, 0, stream>>>(views, num_views, ranges, tile_plan, ids0, ids1, records, images, counters, sticky);
     else
-      raster_fp32_kernel<16><<<blocks, 256, 0, stream>>>(p, ranges, tile_plan, ids0, ids1, records, image, counters, sticky);
+      raster_fp32_kernel<16><<<total_tiles, 256, 0, stream>>>(views, num_views, ranges, tile_plan, ids0, ids1, records, images, counters, sticky);
   } else {
     if (blend_mode == 1)
-      raster_unorm8_kernel<8><<<blocks, 64, 0, stream>>>(p, ranges, tile_plan, ids0, ids1, records, image, counters, sticky);
+      raster_unorm8_kernel<8><<<total_tiles, 64, 0, stream>>>(views, num_views, ranges, tile_plan, ids0, ids1, records, images, counters, sticky);
     else
-      raster_fp32_kernel<8><<<blocks, 64, 0, stream>>>(p, ranges, tile_plan, ids0, ids1, records, image, counters, sticky);
+      raster_fp32_kernel<8><<<total_tiles, 64, 0, stream>>>(views, num_views, ranges, tile_plan, ids0, ids1, records, images, counters, sticky);
   }
 }
 

@@ -1,5 +1,5 @@
 // K3: onesweep LSD radix sort of (u32 key, u32 value) pairs, ascending and
-// stable, 8-bit digits.
+// stable, 8-bit digits, 256 threads and 8 or 16 keys per thread.
 //
 //   1. histogram kernel: one read of the keys builds the digit histograms of
 //      every pass (shared-memory histograms, one global add per bin and block);
@@ -183,24 +183,43 @@ __global__ void __launch_bounds__(kThreads) pass_kernel(const SortPlan *__restri
   uint32_t total;
   s_block_start[d] = block_exclusive_scan(block_count, s_wsum, total);
 
+  // Look back over the predecessor tiles, four status words per step: add
+  // aggregates until the nearest inclusive prefix; restart a step when one
+  // of the words it needs is not published yet.
   uint32_t exclusive = 0;
   if (tile > 0) {
     int32_t t = (int32_t)tile - 1;
     uint32_t spins = 0;
     while (t >= 0) {
-      uint32_t s = ld_relaxed_u32(&status[(size_t)t * 256 + d]);
-      uint32_t flag = s & ~kMask;
-      if (flag == 0) {
+      uint32_t w[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        w[q] = (t - q >= 0) ? ld_relaxed_u32(&status[(size_t)(t - q) * 256 + d]) : kFlagP;
+      bool found = false, stalled = false;
+      uint32_t add = 0;
+      int used = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (found || stalled) continue;
+        uint32_t flag = w[q] & ~kMask;
+        if (flag == 0) {
+          stalled = true;
+          continue;
+        }
+        add += (t - q >= 0) ? (w[q] & kMask) : 0u;
+        ++used;
+        if (flag == kFlagP) found = true;
+      }
+      exclusive += add;
+      t -= used;
+      if (found) break;
+      if (stalled) {
         if (++spins > kSpinLimit) {
           atomicOr(error, kErrLookbackTimeout);
           break;
         }
         __nanosleep(20);
-        continue;
       }
-      exclusive += s & kMask;
-      if (flag == kFlagP) break;
-      --t;
     }
     st_relaxed_u32(&my_status[d], kFlagP | (exclusive + block_count));
   }
@@ -229,6 +248,7 @@ __global__ void __launch_bounds__(kThreads) pass_kernel(const SortPlan *__restri
   }
 }
 
+// Keys per thread: 8 up to 2M keys, 16 above.
 inline uint32_t ipt_for(uint32_t capacity) { return capacity <= (1u << 21) ? 8u : 16u; }
 inline uint32_t tiles_for(uint32_t capacity) {
   uint32_t tile = kThreads * ipt_for(capacity);
@@ -250,8 +270,9 @@ void launch_sort(const SortBuffers &b, cudaStream_t stream) {
   uint32_t *hist = b.work + 64;
   uint32_t *status = b.work + 64 + 4 * 256;
   const uint32_t grid = tiles ? tiles : 1;
+  const uint32_t ipt = ipt_for(b.capacity);
   if (!b.hist) {
-    if (ipt_for(b.capacity) == 8)
+    if (ipt == 8)
       hist_kernel<8><<<grid, kThreads, 0, stream>>>(b.keys0, b.count, b.begin_bit, b.passes, hist);
     else
       hist_kernel<16><<<grid, kThreads, 0, stream>>>(b.keys0, b.count, b.begin_bit, b.passes, hist);
@@ -259,7 +280,7 @@ void launch_sort(const SortBuffers &b, cudaStream_t stream) {
   plan_kernel<<<1, kThreads, 0, stream>>>(b.count, b.hist ? b.hist : hist, b.passes, b.plan);
   for (uint32_t p = 0; p < b.passes; ++p) {
     uint32_t *st = status + (size_t)p * tiles * 256;
-    if (ipt_for(b.capacity) == 8)
+    if (ipt == 8)
       pass_kernel<8><<<grid, kThreads, 0, stream>>>(b.plan, p, b.begin_bit + 8 * p, b.keys0,
                                                     b.vals0, b.keys1, b.vals1, st, tickets + p,
                                                     b.error);

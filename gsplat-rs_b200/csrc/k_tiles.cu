@@ -1,4 +1,5 @@
-// K2: (tile, splat) pair emission, and the tile-range build.
+// K2: (tile, splat) pair emission, and the tile-range build. Tile ids are
+// global over the views of a batch: views[v].tile_base + local tile.
 //
 // Emission walks the depth-sorted visible ids. Each block takes the next
 // 1024 sorted positions from an atomic ticket, sums their tile counts (area
@@ -22,17 +23,26 @@ constexpr int kEmitIpt = 4;
 constexpr int kEmitItems = kEmitThreads * kEmitIpt;
 constexpr int kEmitWarps = kEmitThreads / 32;
 
-__global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b, uint32_t tiles_x) {
+__global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b) {
   __shared__ uint32_t s_incl[kEmitItems];
   __shared__ uint32_t s_id[kEmitItems];
   __shared__ uint2 s_rect[kEmitItems];
+  __shared__ uint16_t s_vi[kEmitItems];
   __shared__ uint32_t s_wsum[kEmitThreads / 32];
   __shared__ uint32_t s_hist[3][256];
   __shared__ uint32_t s_block;
   __shared__ unsigned long long s_prefix;
+  // View table columns: splat base, tile base, tiles per row.
+  extern __shared__ uint32_t s_views[];
+  uint32_t *s_vsb = s_views, *s_vtb = s_views + b.num_views, *s_vtx = s_views + 2 * b.num_views;
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_block = atomicAdd(&b.counters->emit_ticket, 1u);
   for (uint32_t k = tid; k < 3 * 256; k += kEmitThreads) (&s_hist[0][0])[k] = 0;
+  for (uint32_t v = tid; v < b.num_views; v += kEmitThreads) {
+    s_vsb[v] = b.views[v].splat_base;
+    s_vtb[v] = b.views[v].tile_base;
+    s_vtx[v] = b.views[v].p.tiles_x;
+  }
   __syncthreads();
   const uint32_t V = b.counters->visible;
   const uint32_t block = s_block;
@@ -46,7 +56,7 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b, uint3
   for (int k = 0; k < kEmitIpt; ++k) {
     uint32_t slot = tid * kEmitIpt + k;
     uint32_t j = start + slot;
-    uint32_t id = 0, c = 0;
+    uint32_t id = 0, c = 0, vi = 0;
     uint2 r = make_uint2(0u, 0u);
     if (j < V) {
       id = ids[j];
@@ -54,9 +64,17 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b, uint3
       uint32_t w = (r.y & 0xffffu) - (r.x & 0xffffu);
       uint32_t h = (r.y >> 16) - (r.x >> 16);
       c = w * h;
+      uint32_t lo = 0, hi = b.num_views - 1;
+      while (lo < hi) {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (s_vsb[mid] <= id) lo = mid;
+        else hi = mid - 1;
+      }
+      vi = lo;
     }
     s_id[slot] = id;
     s_rect[slot] = r;
+    s_vi[slot] = (uint16_t)vi;
     cnt[k] = c;
     local += c;
   }
@@ -126,12 +144,25 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b, uint3
       uint32_t row = (uint32_t)((float)off * (1.0f / (float)w));
       if (row * w > off) --row;
       else if ((row + 1) * w <= off) ++row;
-      const uint32_t tile = (y0 + row) * tiles_x + x0 + (off - row * w);
+      const uint32_t vi = s_vi[item];
+      const uint32_t tile = s_vtb[vi] + (y0 + row) * s_vtx[vi] + x0 + (off - row * w);
       b.tile_keys[g] = tile;
       b.tile_vals[g] = s_id[item];
       atomicAdd(&s_hist[0][tile & 255u], 1u);
-      if (b.tile_passes > 1) atomicAdd(&s_hist[1][(tile >> 8) & 255u], 1u);
-      if (b.tile_passes > 2) atomicAdd(&s_hist[2][(tile >> 16) & 255u], 1u);
+      // The higher digits of a round's tiles are mostly equal: one add per
+      // distinct digit instead of up to 32 colliding ones.
+      const uint32_t act = __activemask();
+      const uint32_t lt = lanemask_lt();
+      if (b.tile_passes > 1) {
+        const uint32_t d1 = (tile >> 8) & 255u;
+        const uint32_t peers = __match_any_sync(act, d1);
+        if ((peers & lt) == 0) atomicAdd(&s_hist[1][d1], __popc(peers));
+      }
+      if (b.tile_passes > 2) {
+        const uint32_t d2 = (tile >> 16) & 255u;
+        const uint32_t peers = __match_any_sync(act, d2);
+        if ((peers & lt) == 0) atomicAdd(&s_hist[2][d2], __popc(peers));
+      }
     }
     it += __popc(__ballot_sync(0xffffffffu, inc_w <= round_end));
     k = round_end;
@@ -163,10 +194,10 @@ __global__ void fill_kernel(uint32_t *dst, uint32_t value, uint64_t count) {
 
 }  // namespace
 
-void launch_emit(const EmitBuffers &b, const FrameParams &p, cudaStream_t stream) {
+void launch_emit(const EmitBuffers &b, cudaStream_t stream) {
   uint32_t blocks = (b.n + kEmitItems - 1) / kEmitItems;
-  if (blocks == 0) return;
-  emit_kernel<<<blocks, kEmitThreads, 0, stream>>>(b, p.tiles_x);
+  if (blocks == 0 || b.num_views == 0) return;
+  emit_kernel<<<blocks, kEmitThreads, 3 * 4 * b.num_views, stream>>>(b);
 }
 
 void launch_ranges(const SortPlan *tile_plan, const uint32_t *keys0, const uint32_t *keys1,

@@ -9,24 +9,29 @@
 namespace gsr {
 
 struct SceneDev;
+struct ViewDev;
+struct ViewCounters;
 struct Record;
 struct ProjectedDev;
 struct FrameCounters;
 struct SortPlan;
 
 // ---- K1: preprocess -------------------------------------------------------
+// Splats are indexed by gid = views[v].splat_base + i across all views.
 struct K1Buffers {
-  uint32_t *vis_keys;          // [n] ~depth bits of visible splats, compacted
-  uint32_t *vis_ids;           // [n] their ids, ascending
-  uint2 *rects;                // [n] tile rect per visible splat
-  Record *records;             // [n] raster record per drawn splat
-  unsigned long long *status;  // [ceil(n/256)] look-back words, zeroed
+  uint32_t *vis_keys;          // [total splats] ~depth bits of visible splats, compacted
+  uint32_t *vis_ids;           // [total splats] their gids, view-major then ascending id
+  uint2 *rects;                // [gid] tile rect per visible splat
+  Record *records;             // [gid] raster record per drawn splat
+  unsigned long long *status;  // [total blocks] look-back words, zeroed
   FrameCounters *counters;
   uint32_t *key_hist;          // [4][256] digit histograms of the depth keys, zeroed
-  ProjectedDev *projected;     // [n] debug tap, or null
+  ViewCounters *view_counters; // [views], zeroed
+  ProjectedDev *projected;     // [gid] debug tap, or null
 };
-void launch_preprocess(const SceneDev &sc, const FrameParams &p, const K1Buffers &b, bool debug,
-                       cudaStream_t stream);
+uint32_t preprocess_blocks(uint32_t splats);  // blocks one view of `splats` splats needs
+void launch_preprocess(const ViewDev *views, uint32_t num_views, uint32_t total_blocks,
+                       uint32_t max_planes, const K1Buffers &b, bool debug, cudaStream_t stream);
 
 // ---- K3: onesweep LSD radix sort of (u32 key, u32 value) pairs -----------
 // Sorts ascending and stably over bits [begin_bit, begin_bit + 8*passes) of
@@ -54,17 +59,20 @@ void launch_sort(const SortBuffers &b, cudaStream_t stream);
 // ---- K2: tile-pair emission over the depth-sorted visible ids ------------
 struct EmitBuffers {
   const SortPlan *depth_plan;      // selects the buffer holding the sorted ids
-  const uint32_t *ids0, *ids1;     // depth-sorted ids, [visible]
-  const uint2 *rects;
-  uint32_t *tile_keys, *tile_vals; // [capacity] output pairs
+  const uint32_t *ids0, *ids1;     // depth-sorted gids, [visible]
+  const uint2 *rects;              // [gid]
+  uint32_t *tile_keys, *tile_vals; // [capacity] output pairs (global tile id, gid)
   uint64_t capacity;
-  unsigned long long *status;      // [ceil(n/1024)] look-back words, zeroed
+  unsigned long long *status;      // [ceil(total splats/1024)] look-back words, zeroed
   FrameCounters *counters;
   uint32_t *tile_hist;             // [passes][256] digit histograms of the tile ids, zeroed
   uint32_t tile_passes;
-  uint32_t n;                      // splat count (upper bound of visible)
+  uint32_t n;                      // total splats over the views (upper bound of visible)
+  const ViewDev *views;
+  uint32_t num_views;              // at most kMaxViewsPerLaunch
 };
-void launch_emit(const EmitBuffers &b, const FrameParams &p, cudaStream_t stream);
+constexpr uint32_t kMaxViewsPerLaunch = 1024;
+void launch_emit(const EmitBuffers &b, cudaStream_t stream);
 
 // ---- tile ranges from the tile-sorted keys -------------------------------
 void launch_ranges(const SortPlan *tile_plan, const uint32_t *keys0, const uint32_t *keys1,
@@ -72,10 +80,13 @@ void launch_ranges(const SortPlan *tile_plan, const uint32_t *keys0, const uint3
                    cudaStream_t stream);
 
 // ---- K4: tile raster ------------------------------------------------------
-void launch_raster(const FrameParams &p, const uint2 *ranges, const SortPlan *tile_plan,
-                   const uint32_t *ids0, const uint32_t *ids1, const Record *records,
-                   uint32_t *image, uint32_t blend_mode, const FrameCounters *counters,
-                   uint32_t *sticky, cudaStream_t stream);
+// One block per global tile of the batch; images holds every view's RGBA8
+// pixels at views[v].image_base.
+void launch_raster(const ViewDev *views, uint32_t num_views, uint32_t total_tiles, uint32_t tile,
+                   const uint2 *ranges, const SortPlan *tile_plan, const uint32_t *ids0,
+                   const uint32_t *ids1, const Record *records, uint32_t *images,
+                   uint32_t blend_mode, const FrameCounters *counters, uint32_t *sticky,
+                   cudaStream_t stream);
 
 // ---- small helpers ----------------------------------------------------------
 void launch_fill_u32(uint32_t *dst, uint32_t value, uint64_t count, cudaStream_t stream);

@@ -1,0 +1,503 @@
+// Host orchestration of the frame pipeline over a list of views (no device
+// code in this file).
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <string>
+
+#include "kernels.h"
+#include "pipeline.h"
+
+namespace gsr {
+
+#define GSR_CUDA(expr)                                                                    \
+  do {                                                                                    \
+    cudaError_t err__ = (expr);                                                           \
+    if (err__ != cudaSuccess)                                                             \
+      throw Error(Code::Internal, std::string("CUDA error: ") + cudaGetErrorString(err__) + \
+                                      " (" #expr ")");                                    \
+  } while (0)
+
+namespace {
+inline uint64_t align256(uint64_t v) { return (v + 255) & ~uint64_t(255); }
+constexpr uint64_t kMaxSortItems = (1u << 30) - 1;
+constexpr uint64_t kInitialPairsPerSplat = 16;
+}  // namespace
+
+DeviceBuffer::~DeviceBuffer() {
+  if (ptr_) cudaFree(ptr_);
+}
+
+void DeviceBuffer::reset(uint64_t bytes) {
+  if (ptr_) {
+    cudaFree(ptr_);
+    ptr_ = nullptr;
+    bytes_ = 0;
+  }
+  if (bytes == 0) return;
+  cudaError_t e = cudaMalloc(&ptr_, bytes);
+  if (e != cudaSuccess) {
+    ptr_ = nullptr;
+    cudaGetLastError();
+    throw Error(Code::Internal, "device allocation of " + std::to_string(bytes) +
+                                    " bytes failed: " + cudaGetErrorString(e));
+  }
+  bytes_ = bytes;
+}
+
+uint32_t tile_sort_passes(uint32_t num_tiles) {
+  uint32_t bits = 0;
+  while (bits < 32 && (1ull << bits) < num_tiles) ++bits;
+  return std::max(1u, (bits + 7) / 8);
+}
+
+std::unique_ptr<DeviceScene> upload_scene(const HostScene &s, cudaStream_t stream) {
+  const uint64_t n = s.size();
+  if (n > kMaxSortItems)
+    throw Error(Code::Unsupported, "scene has more splats than the renderer supports (2^30 - 1)");
+  ScenePacked packed;
+  pack_scene(s, packed);
+  auto sc = std::make_unique<DeviceScene>();
+  sc->n = (uint32_t)n;
+  sc->sh_degree = s.sh_degree;
+  sc->positions = s.positions;
+  // Three geometry planes, then the colour planes as one tight region so
+  // that plane p of splat i sits at color[p * n + i].
+  const uint64_t plane = align256(16 * std::max<uint64_t>(n, 1));
+  const uint64_t color_bytes = align256(16 * std::max<uint64_t>(n, 1) * packed.planes);
+  sc->mem.reset(3 * plane + color_bytes);
+  char *base = sc->mem.as<char>();
+  if (n) {
+    GSR_CUDA(cudaMemcpyAsync(base, packed.pos_alpha.data(), 16 * n, cudaMemcpyHostToDevice, stream));
+    GSR_CUDA(cudaMemcpyAsync(base + plane, packed.cov_a.data(), 16 * n, cudaMemcpyHostToDevice, stream));
+    GSR_CUDA(cudaMemcpyAsync(base + 2 * plane, packed.cov_b.data(), 16 * n, cudaMemcpyHostToDevice, stream));
+    GSR_CUDA(cudaMemcpyAsync(base + 3 * plane, packed.color.data(), 16 * n * packed.planes,
+                             cudaMemcpyHostToDevice, stream));
+  }
+  GSR_CUDA(cudaStreamSynchronize(stream));
+  sc->dev.pos_alpha = reinterpret_cast<const float4 *>(base);
+  sc->dev.cov_a = reinterpret_cast<const float4 *>(base + plane);
+  sc->dev.cov_b = reinterpret_cast<const float4 *>(base + 2 * plane);
+  sc->dev.color = reinterpret_cast<const float4 *>(base + 3 * plane);
+  sc->dev.n = (uint32_t)n;
+  sc->dev.planes = packed.planes;
+  return sc;
+}
+
+Pipeline::Pipeline(int device, cudaStream_t stream) : device_(device), stream_(stream) {
+  for (auto &ev : ev_) GSR_CUDA(cudaEventCreate(&ev));
+  for (auto &ev : slot_ev_) GSR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  GSR_CUDA(cudaMallocHost(&counters_host_, sizeof(FrameCounters)));
+  std::memset(counters_host_, 0, sizeof(FrameCounters));
+  // fixed scratch: [counters | key hist | tile hist] zeroed per run, then
+  // plans and the sticky word.
+  uint64_t off = 0;
+  const uint64_t o_counters = off; off += align256(sizeof(FrameCounters));
+  const uint64_t o_khist = off; off += align256(4 * 4 * 256);
+  const uint64_t o_thist = off; off += align256(4 * 4 * 256);
+  const uint64_t zero_end = off;
+  const uint64_t o_dplan = off; off += align256(sizeof(SortPlan));
+  const uint64_t o_tplan = off; off += align256(sizeof(SortPlan));
+  const uint64_t o_sticky = off; off += 256;
+  fixed_.reset(off);
+  GSR_CUDA(cudaMemset(fixed_.get(), 0, off));
+  counters_ = fixed_.as<FrameCounters>(o_counters);
+  key_hist_ = fixed_.as<uint32_t>(o_khist);
+  tile_hist_ = fixed_.as<uint32_t>(o_thist);
+  depth_plan_ = fixed_.as<SortPlan>(o_dplan);
+  tile_plan_ = fixed_.as<SortPlan>(o_tplan);
+  sticky_ = fixed_.as<uint32_t>(o_sticky);
+  (void)zero_end;
+}
+
+Pipeline::~Pipeline() {
+  cudaSetDevice(device_);
+  cudaStreamSynchronize(stream_);
+  drop_graph();
+  for (auto &ev : ev_)
+    if (ev) cudaEventDestroy(ev);
+  for (auto &ev : slot_ev_)
+    if (ev) cudaEventDestroy(ev);
+  if (counters_host_) cudaFreeHost(counters_host_);
+  if (view_counters_pinned_) cudaFreeHost(view_counters_pinned_);
+  if (views_pinned_) cudaFreeHost(views_pinned_);
+}
+
+void Pipeline::record(int k) {
+  if (capturing_)
+    GSR_CUDA(cudaEventRecordWithFlags(ev_[k], stream_, cudaEventRecordExternal));
+  else
+    GSR_CUDA(cudaEventRecord(ev_[k], stream_));
+}
+
+void Pipeline::drop_graph() {
+  if (graph_) {
+    cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+  }
+}
+
+Pipeline::Layout Pipeline::plan_views(const std::vector<ViewSpec> &views,
+                                      const std::vector<uint64_t> &image_bases) {
+  if (views.empty()) throw Error(Code::InvalidArgument, "no views to render");
+  if (views.size() > kMaxViewsPerLaunch)
+    throw Error(Code::Unsupported, "more than 1024 views in one pipeline run");
+  Layout l;
+  l.views = (uint32_t)views.size();
+  views_host_.resize(views.size());
+  uint64_t splats = 0, blocks = 0, tiles = 0;
+  for (size_t v = 0; v < views.size(); ++v) {
+    const ViewSpec &vs = views[v];
+    if (!camera_valid(vs.camera)) throw Error(Code::InvalidArgument, "invalid camera");
+    if (vs.width == 0 || vs.height == 0)
+      throw Error(Code::InvalidArgument, "invalid renderer configuration");
+    ViewDev &d = views_host_[v];
+    std::memset(&d, 0, sizeof(d));
+    d.p = make_frame_params(vs.camera, vs.width, vs.height, tile_, vs.scene->sh_degree,
+                            vs.scene->n);
+    d.sc = vs.scene->dev;
+    d.splat_base = (uint32_t)splats;
+    d.block_base = (uint32_t)blocks;
+    d.tile_base = (uint32_t)tiles;
+    d.image_base = image_bases[v];
+    splats += vs.scene->n;
+    blocks += preprocess_blocks(vs.scene->n);
+    tiles += d.p.num_tiles;
+    l.max_planes = std::max(l.max_planes, vs.scene->dev.planes);
+  }
+  if (splats > kMaxSortItems)
+    throw Error(Code::Unsupported, "splats over the views of one run exceed 2^30 - 1");
+  if (tiles > (1u << 24)) throw Error(Code::Unsupported, "too many tiles in one run");
+  l.total_splats = (uint32_t)splats;
+  l.total_blocks = (uint32_t)blocks;
+  l.total_tiles = (uint32_t)tiles;
+  l.tile_passes = tile_sort_passes(l.total_tiles);
+  return l;
+}
+
+void Pipeline::ensure_workspace(const Layout &l) {
+  const uint32_t n = std::max<uint32_t>(l.total_splats, 1);
+  if (l.views > view_cap_ || n > splat_cap_ || !view_ws_.get()) {
+    drop_graph();
+    const uint32_t vcap = std::max(l.views, view_cap_);
+    const uint32_t ncap = std::max(n, splat_cap_);
+    // view workspace: [view counters | K1 status | emit status] zeroed, then the table.
+    const uint64_t k1_words = (ncap + 255) / 256 + 1;  // + views: blocks round up per view
+    const uint64_t k1_total = k1_words + vcap;
+    const uint64_t emit_words = (ncap + 1023) / 1024;
+    uint64_t off = 0;
+    const uint64_t o_vc = off; off += align256(sizeof(ViewCounters) * vcap);
+    const uint64_t o_k1 = off; off += align256(8 * k1_total);
+    const uint64_t o_em = off; off += align256(8 * emit_words);
+    view_zero_bytes_ = off;
+    const uint64_t o_tab = off; off += align256(sizeof(ViewDev) * vcap);
+    view_ws_.reset(off);
+    view_counters_ = view_ws_.as<ViewCounters>(o_vc);
+    k1_status_ = view_ws_.as<unsigned long long>(o_k1);
+    emit_status_ = view_ws_.as<unsigned long long>(o_em);
+    views_dev_ = view_ws_.as<ViewDev>(o_tab);
+    view_cap_ = vcap;
+    if (view_counters_pinned_cap_ < vcap) {
+      // in-flight runs may still read or write the pinned host arrays
+      GSR_CUDA(cudaStreamSynchronize(stream_));
+      if (view_counters_pinned_) cudaFreeHost(view_counters_pinned_);
+      if (views_pinned_) cudaFreeHost(views_pinned_);
+      view_counters_pinned_ = nullptr;
+      views_pinned_ = nullptr;
+      GSR_CUDA(cudaMallocHost(&view_counters_pinned_, sizeof(ViewCounters) * vcap));
+      GSR_CUDA(cudaMallocHost(&views_pinned_, sizeof(ViewDev) * vcap * kViewSlots));
+      view_counters_pinned_cap_ = vcap;
+    }
+    if (n > splat_cap_) {
+      const uint64_t words = sort_work_words(ncap, 4);
+      off = 0;
+      uint64_t o_k0 = off; off += align256(4ull * ncap);
+      uint64_t o_v0 = off; off += align256(4ull * ncap);
+      uint64_t o_k1b = off; off += align256(4ull * ncap);
+      uint64_t o_v1 = off; off += align256(4ull * ncap);
+      uint64_t o_rect = off; off += align256(8ull * ncap);
+      uint64_t o_rec = off; off += align256(sizeof(Record) * (uint64_t)ncap);
+      uint64_t o_work = off; off += align256(4 * words);
+      splat_ws_.reset(0);
+      splat_ws_.reset(off);
+      vis_keys0_ = splat_ws_.as<uint32_t>(o_k0);
+      vis_vals0_ = splat_ws_.as<uint32_t>(o_v0);
+      vis_keys1_ = splat_ws_.as<uint32_t>(o_k1b);
+      vis_vals1_ = splat_ws_.as<uint32_t>(o_v1);
+      rects_ = splat_ws_.as<uint2>(o_rect);
+      records_ = splat_ws_.as<Record>(o_rec);
+      depth_sort_work_ = splat_ws_.as<uint32_t>(o_work);
+      splat_cap_ = ncap;
+      projected_.reset(0);
+    }
+  }
+  if (l.total_tiles > tile_cap_ || !tile_ws_.get()) {
+    drop_graph();
+    tile_cap_ = std::max(l.total_tiles, tile_cap_);
+    tile_ws_.reset(align256(8ull * std::max<uint32_t>(tile_cap_, 1)));
+    ranges_ = tile_ws_.as<uint2>();
+  }
+  if (key_cap_ == 0)
+    ensure_key_workspace(std::min<uint64_t>(std::max<uint64_t>(kInitialPairsPerSplat * n, 1u << 20),
+                                            kMaxSortItems));
+  if (debug_) {
+    const uint64_t need = sizeof(ProjectedDev) * (uint64_t)splat_cap_;
+    if (projected_.size() < need) {
+      drop_graph();
+      projected_.reset(need);
+    }
+    if (debug_pairs_.size() < 8 * key_cap_) {
+      drop_graph();
+      debug_pairs_.reset(8 * key_cap_);
+    }
+  }
+}
+
+void Pipeline::ensure_key_workspace(uint64_t capacity) {
+  const uint32_t passes = 3;  // enough for any tile count below 2^24
+  if (key_cap_ >= capacity && key_ws_.get()) return;
+  if (capacity > kMaxSortItems)
+    throw Error(Code::Unsupported, "tile pair count " + std::to_string(capacity) +
+                                       " exceeds the renderer's limit of 2^30 - 1");
+  drop_graph();
+  const uint32_t cap = (uint32_t)capacity;
+  const uint64_t words = sort_work_words(cap, passes);
+  uint64_t off = 0;
+  uint64_t o_k0 = off; off += align256(4ull * cap);
+  uint64_t o_v0 = off; off += align256(4ull * cap);
+  uint64_t o_k1 = off; off += align256(4ull * cap);
+  uint64_t o_v1 = off; off += align256(4ull * cap);
+  uint64_t o_work = off; off += align256(4 * words);
+  key_ws_.reset(0);
+  key_ws_.reset(off);
+  tile_keys0_ = key_ws_.as<uint32_t>(o_k0);
+  tile_vals0_ = key_ws_.as<uint32_t>(o_v0);
+  tile_keys1_ = key_ws_.as<uint32_t>(o_k1);
+  tile_vals1_ = key_ws_.as<uint32_t>(o_v1);
+  tile_sort_work_ = key_ws_.as<uint32_t>(o_work);
+  key_cap_ = cap;
+  debug_pairs_.reset(0);
+}
+
+void Pipeline::launch_all(const Layout &l, uint32_t *images) {
+  const uint32_t n = std::max<uint32_t>(l.total_splats, 1);
+  GSR_CUDA(cudaMemsetAsync(fixed_.get(), 0,
+                           (char *)depth_plan_ - (char *)fixed_.get(), stream_));
+  GSR_CUDA(cudaMemsetAsync(view_ws_.get(), 0, view_zero_bytes_, stream_));
+  GSR_CUDA(cudaMemsetAsync(ranges_, 0, 8ull * l.total_tiles, stream_));
+  record(0);
+
+  K1Buffers k1{vis_keys0_, vis_vals0_, rects_, records_, k1_status_, counters_, key_hist_,
+               view_counters_, debug_ ? projected_.as<ProjectedDev>() : nullptr};
+  launch_preprocess(views_dev_, l.views, l.total_blocks, l.max_planes, k1, debug_, stream_);
+  record(1);
+
+  SortBuffers ds{vis_keys0_, vis_vals0_, vis_keys1_, vis_vals1_, &counters_->visible, n, 0, 4,
+                 depth_plan_, depth_sort_work_, &counters_->error, key_hist_};
+  launch_sort(ds, stream_);
+  record(2);
+
+  EmitBuffers eb{depth_plan_, vis_vals0_, vis_vals1_, rects_, tile_keys0_, tile_vals0_, key_cap_,
+                 emit_status_, counters_, tile_hist_, l.tile_passes, l.total_splats, views_dev_,
+                 l.views};
+  launch_emit(eb, stream_);
+  if (debug_) {
+    GSR_CUDA(cudaMemcpyAsync(debug_pairs_.as<uint32_t>(), tile_keys0_, 4 * key_cap_,
+                             cudaMemcpyDeviceToDevice, stream_));
+    GSR_CUDA(cudaMemcpyAsync(debug_pairs_.as<uint32_t>(4 * key_cap_), tile_vals0_, 4 * key_cap_,
+                             cudaMemcpyDeviceToDevice, stream_));
+  }
+  record(3);
+  SortBuffers ts{tile_keys0_, tile_vals0_, tile_keys1_, tile_vals1_, &counters_->pairs,
+                 (uint32_t)key_cap_, 0, l.tile_passes, tile_plan_, tile_sort_work_,
+                 &counters_->error, tile_hist_};
+  launch_sort(ts, stream_);
+  record(4);
+  launch_ranges(tile_plan_, tile_keys0_, tile_keys1_, counters_, (uint32_t)key_cap_, ranges_,
+                stream_);
+  record(5);
+  launch_raster(views_dev_, l.views, l.total_tiles, tile_, ranges_, tile_plan_, tile_vals0_,
+                tile_vals1_, records_, images, blend_mode_, counters_, sticky_, stream_);
+  record(6);
+  GSR_CUDA(cudaMemcpyAsync(counters_host_, counters_, sizeof(FrameCounters),
+                           cudaMemcpyDeviceToHost, stream_));
+  GSR_CUDA(cudaMemcpyAsync(view_counters_pinned_, view_counters_, sizeof(ViewCounters) * l.views,
+                           cudaMemcpyDeviceToHost, stream_));
+}
+
+void Pipeline::enqueue(const std::vector<ViewSpec> &views, uint32_t *images,
+                       const std::vector<uint64_t> &image_bases) {
+  GSR_CUDA(cudaSetDevice(device_));
+  const Layout l = plan_views(views, image_bases);
+  ensure_workspace(l);
+  // The view table goes up from a pinned ring slot, asynchronously; the
+  // slot's previous copy is long done in steady state.
+  GSR_CUDA(cudaEventSynchronize(slot_ev_[slot_]));
+  ViewDev *staged = views_pinned_ + (uint64_t)slot_ * view_cap_;
+  std::memcpy(staged, views_host_.data(), sizeof(ViewDev) * l.views);
+  GSR_CUDA(cudaMemcpyAsync(views_dev_, staged, sizeof(ViewDev) * l.views, cudaMemcpyHostToDevice,
+                           stream_));
+  GSR_CUDA(cudaEventRecord(slot_ev_[slot_], stream_));
+  slot_ = (slot_ + 1) % kViewSlots;
+  const bool graph_ok = graph_ && graph_layout_ == l && graph_images_ == images &&
+                        graph_key_cap_ == key_cap_ && graph_tile_ == tile_ &&
+                        graph_blend_ == blend_mode_ && graph_debug_ == debug_;
+  if (graph_ok) {
+    GSR_CUDA(cudaGraphLaunch(graph_, stream_));
+  } else if (use_graph_) {
+    drop_graph();
+    cudaGraph_t g = nullptr;
+    GSR_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    capturing_ = true;
+    try {
+      launch_all(l, images);
+    } catch (...) {
+      capturing_ = false;
+      cudaStreamEndCapture(stream_, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      throw;
+    }
+    capturing_ = false;
+    GSR_CUDA(cudaStreamEndCapture(stream_, &g));
+    cudaError_t e = cudaGraphInstantiate(&graph_, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      graph_ = nullptr;
+      throw Error(Code::Internal, std::string("CUDA graph instantiation failed: ") +
+                                      cudaGetErrorString(e));
+    }
+    graph_layout_ = l;
+    graph_images_ = images;
+    graph_key_cap_ = key_cap_;
+    graph_tile_ = tile_;
+    graph_blend_ = blend_mode_;
+    graph_debug_ = debug_;
+    GSR_CUDA(cudaGraphLaunch(graph_, stream_));
+  } else {
+    launch_all(l, images);
+  }
+  GSR_CUDA(cudaGetLastError());
+  last_layout_ = l;
+  has_run_ = true;
+}
+
+void Pipeline::collect(RunResult &r) {
+  float t[kPhaseCount];
+  for (int k = 0; k < kPhaseCount; ++k) GSR_CUDA(cudaEventElapsedTime(&t[k], ev_[k], ev_[k + 1]));
+  for (int k = 0; k < kPhaseCount; ++k) r.phase_ms[k] = t[k];
+  r.preprocess_ms = t[kPhasePreprocess];
+  r.sort_ms = t[kPhaseDepthSort] + t[kPhaseEmit] + t[kPhaseTileSort] + t[kPhaseRanges];
+  r.raster_ms = t[kPhaseRaster];
+  r.visible = counters_host_->visible;
+  r.drawn = counters_host_->drawn;
+  r.keys = counters_host_->keys;
+  view_counters_host_.assign(view_counters_pinned_, view_counters_pinned_ + last_layout_.views);
+}
+
+RunResult Pipeline::run(const std::vector<ViewSpec> &views, uint32_t *images,
+                        const std::vector<uint64_t> &image_bases) {
+  auto t0 = std::chrono::steady_clock::now();
+  RunResult r;
+  for (;;) {
+    enqueue(views, images, image_bases);
+    GSR_CUDA(cudaStreamSynchronize(stream_));
+    if (counters_host_->error)
+      throw Error(Code::Internal, "device wait limit reached in a look-back scan (error bits " +
+                                      std::to_string(counters_host_->error) + ")");
+    if (!counters_host_->overflow) break;
+    // Grow the pair buffers to the exact need plus headroom and run again.
+    const uint64_t need = counters_host_->keys;
+    if (need > kMaxSortItems)
+      throw Error(Code::Unsupported, "tile pair count " + std::to_string(need) +
+                                         " exceeds the renderer's limit of 2^30 - 1");
+    ensure_key_workspace(std::min<uint64_t>(need + need / 4 + 1024, kMaxSortItems));
+    if (debug_) debug_pairs_.reset(8 * key_cap_);
+    ++r.reruns;
+  }
+  GSR_CUDA(cudaMemsetAsync(sticky_, 0, 4, stream_));
+  collect(r);
+  r.frame_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  last_ = r;
+  return r;
+}
+
+RunResult Pipeline::sync() {
+  GSR_CUDA(cudaSetDevice(device_));
+  uint32_t sticky = 0;
+  GSR_CUDA(cudaMemcpyAsync(&sticky, sticky_, 4, cudaMemcpyDeviceToHost, stream_));
+  GSR_CUDA(cudaMemsetAsync(sticky_, 0, 4, stream_));
+  GSR_CUDA(cudaStreamSynchronize(stream_));
+  RunResult r;
+  if (!has_run_) return r;
+  collect(r);
+  r.frame_ms = r.preprocess_ms + r.sort_ms + r.raster_ms;
+  last_ = r;
+  if (sticky & 0x7fffffffu)
+    throw Error(Code::Internal, "device wait limit reached in a look-back scan");
+  if (sticky & 0x80000000u)
+    throw Error(Code::Internal,
+                "an enqueued frame overflowed its tile-pair buffers; render it synchronously "
+                "once to size them");
+  return r;
+}
+
+SortPlan Pipeline::read_plan(int which) {
+  SortPlan plan;
+  GSR_CUDA(cudaMemcpyAsync(&plan, which == 0 ? depth_plan_ : tile_plan_, sizeof(SortPlan),
+                           cudaMemcpyDeviceToHost, stream_));
+  GSR_CUDA(cudaStreamSynchronize(stream_));
+  return plan;
+}
+
+std::vector<uint32_t> Pipeline::debug_order() {
+  GSR_CUDA(cudaSetDevice(device_));
+  SortPlan plan = read_plan(0);
+  std::vector<uint32_t> out(last_.visible);
+  if (!out.empty())
+    GSR_CUDA(cudaMemcpy(out.data(), plan.final_buffer == 0 ? vis_vals0_ : vis_vals1_,
+                        4 * out.size(), cudaMemcpyDeviceToHost));
+  return out;
+}
+
+std::vector<ProjectedDev> Pipeline::debug_projected(uint32_t count) {
+  if (!debug_ || !projected_.get())
+    throw Error(Code::InvalidArgument, "debug taps were not enabled for the last frame");
+  GSR_CUDA(cudaSetDevice(device_));
+  std::vector<ProjectedDev> out(count);
+  if (count)
+    GSR_CUDA(cudaMemcpy(out.data(), projected_.get(), sizeof(ProjectedDev) * count,
+                        cudaMemcpyDeviceToHost));
+  return out;
+}
+
+void Pipeline::debug_tile_pairs(std::vector<uint32_t> &tiles, std::vector<uint32_t> &ids) {
+  if (!debug_ || !debug_pairs_.get())
+    throw Error(Code::InvalidArgument, "debug taps were not enabled for the last frame");
+  GSR_CUDA(cudaSetDevice(device_));
+  const uint64_t k = std::min<uint64_t>(last_.keys, key_cap_);
+  tiles.resize(k);
+  ids.resize(k);
+  if (k) {
+    GSR_CUDA(cudaMemcpy(tiles.data(), debug_pairs_.get(), 4 * k, cudaMemcpyDeviceToHost));
+    GSR_CUDA(cudaMemcpy(ids.data(), debug_pairs_.as<uint32_t>(4 * key_cap_), 4 * k,
+                        cudaMemcpyDeviceToHost));
+  }
+}
+
+void Pipeline::debug_tile_ranges(uint32_t num_tiles, std::vector<uint32_t> &ranges,
+                                 std::vector<uint32_t> &ids) {
+  GSR_CUDA(cudaSetDevice(device_));
+  SortPlan plan = read_plan(1);
+  ranges.resize(2ull * num_tiles);
+  if (num_tiles)
+    GSR_CUDA(cudaMemcpy(ranges.data(), ranges_, 4 * ranges.size(), cudaMemcpyDeviceToHost));
+  const uint64_t k = std::min<uint64_t>(last_.keys, key_cap_);
+  ids.resize(k);
+  if (k)
+    GSR_CUDA(cudaMemcpy(ids.data(), plan.final_buffer == 0 ? tile_vals0_ : tile_vals1_, 4 * k,
+                        cudaMemcpyDeviceToHost));
+}
+
+}  // namespace gsr

@@ -1,0 +1,171 @@
+// The frame pipeline over a list of views (a plain frame is one view):
+// K1 -> depth sort -> K2 -> tile sort -> ranges -> K4 on one CUDA stream.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <memory>
+#include <vector>
+
+#include "device_types.h"
+#include "gsr_host.h"
+
+namespace gsr {
+
+// One device allocation, freed on destruction.
+class DeviceBuffer {
+ public:
+  DeviceBuffer() = default;
+  ~DeviceBuffer();
+  DeviceBuffer(const DeviceBuffer &) = delete;
+  DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+  void reset(uint64_t bytes);  // frees, then allocates `bytes` (0 = free only)
+  void *get() const { return ptr_; }
+  uint64_t size() const { return bytes_; }
+  template <typename T>
+  T *as(uint64_t byte_offset = 0) const {
+    return reinterpret_cast<T *>(static_cast<char *>(ptr_) + byte_offset);
+  }
+
+ private:
+  void *ptr_ = nullptr;
+  uint64_t bytes_ = 0;
+};
+
+// Scene resident in HBM (SoA float4 planes, see device_types.h SceneDev).
+struct DeviceScene {
+  DeviceBuffer mem;
+  SceneDev dev{};
+  uint32_t n = 0;
+  uint32_t sh_degree = 0;
+  std::vector<float> positions;  // host copy for automatic camera framing
+  uint64_t bytes() const { return mem.size(); }
+};
+std::unique_ptr<DeviceScene> upload_scene(const HostScene &s, cudaStream_t stream);
+
+// Device-timed phases of one run (CUDA events on the pipeline's stream).
+enum Phase : int { kPhasePreprocess, kPhaseDepthSort, kPhaseEmit, kPhaseTileSort, kPhaseRanges,
+                   kPhaseRaster, kPhaseCount };
+
+struct ViewSpec {
+  const DeviceScene *scene;
+  GsplatCamera camera;
+  uint32_t width, height;
+};
+
+struct RunResult {
+  float phase_ms[kPhaseCount] = {};
+  float preprocess_ms = 0, sort_ms = 0, raster_ms = 0, frame_ms = 0;
+  uint64_t visible = 0, drawn = 0, keys = 0;
+  uint32_t reruns = 0;
+};
+
+class Pipeline {
+ public:
+  Pipeline(int device, cudaStream_t stream);
+  ~Pipeline();
+
+  void set_tile(uint32_t tile) { tile_ = tile; }
+  uint32_t tile() const { return tile_; }
+  void set_blend_mode(uint32_t mode) { blend_mode_ = mode; }
+  uint32_t blend_mode() const { return blend_mode_; }
+  void set_debug(bool on) { debug_ = on; }
+  bool debug() const { return debug_; }
+  void set_use_graph(bool on) { use_graph_ = on; }
+
+  // Renders `views` into `images` (device, RGBA8 words) at the given pixel
+  // offsets and waits. Grows the pair buffers and re-runs on overflow.
+  RunResult run(const std::vector<ViewSpec> &views, uint32_t *images,
+                const std::vector<uint64_t> &image_bases);
+  // Enqueues without waiting (pair capacity as sized by earlier runs);
+  // errors and overflow of enqueued runs surface at sync().
+  void enqueue(const std::vector<ViewSpec> &views, uint32_t *images,
+               const std::vector<uint64_t> &image_bases);
+  RunResult sync();
+
+  uint64_t key_capacity() const { return key_cap_; }
+  const std::vector<ViewCounters> &view_counters() const { return view_counters_host_; }
+
+  // Debug taps of the last run (valid until the next run).
+  std::vector<uint32_t> debug_order();
+  std::vector<ProjectedDev> debug_projected(uint32_t count);
+  void debug_tile_pairs(std::vector<uint32_t> &tiles, std::vector<uint32_t> &ids);
+  void debug_tile_ranges(uint32_t num_tiles, std::vector<uint32_t> &ranges,
+                         std::vector<uint32_t> &ids);
+
+ private:
+  struct Layout {
+    uint32_t views = 0, total_splats = 0, total_blocks = 0, total_tiles = 0, max_planes = 1;
+    uint32_t tile_passes = 1;
+    bool operator==(const Layout &o) const {
+      return views == o.views && total_splats == o.total_splats &&
+             total_blocks == o.total_blocks && total_tiles == o.total_tiles &&
+             max_planes == o.max_planes && tile_passes == o.tile_passes;
+    }
+  };
+  Layout plan_views(const std::vector<ViewSpec> &views, const std::vector<uint64_t> &image_bases);
+  void ensure_workspace(const Layout &l);
+  void ensure_key_workspace(uint64_t capacity);
+  void launch_all(const Layout &l, uint32_t *images);
+  void collect(RunResult &r);
+  SortPlan read_plan(int which);
+  void drop_graph();
+  void record(int k);  // phase event k (a graph node while capturing)
+
+  int device_;
+  cudaStream_t stream_;
+  cudaEvent_t ev_[kPhaseCount + 1] = {};
+  uint32_t tile_ = 16, blend_mode_ = 0;
+  bool debug_ = false, use_graph_ = true, has_run_ = false, capturing_ = false;
+  Layout last_layout_;
+  RunResult last_;
+  std::vector<ViewDev> views_host_;
+  std::vector<ViewCounters> view_counters_host_;
+
+  // Fixed-size scratch: counters, plans, histograms, sticky word; zeroed
+  // region first (one memset per run).
+  DeviceBuffer fixed_;
+  FrameCounters *counters_ = nullptr;
+  uint32_t *key_hist_ = nullptr, *tile_hist_ = nullptr, *sticky_ = nullptr;
+  SortPlan *depth_plan_ = nullptr, *tile_plan_ = nullptr;
+  FrameCounters *counters_host_ = nullptr;  // pinned
+  // Per-layout scratch.
+  DeviceBuffer view_ws_;  // view table + view counters + look-back words (zeroed part)
+  uint64_t view_zero_bytes_ = 0;
+  ViewDev *views_dev_ = nullptr;
+  ViewCounters *view_counters_ = nullptr;
+  unsigned long long *k1_status_ = nullptr, *emit_status_ = nullptr;
+  uint32_t view_cap_ = 0, splat_cap_ = 0, tile_cap_ = 0;
+  DeviceBuffer splat_ws_;
+  uint32_t *vis_keys0_ = nullptr, *vis_vals0_ = nullptr, *vis_keys1_ = nullptr,
+           *vis_vals1_ = nullptr, *depth_sort_work_ = nullptr;
+  uint2 *rects_ = nullptr;
+  Record *records_ = nullptr;
+  DeviceBuffer projected_;
+  DeviceBuffer tile_ws_;
+  uint2 *ranges_ = nullptr;
+  DeviceBuffer key_ws_;
+  uint64_t key_cap_ = 0;
+  uint32_t *tile_keys0_ = nullptr, *tile_vals0_ = nullptr, *tile_keys1_ = nullptr,
+           *tile_vals1_ = nullptr, *tile_sort_work_ = nullptr;
+  DeviceBuffer debug_pairs_;
+  ViewCounters *view_counters_pinned_ = nullptr;
+  uint32_t view_counters_pinned_cap_ = 0;
+  // Pinned staging ring for the view table: slot s is rewritten only after
+  // the copy that last read it has completed (slot_ev_[s]).
+  static constexpr int kViewSlots = 4;
+  ViewDev *views_pinned_ = nullptr;
+  cudaEvent_t slot_ev_[kViewSlots] = {};
+  int slot_ = 0;
+  // CUDA graph of launch_all for the current layout and buffers.
+  cudaGraphExec_t graph_ = nullptr;
+  Layout graph_layout_;
+  uint32_t *graph_images_ = nullptr;
+  uint64_t graph_key_cap_ = 0;
+  uint32_t graph_tile_ = 0, graph_blend_ = 0;
+  bool graph_debug_ = false;
+};
+
+uint32_t tile_sort_passes(uint32_t num_tiles);
+
+}  // namespace gsr

@@ -148,6 +148,7 @@ _SIGS = [
     ("gsplat_context_set_blend_mode", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
     ("gsplat_context_set_tile_size", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
     ("gsplat_context_set_debug_taps", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
+    ("gsplat_context_set_cuda_graph", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
     ("gsplat_context_load_scene_buffers", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.POINTER(GsplatSceneDesc)]),
     ("gsplat_context_readback_rgba8", ctypes.c_int32, [ctypes.c_void_p, _u8p, ctypes.c_uint64]),
@@ -288,6 +289,9 @@ class Context:
 
     def set_debug_taps(self, on=True):
         check(lib().gsplat_context_set_debug_taps(self.ptr, 1 if on else 0))
+
+    def set_cuda_graph(self, on=True):
+        check(lib().gsplat_context_set_cuda_graph(self.ptr, 1 if on else 0))
 
     def load_scene_path(self, path):
         check(lib().gsplat_context_load_scene_path(self.ptr, os.fsencode(path)))

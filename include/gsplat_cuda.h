@@ -89,6 +89,11 @@ int32_t gsplat_context_set_tile_size(GsplatContext *ctx, uint32_t tile);
 /* When enabled, render_frame also keeps the per-splat projected records for
  * gsplat_context_debug_projected. Off by default. */
 int32_t gsplat_context_set_debug_taps(GsplatContext *ctx, uint32_t enabled);
+/* When enabled (the default), a frame's launches are captured once into a
+ * CUDA graph and replayed while the image size, tile size, blend mode, debug
+ * taps and pair capacity stay the same; disabled, every launch is issued
+ * separately. Images are identical either way. */
+int32_t gsplat_context_set_cuda_graph(GsplatContext *ctx, uint32_t enabled);
 
 /* Load a scene from host memory (validated like SceneBuffers::validate,
  * crates/gsplat-core/src/lib.rs:224-276). Replaces any loaded scene. */
