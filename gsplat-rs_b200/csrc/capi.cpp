@@ -11,6 +11,7 @@
 #include "../../include/gsplat.h"
 #include "../../include/gsplat_cuda.h"
 #include "gsr_host.h"
+#include "batch.h"
 #include "renderer.h"
 #include "sort_api.h"
 
@@ -22,6 +23,10 @@ struct GsplatContext {
   GsplatCamera camera;
   std::unique_ptr<gsr::Renderer> renderer;
   GsplatStats stats;
+};
+
+struct GsplatBatch {
+  std::unique_ptr<gsr::Batch> batch;
 };
 
 struct GsplatHostScene {
@@ -56,6 +61,19 @@ int32_t guarded(const char *op, F &&body) {
   } catch (...) {
     return fail(Code::Internal, std::string(op) + ": exception caught at C ABI boundary");
   }
+}
+
+// str::from_utf8 check of the reference (lib.rs:481-489).
+bool valid_utf8(const std::string &p) {
+  for (size_t i = 0; i < p.size();) {
+    unsigned char c = (unsigned char)p[i];
+    size_t len = c < 0x80 ? 1 : (c >> 5) == 6 ? 2 : (c >> 4) == 14 ? 3 : (c >> 3) == 30 ? 4 : 0;
+    bool good = len != 0 && i + len <= p.size();
+    for (size_t k = 1; good && k < len; ++k) good = ((unsigned char)p[i + k] & 0xC0) == 0x80;
+    if (!good) return false;
+    i += len;
+  }
+  return true;
 }
 
 gsr::HostScene host_scene_from_desc(const GsplatSceneDesc &d) {
@@ -164,17 +182,8 @@ int32_t gsplat_context_load_scene_path(GsplatContext *ctx, const char *path) {
     if (!ctx) return fail(Code::InvalidArgument, "gsplat_context_load_scene_path: ctx is null");
     if (!path) return fail(Code::InvalidArgument, "gsplat_context_load_scene_path: path is null");
     std::string p(path);
-    // str::from_utf8 check of the reference (lib.rs:481-489)
-    for (size_t i = 0; i < p.size();) {
-      unsigned char c = (unsigned char)p[i];
-      size_t len = c < 0x80 ? 1 : (c >> 5) == 6 ? 2 : (c >> 4) == 14 ? 3 : (c >> 3) == 30 ? 4 : 0;
-      bool good = len != 0 && i + len <= p.size();
-      for (size_t k = 1; good && k < len; ++k) good = ((unsigned char)p[i + k] & 0xC0) == 0x80;
-      if (!good)
-        return fail(Code::InvalidArgument,
-                    "gsplat_context_load_scene_path: path is not valid UTF-8");
-      i += len;
-    }
+    if (!valid_utf8(p))
+      return fail(Code::InvalidArgument, "gsplat_context_load_scene_path: path is not valid UTF-8");
     gsr::HostScene s = gsr::load_ply(p);
     ctx->renderer->load_scene(s);
     return ok();
@@ -561,6 +570,160 @@ int32_t gsplat_cuda_device_info(char *name, uint64_t name_capacity, int32_t *sm_
                                 int32_t *cc_major, int32_t *cc_minor) {
   return guarded("gsplat_cuda_device_info", [&]() -> int32_t {
     gsr::device_info(name, name_capacity, sm_count, cc_major, cc_minor);
+    return ok();
+  });
+}
+
+// ---- batched frames (gsplat_cuda.h) ----------------------------------------
+
+int32_t gsplat_batch_create(GsplatBatch **out_batch) {
+  return guarded("gsplat_batch_create", [&]() -> int32_t {
+    if (!out_batch) return fail(Code::InvalidArgument, "gsplat_batch_create: out_batch is null");
+    *out_batch = nullptr;
+    auto b = std::make_unique<GsplatBatch>();
+    b->batch = std::make_unique<gsr::Batch>();
+    *out_batch = b.release();
+    return ok();
+  });
+}
+
+void gsplat_batch_destroy(GsplatBatch *batch) {
+  try {
+    delete batch;
+  } catch (...) {
+  }
+}
+
+#define GSR_BATCH_CHECK(op) \
+  if (!batch || !batch->batch) return fail(Code::InvalidArgument, op ": batch is null")
+
+int32_t gsplat_batch_set_scene_budget(GsplatBatch *batch, uint64_t bytes) {
+  return guarded("gsplat_batch_set_scene_budget", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_set_scene_budget");
+    batch->batch->scenes().set_budget(bytes);
+    return ok();
+  });
+}
+
+int32_t gsplat_batch_add_scene_buffers(GsplatBatch *batch, const GsplatSceneDesc *scene,
+                                       uint32_t *out_scene) {
+  return guarded("gsplat_batch_add_scene_buffers", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_add_scene_buffers");
+    if (!scene || !out_scene)
+      return fail(Code::InvalidArgument, "gsplat_batch_add_scene_buffers: null argument");
+    gsr::HostScene s = host_scene_from_desc(*scene);
+    *out_scene = batch->batch->scenes().add(s, batch->batch->stream());
+    return ok();
+  });
+}
+
+int32_t gsplat_batch_add_scene_path(GsplatBatch *batch, const char *path, uint32_t *out_scene) {
+  return guarded("gsplat_batch_add_scene_path", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_add_scene_path");
+    if (!path || !out_scene)
+      return fail(Code::InvalidArgument, "gsplat_batch_add_scene_path: null argument");
+    std::string p(path);
+    if (!valid_utf8(p))
+      return fail(Code::InvalidArgument, "gsplat_batch_add_scene_path: path is not valid UTF-8");
+    gsr::HostScene s = gsr::load_ply(p);
+    *out_scene = batch->batch->scenes().add(s, batch->batch->stream());
+    return ok();
+  });
+}
+
+int32_t gsplat_batch_set_tile_size(GsplatBatch *batch, uint32_t tile) {
+  return guarded("gsplat_batch_set_tile_size", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_set_tile_size");
+    batch->batch->set_tile(tile);
+    return ok();
+  });
+}
+
+int32_t gsplat_batch_set_blend_mode(GsplatBatch *batch, uint32_t mode) {
+  return guarded("gsplat_batch_set_blend_mode", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_set_blend_mode");
+    batch->batch->set_blend_mode(mode);
+    return ok();
+  });
+}
+
+int32_t gsplat_batch_set_limits(GsplatBatch *batch, uint32_t max_views, uint64_t max_pairs,
+                                uint64_t max_splats) {
+  return guarded("gsplat_batch_set_limits", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_set_limits");
+    gsr::GroupLimits l = batch->batch->limits();
+    if (max_views) l.max_views = max_views;
+    if (max_pairs) l.max_pairs = max_pairs;
+    if (max_splats) l.max_splats = max_splats;
+    batch->batch->set_limits(l);
+    return ok();
+  });
+}
+
+int32_t gsplat_batch_render(GsplatBatch *batch, const GsplatBatchView *views, uint32_t count) {
+  return guarded("gsplat_batch_render", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_render");
+    if (!views || count == 0) return fail(Code::InvalidArgument, "gsplat_batch_render: no views");
+    std::vector<gsr::BatchView> v(count);
+    for (uint32_t i = 0; i < count; ++i) {
+      if (views[i].reserved != 0)
+        return fail(Code::InvalidArgument, "gsplat_batch_render: reserved field must be 0");
+      v[i] = gsr::BatchView{views[i].scene, views[i].camera, views[i].width, views[i].height};
+    }
+    batch->batch->render(v);
+    return ok();
+  });
+}
+
+int32_t gsplat_batch_get_times(const GsplatBatch *batch, GsplatBatchTimes *out_times) {
+  return guarded("gsplat_batch_get_times", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_get_times");
+    if (!out_times) return fail(Code::InvalidArgument, "gsplat_batch_get_times: out_times is null");
+    const gsr::BatchResult &r = batch->batch->last();
+    *out_times = GsplatBatchTimes{r.device_ms, r.wall_ms, r.groups, r.reruns, r.launches, 0, r.pairs};
+    return ok();
+  });
+}
+
+int32_t gsplat_batch_get_view_stats(const GsplatBatch *batch, uint32_t view,
+                                    GsplatBatchViewStats *out_stats) {
+  return guarded("gsplat_batch_get_view_stats", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_get_view_stats");
+    if (!out_stats)
+      return fail(Code::InvalidArgument, "gsplat_batch_get_view_stats: out_stats is null");
+    const gsr::ViewCounters &c = batch->batch->view_stats(view);
+    *out_stats = GsplatBatchViewStats{c.visible, c.drawn, c.pairs, batch->batch->view_group(view)};
+    return ok();
+  });
+}
+
+int32_t gsplat_batch_readback_rgba8(GsplatBatch *batch, uint32_t view, uint8_t *out,
+                                    uint64_t out_len) {
+  return guarded("gsplat_batch_readback_rgba8", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_readback_rgba8");
+    if (!out) return fail(Code::InvalidArgument, "gsplat_batch_readback_rgba8: out is null");
+    batch->batch->readback_rgba8(view, out, out_len);
+    return ok();
+  });
+}
+
+int32_t gsplat_batch_image_device(const GsplatBatch *batch, uint32_t view, const void **out_ptr,
+                                  uint64_t *out_bytes) {
+  return guarded("gsplat_batch_image_device", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_image_device");
+    if (!out_ptr || !out_bytes)
+      return fail(Code::InvalidArgument, "gsplat_batch_image_device: null argument");
+    *out_ptr = batch->batch->image_device(view, out_bytes);
+    return ok();
+  });
+}
+
+int32_t gsplat_batch_get_stream(const GsplatBatch *batch, void **out_stream) {
+  return guarded("gsplat_batch_get_stream", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_get_stream");
+    if (!out_stream)
+      return fail(Code::InvalidArgument, "gsplat_batch_get_stream: out_stream is null");
+    *out_stream = (void *)batch->batch->stream();
     return ok();
   });
 }

@@ -80,9 +80,9 @@ struct ViewDev {
 
 // Per-view counters of a batch (zeroed per batch).
 struct ViewCounters {
-  uint32_t visible;
-  uint32_t drawn;
-  uint32_t pairs;
+  uint32_t visible;  // depth-visible splats
+  uint32_t drawn;    // splats with a raster record
+  uint32_t pairs;    // tile pairs the view emits (sum of its splats' tile-rect areas)
   uint32_t pad;
 };
 

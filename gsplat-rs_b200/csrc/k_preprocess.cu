@@ -312,11 +312,13 @@ __global__ void __launch_bounds__(kK1Threads) preprocess_kernel(const ViewDev *_
     *dbg = z;
   }
   const uint32_t key = ~__float_as_uint(fmaxf(depth, 0.0f));
+  uint32_t area = 0;  // tile pairs this splat will emit
   if (vis) {
     Record rec;
     uint2 rect = make_uint2(0u, 0u);
     bool drawn = project<kPlanes>(sc, p, i, pa, rel, depth, rec, rect, dbg);
     b.rects[gid] = rect;
+    area = ((rect.y & 0xffffu) - (rect.x & 0xffffu)) * ((rect.y >> 16) - (rect.x >> 16));
     if (drawn) {
       b.records[gid] = rec;
       uint32_t dmask = __ballot_sync(__activemask(), true);
@@ -329,6 +331,9 @@ __global__ void __launch_bounds__(kK1Threads) preprocess_kernel(const ViewDev *_
 #pragma unroll
     for (int d = 0; d < 4; ++d) atomicAdd(&s_hist[d][(key >> (8 * d)) & 255u], 1u);
   }
+  // Per-view pair count (what K2 will emit for this view), one add per warp.
+  area = warp_sum(area);
+  if (lane == 0 && area) atomicAdd(&b.view_counters[view].pairs, area);
   // Every warp resolves the block's offset on its own (no second block
   // barrier); warp 0 publishes the inclusive prefix.
   const unsigned long long prefix = lookback_resolve(b.status, block, &b.counters->error);

@@ -7,17 +7,10 @@
 #include <string>
 
 #include "kernels.h"
+#include "cuda_check.h"
 #include "pipeline.h"
 
 namespace gsr {
-
-#define GSR_CUDA(expr)                                                                    \
-  do {                                                                                    \
-    cudaError_t err__ = (expr);                                                           \
-    if (err__ != cudaSuccess)                                                             \
-      throw Error(Code::Internal, std::string("CUDA error: ") + cudaGetErrorString(err__) + \
-                                      " (" #expr ")");                                    \
-  } while (0)
 
 namespace {
 inline uint64_t align256(uint64_t v) { return (v + 255) & ~uint64_t(255); }
@@ -50,6 +43,11 @@ uint32_t tile_sort_passes(uint32_t num_tiles) {
   uint32_t bits = 0;
   while (bits < 32 && (1ull << bits) < num_tiles) ++bits;
   return std::max(1u, (bits + 7) / 8);
+}
+
+uint64_t scene_device_bytes(const HostScene &s) {
+  const uint64_t n = std::max<uint64_t>(s.size(), 1);
+  return 3 * align256(16 * n) + align256(16 * n * color_planes(s.sh_degree));
 }
 
 std::unique_ptr<DeviceScene> upload_scene(const HostScene &s, cudaStream_t stream) {
@@ -132,22 +130,20 @@ void Pipeline::record(int k) {
 }
 
 void Pipeline::drop_graph() {
-  if (graph_) {
-    cudaGraphExecDestroy(graph_);
-    graph_ = nullptr;
-  }
+  for (auto &g : graphs_) cudaGraphExecDestroy(g.exec);
+  graphs_.clear();
 }
 
-Pipeline::Layout Pipeline::plan_views(const std::vector<ViewSpec> &views,
-                                      const std::vector<uint64_t> &image_bases) {
-  if (views.empty()) throw Error(Code::InvalidArgument, "no views to render");
-  if (views.size() > kMaxViewsPerLaunch)
+Pipeline::Layout Pipeline::plan_views(const ViewSpec *views, uint32_t count,
+                                      const uint64_t *image_bases) {
+  if (count == 0) throw Error(Code::InvalidArgument, "no views to render");
+  if (count > kMaxViewsPerLaunch)
     throw Error(Code::Unsupported, "more than 1024 views in one pipeline run");
   Layout l;
-  l.views = (uint32_t)views.size();
-  views_host_.resize(views.size());
+  l.views = count;
+  views_host_.resize(count);
   uint64_t splats = 0, blocks = 0, tiles = 0;
-  for (size_t v = 0; v < views.size(); ++v) {
+  for (uint32_t v = 0; v < count; ++v) {
     const ViewSpec &vs = views[v];
     if (!camera_valid(vs.camera)) throw Error(Code::InvalidArgument, "invalid camera");
     if (vs.width == 0 || vs.height == 0)
@@ -179,6 +175,7 @@ Pipeline::Layout Pipeline::plan_views(const std::vector<ViewSpec> &views,
 void Pipeline::ensure_workspace(const Layout &l) {
   const uint32_t n = std::max<uint32_t>(l.total_splats, 1);
   if (l.views > view_cap_ || n > splat_cap_ || !view_ws_.get()) {
+    GSR_CUDA(cudaStreamSynchronize(stream_));  // earlier runs may still use the old buffers
     drop_graph();
     const uint32_t vcap = std::max(l.views, view_cap_);
     const uint32_t ncap = std::max(n, splat_cap_);
@@ -233,6 +230,7 @@ void Pipeline::ensure_workspace(const Layout &l) {
     }
   }
   if (l.total_tiles > tile_cap_ || !tile_ws_.get()) {
+    GSR_CUDA(cudaStreamSynchronize(stream_));
     drop_graph();
     tile_cap_ = std::max(l.total_tiles, tile_cap_);
     tile_ws_.reset(align256(8ull * std::max<uint32_t>(tile_cap_, 1)));
@@ -244,10 +242,12 @@ void Pipeline::ensure_workspace(const Layout &l) {
   if (debug_) {
     const uint64_t need = sizeof(ProjectedDev) * (uint64_t)splat_cap_;
     if (projected_.size() < need) {
+      GSR_CUDA(cudaStreamSynchronize(stream_));
       drop_graph();
       projected_.reset(need);
     }
     if (debug_pairs_.size() < 8 * key_cap_) {
+      GSR_CUDA(cudaStreamSynchronize(stream_));
       drop_graph();
       debug_pairs_.reset(8 * key_cap_);
     }
@@ -260,6 +260,7 @@ void Pipeline::ensure_key_workspace(uint64_t capacity) {
   if (capacity > kMaxSortItems)
     throw Error(Code::Unsupported, "tile pair count " + std::to_string(capacity) +
                                        " exceeds the renderer's limit of 2^30 - 1");
+  GSR_CUDA(cudaStreamSynchronize(stream_));
   drop_graph();
   const uint32_t cap = (uint32_t)capacity;
   const uint64_t words = sort_work_words(cap, passes);
@@ -280,7 +281,7 @@ void Pipeline::ensure_key_workspace(uint64_t capacity) {
   debug_pairs_.reset(0);
 }
 
-void Pipeline::launch_all(const Layout &l, uint32_t *images) {
+void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &sinks) {
   const uint32_t n = std::max<uint32_t>(l.total_splats, 1);
   GSR_CUDA(cudaMemsetAsync(fixed_.get(), 0,
                            (char *)depth_plan_ - (char *)fixed_.get(), stream_));
@@ -320,17 +321,19 @@ void Pipeline::launch_all(const Layout &l, uint32_t *images) {
   launch_raster(views_dev_, l.views, l.total_tiles, tile_, ranges_, tile_plan_, tile_vals0_,
                 tile_vals1_, records_, images, blend_mode_, counters_, sticky_, stream_);
   record(6);
-  GSR_CUDA(cudaMemcpyAsync(counters_host_, counters_, sizeof(FrameCounters),
+  GSR_CUDA(cudaMemcpyAsync(sinks.counters, counters_, sizeof(FrameCounters),
                            cudaMemcpyDeviceToHost, stream_));
-  GSR_CUDA(cudaMemcpyAsync(view_counters_pinned_, view_counters_, sizeof(ViewCounters) * l.views,
+  GSR_CUDA(cudaMemcpyAsync(sinks.views, view_counters_, sizeof(ViewCounters) * l.views,
                            cudaMemcpyDeviceToHost, stream_));
 }
 
-void Pipeline::enqueue(const std::vector<ViewSpec> &views, uint32_t *images,
-                       const std::vector<uint64_t> &image_bases) {
+void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
+                       const uint64_t *image_bases, HostSinks sinks) {
   GSR_CUDA(cudaSetDevice(device_));
-  const Layout l = plan_views(views, image_bases);
+  const Layout l = plan_views(views, count, image_bases);
   ensure_workspace(l);
+  if (!sinks.counters) sinks.counters = counters_host_;
+  if (!sinks.views) sinks.views = view_counters_pinned_;
   // The view table goes up from a pinned ring slot, asynchronously; the
   // slot's previous copy is long done in steady state.
   GSR_CUDA(cudaEventSynchronize(slot_ev_[slot_]));
@@ -340,46 +343,52 @@ void Pipeline::enqueue(const std::vector<ViewSpec> &views, uint32_t *images,
                            stream_));
   GSR_CUDA(cudaEventRecord(slot_ev_[slot_], stream_));
   slot_ = (slot_ + 1) % kViewSlots;
-  const bool graph_ok = graph_ && graph_layout_ == l && graph_images_ == images &&
-                        graph_key_cap_ == key_cap_ && graph_tile_ == tile_ &&
-                        graph_blend_ == blend_mode_ && graph_debug_ == debug_;
-  if (graph_ok) {
-    GSR_CUDA(cudaGraphLaunch(graph_, stream_));
-  } else if (use_graph_) {
-    drop_graph();
-    cudaGraph_t g = nullptr;
-    GSR_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-    capturing_ = true;
-    try {
-      launch_all(l, images);
-    } catch (...) {
-      capturing_ = false;
-      cudaStreamEndCapture(stream_, &g);
-      if (g) cudaGraphDestroy(g);
-      cudaGetLastError();
-      throw;
-    }
-    capturing_ = false;
-    GSR_CUDA(cudaStreamEndCapture(stream_, &g));
-    cudaError_t e = cudaGraphInstantiate(&graph_, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) {
-      graph_ = nullptr;
-      throw Error(Code::Internal, std::string("CUDA graph instantiation failed: ") +
-                                      cudaGetErrorString(e));
-    }
-    graph_layout_ = l;
-    graph_images_ = images;
-    graph_key_cap_ = key_cap_;
-    graph_tile_ = tile_;
-    graph_blend_ = blend_mode_;
-    graph_debug_ = debug_;
-    GSR_CUDA(cudaGraphLaunch(graph_, stream_));
+
+  if (!use_graph_) {
+    launch_all(l, images, sinks);
   } else {
-    launch_all(l, images);
+    const GraphKey key{l, images, key_cap_, tile_, blend_mode_, debug_, sinks.counters, sinks.views};
+    GraphEntry *hit = nullptr;
+    for (auto &g : graphs_)
+      if (g.key == key) hit = &g;
+    if (!hit) {
+      if (graphs_.size() >= kGraphCacheSize) {
+        auto lru = std::min_element(graphs_.begin(), graphs_.end(),
+                                    [](const GraphEntry &a, const GraphEntry &b) {
+                                      return a.last_use < b.last_use;
+                                    });
+        cudaGraphExecDestroy(lru->exec);
+        graphs_.erase(lru);
+      }
+      cudaGraph_t g = nullptr;
+      GSR_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+      capturing_ = true;
+      try {
+        launch_all(l, images, sinks);
+      } catch (...) {
+        capturing_ = false;
+        cudaStreamEndCapture(stream_, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        throw;
+      }
+      capturing_ = false;
+      GSR_CUDA(cudaStreamEndCapture(stream_, &g));
+      cudaGraphExec_t exec = nullptr;
+      cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess)
+        throw Error(Code::Internal, std::string("CUDA graph instantiation failed: ") +
+                                        cudaGetErrorString(e));
+      graphs_.push_back(GraphEntry{key, exec, 0});
+      hit = &graphs_.back();
+    }
+    hit->last_use = ++graph_clock_;
+    GSR_CUDA(cudaGraphLaunch(hit->exec, stream_));
   }
   GSR_CUDA(cudaGetLastError());
   last_layout_ = l;
+  last_sinks_ = sinks;
   has_run_ = true;
 }
 
@@ -390,18 +399,18 @@ void Pipeline::collect(RunResult &r) {
   r.preprocess_ms = t[kPhasePreprocess];
   r.sort_ms = t[kPhaseDepthSort] + t[kPhaseEmit] + t[kPhaseTileSort] + t[kPhaseRanges];
   r.raster_ms = t[kPhaseRaster];
-  r.visible = counters_host_->visible;
-  r.drawn = counters_host_->drawn;
-  r.keys = counters_host_->keys;
-  view_counters_host_.assign(view_counters_pinned_, view_counters_pinned_ + last_layout_.views);
+  r.visible = last_sinks_.counters->visible;
+  r.drawn = last_sinks_.counters->drawn;
+  r.keys = last_sinks_.counters->keys;
+  view_counters_host_.assign(last_sinks_.views, last_sinks_.views + last_layout_.views);
 }
 
-RunResult Pipeline::run(const std::vector<ViewSpec> &views, uint32_t *images,
-                        const std::vector<uint64_t> &image_bases) {
+RunResult Pipeline::run(const ViewSpec *views, uint32_t count, uint32_t *images,
+                        const uint64_t *image_bases) {
   auto t0 = std::chrono::steady_clock::now();
   RunResult r;
   for (;;) {
-    enqueue(views, images, image_bases);
+    enqueue(views, count, images, image_bases);
     GSR_CUDA(cudaStreamSynchronize(stream_));
     if (counters_host_->error)
       throw Error(Code::Internal, "device wait limit reached in a look-back scan (error bits " +
@@ -441,6 +450,13 @@ RunResult Pipeline::sync() {
                 "an enqueued frame overflowed its tile-pair buffers; render it synchronously "
                 "once to size them");
   return r;
+}
+
+uint32_t Pipeline::launches_per_run() const {
+  // preprocess; depth sort plan + 4 passes (histograms come from K1); emit;
+  // tile sort plan + passes (histograms from K2); ranges; raster.
+  const uint32_t tile_passes = last_layout_.tile_passes;
+  return 1 + (1 + 4) + 1 + (1 + tile_passes) + 1 + 1;
 }
 
 SortPlan Pipeline::read_plan(int which) {

@@ -42,6 +42,8 @@ struct DeviceScene {
   uint64_t bytes() const { return mem.size(); }
 };
 std::unique_ptr<DeviceScene> upload_scene(const HostScene &s, cudaStream_t stream);
+// HBM bytes upload_scene allocates for `s`.
+uint64_t scene_device_bytes(const HostScene &s);
 
 // Device-timed phases of one run (CUDA events on the pipeline's stream).
 enum Phase : int { kPhasePreprocess, kPhaseDepthSort, kPhaseEmit, kPhaseTileSort, kPhaseRanges,
@@ -60,6 +62,12 @@ struct RunResult {
   uint32_t reruns = 0;
 };
 
+// Pinned host destinations of a run's counters (default: the pipeline's own).
+struct HostSinks {
+  FrameCounters *counters = nullptr;
+  ViewCounters *views = nullptr;  // one entry per view of the run
+};
+
 class Pipeline {
  public:
   Pipeline(int device, cudaStream_t stream);
@@ -73,17 +81,33 @@ class Pipeline {
   bool debug() const { return debug_; }
   void set_use_graph(bool on) { use_graph_ = on; }
 
-  // Renders `views` into `images` (device, RGBA8 words) at the given pixel
-  // offsets and waits. Grows the pair buffers and re-runs on overflow.
+  // Renders `count` views into `images` (device, RGBA8 words) at the given
+  // pixel offsets and waits. Grows the pair buffers and re-runs on overflow.
+  RunResult run(const ViewSpec *views, uint32_t count, uint32_t *images,
+                const uint64_t *image_bases);
   RunResult run(const std::vector<ViewSpec> &views, uint32_t *images,
-                const std::vector<uint64_t> &image_bases);
+                const std::vector<uint64_t> &image_bases) {
+    return run(views.data(), (uint32_t)views.size(), images, image_bases.data());
+  }
   // Enqueues without waiting (pair capacity as sized by earlier runs);
-  // errors and overflow of enqueued runs surface at sync().
+  // errors and overflow of enqueued runs surface at sync(), or in the
+  // counters written to `sinks` once the stream reaches them.
+  void enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
+               const uint64_t *image_bases, HostSinks sinks = {});
   void enqueue(const std::vector<ViewSpec> &views, uint32_t *images,
-               const std::vector<uint64_t> &image_bases);
+               const std::vector<uint64_t> &image_bases, HostSinks sinks = {}) {
+    enqueue(views.data(), (uint32_t)views.size(), images, image_bases.data(), sinks);
+  }
   RunResult sync();
+  // Grows the pair buffers to hold at least `pairs` tile pairs.
+  void reserve_pairs(uint64_t pairs) { ensure_key_workspace(pairs); }
 
   uint64_t key_capacity() const { return key_cap_; }
+  cudaStream_t stream() const { return stream_; }
+  int device() const { return device_; }
+  // Kernel launches of one run with the current settings (excluding copies
+  // and memsets).
+  uint32_t launches_per_run() const;
   const std::vector<ViewCounters> &view_counters() const { return view_counters_host_; }
 
   // Debug taps of the last run (valid until the next run).
@@ -103,10 +127,10 @@ class Pipeline {
              max_planes == o.max_planes && tile_passes == o.tile_passes;
     }
   };
-  Layout plan_views(const std::vector<ViewSpec> &views, const std::vector<uint64_t> &image_bases);
+  Layout plan_views(const ViewSpec *views, uint32_t count, const uint64_t *image_bases);
   void ensure_workspace(const Layout &l);
   void ensure_key_workspace(uint64_t capacity);
-  void launch_all(const Layout &l, uint32_t *images);
+  void launch_all(const Layout &l, uint32_t *images, const HostSinks &sinks);
   void collect(RunResult &r);
   SortPlan read_plan(int which);
   void drop_graph();
@@ -118,6 +142,7 @@ class Pipeline {
   uint32_t tile_ = 16, blend_mode_ = 0;
   bool debug_ = false, use_graph_ = true, has_run_ = false, capturing_ = false;
   Layout last_layout_;
+  HostSinks last_sinks_;
   RunResult last_;
   std::vector<ViewDev> views_host_;
   std::vector<ViewCounters> view_counters_host_;
@@ -157,13 +182,29 @@ class Pipeline {
   ViewDev *views_pinned_ = nullptr;
   cudaEvent_t slot_ev_[kViewSlots] = {};
   int slot_ = 0;
-  // CUDA graph of launch_all for the current layout and buffers.
-  cudaGraphExec_t graph_ = nullptr;
-  Layout graph_layout_;
-  uint32_t *graph_images_ = nullptr;
-  uint64_t graph_key_cap_ = 0;
-  uint32_t graph_tile_ = 0, graph_blend_ = 0;
-  bool graph_debug_ = false;
+  // CUDA graphs of launch_all, one per layout, buffer set and setting.
+  struct GraphKey {
+    Layout layout;
+    uint32_t *images;
+    uint64_t key_cap;
+    uint32_t tile, blend;
+    bool debug;
+    FrameCounters *host_counters;
+    ViewCounters *host_views;
+    bool operator==(const GraphKey &o) const {
+      return layout == o.layout && images == o.images && key_cap == o.key_cap &&
+             tile == o.tile && blend == o.blend && debug == o.debug &&
+             host_counters == o.host_counters && host_views == o.host_views;
+    }
+  };
+  struct GraphEntry {
+    GraphKey key;
+    cudaGraphExec_t exec;
+    uint64_t last_use;
+  };
+  static constexpr size_t kGraphCacheSize = 32;
+  std::vector<GraphEntry> graphs_;
+  uint64_t graph_clock_ = 0;
 };
 
 uint32_t tile_sort_passes(uint32_t num_tiles);

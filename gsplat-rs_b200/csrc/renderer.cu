@@ -2,17 +2,10 @@
 
 #include <string>
 
+#include "cuda_check.h"
 #include "renderer.h"
 
 namespace gsr {
-
-#define GSR_CUDA(expr)                                                                    \
-  do {                                                                                    \
-    cudaError_t err__ = (expr);                                                           \
-    if (err__ != cudaSuccess)                                                             \
-      throw Error(Code::Internal, std::string("CUDA error: ") + cudaGetErrorString(err__) + \
-                                      " (" #expr ")");                                    \
-  } while (0)
 
 int require_b200() {
   int count = 0;

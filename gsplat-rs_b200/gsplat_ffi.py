@@ -90,6 +90,23 @@ class GsplatFrameCounts(ctypes.Structure):
                 ("frame_reruns", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
+class GsplatBatchView(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_uint32), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("camera", GsplatCamera)]
+
+
+class GsplatBatchViewStats(ctypes.Structure):
+    _fields_ = [("visible_count", ctypes.c_uint32), ("drawn_count", ctypes.c_uint32),
+                ("tile_pairs", ctypes.c_uint32), ("group", ctypes.c_uint32)]
+
+
+class GsplatBatchTimes(ctypes.Structure):
+    _fields_ = [("device_ms", ctypes.c_float), ("wall_ms", ctypes.c_float),
+                ("groups", ctypes.c_uint32), ("reruns", ctypes.c_uint32),
+                ("kernel_launches", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("tile_pairs", ctypes.c_uint64)]
+
+
 PROJECTED_DTYPE = np.dtype([("center_ndc", "<f4", 2), ("axis_u", "<f4", 2), ("axis_v", "<f4", 2),
                             ("color", "<f4", 4), ("extent_scale", "<f4"), ("depth", "<f4"),
                             ("flags", "<u4"), ("tile_x0", "<u2"), ("tile_y0", "<u2"),
@@ -172,6 +189,27 @@ _SIGS = [
     ("gsplat_cuda_sort_pairs", ctypes.c_int32, [_u32p, _u32p, ctypes.c_uint64]),
     ("gsplat_cuda_sort_values_by_keys_noalloc", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
+    ("gsplat_batch_create", ctypes.c_int32, [ctypes.POINTER(ctypes.c_void_p)]),
+    ("gsplat_batch_destroy", None, [ctypes.c_void_p]),
+    ("gsplat_batch_set_scene_budget", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64]),
+    ("gsplat_batch_add_scene_buffers", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.POINTER(GsplatSceneDesc), _u32p]),
+    ("gsplat_batch_add_scene_path", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_char_p, _u32p]),
+    ("gsplat_batch_set_tile_size", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
+    ("gsplat_batch_set_blend_mode", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
+    ("gsplat_batch_set_limits", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64]),
+    ("gsplat_batch_render", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.POINTER(GsplatBatchView), ctypes.c_uint32]),
+    ("gsplat_batch_get_times", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(GsplatBatchTimes)]),
+    ("gsplat_batch_get_view_stats", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(GsplatBatchViewStats)]),
+    ("gsplat_batch_readback_rgba8", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_uint32, _u8p, ctypes.c_uint64]),
+    ("gsplat_batch_image_device", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p),
+      ctypes.POINTER(ctypes.c_uint64)]),
+    ("gsplat_batch_get_stream", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     ("gsplat_ply_load", ctypes.c_int32, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
     ("gsplat_host_scene_destroy", None, [ctypes.c_void_p]),
     ("gsplat_host_scene_view", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(GsplatSceneDesc)]),
@@ -375,6 +413,98 @@ class Context:
                                                      ids.ctypes.data_as(_u32p), ids.size,
                                                      ctypes.byref(n)))
         return r.reshape(-1, 2), ids[:n.value]
+
+
+class Batch:
+    """One GsplatBatch: resident scenes and many views rendered per call."""
+
+    def __init__(self):
+        self.ptr = ctypes.c_void_p()
+        check(lib().gsplat_batch_create(ctypes.byref(self.ptr)))
+        self.sizes = []
+
+    def close(self):
+        if self.ptr:
+            lib().gsplat_batch_destroy(self.ptr)
+            self.ptr = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_scene_budget(self, nbytes):
+        check(lib().gsplat_batch_set_scene_budget(self.ptr, int(nbytes)))
+
+    def add_scene(self, scene):
+        sd = SceneDesc(scene)
+        sid = ctypes.c_uint32()
+        check(lib().gsplat_batch_add_scene_buffers(self.ptr, ctypes.byref(sd.desc), ctypes.byref(sid)))
+        return sid.value
+
+    def add_scene_path(self, path):
+        sid = ctypes.c_uint32()
+        check(lib().gsplat_batch_add_scene_path(self.ptr, os.fsencode(path), ctypes.byref(sid)))
+        return sid.value
+
+    def set_tile_size(self, tile):
+        check(lib().gsplat_batch_set_tile_size(self.ptr, tile))
+
+    def set_blend_mode(self, mode):
+        check(lib().gsplat_batch_set_blend_mode(self.ptr, mode))
+
+    def set_limits(self, max_views=0, max_pairs=0, max_splats=0):
+        check(lib().gsplat_batch_set_limits(self.ptr, max_views, max_pairs, max_splats))
+
+    @staticmethod
+    def make_views(views):
+        """views: iterable of (scene, camera, width, height)."""
+        views = list(views)
+        arr = (GsplatBatchView * len(views))()
+        for k, (sid, cam, w, h) in enumerate(views):
+            arr[k].scene, arr[k].width, arr[k].height, arr[k].reserved = sid, w, h, 0
+            arr[k].camera = cam if isinstance(cam, GsplatCamera) else GsplatCamera.from_dict(cam)
+        return arr
+
+    def render(self, views):
+        arr = views if isinstance(views, ctypes.Array) else self.make_views(views)
+        check(lib().gsplat_batch_render(self.ptr, arr, len(arr)))
+        self.sizes = [(arr[k].width, arr[k].height) for k in range(len(arr))]
+        return self.times()
+
+    def times(self):
+        t = GsplatBatchTimes()
+        check(lib().gsplat_batch_get_times(self.ptr, ctypes.byref(t)))
+        return t
+
+    def view_stats(self, view):
+        s = GsplatBatchViewStats()
+        check(lib().gsplat_batch_get_view_stats(self.ptr, view, ctypes.byref(s)))
+        return s
+
+    def readback_rgba8(self, view, out=None):
+        w, h = self.sizes[view] if view < len(self.sizes) else (1, 1)
+        if out is None:
+            out = np.empty(w * h * 4, np.uint8)
+        check(lib().gsplat_batch_readback_rgba8(self.ptr, view, out.ctypes.data_as(_u8p), out.nbytes))
+        return out.reshape(h, w, 4)
+
+    def image_device(self, view):
+        p, n = ctypes.c_void_p(), ctypes.c_uint64()
+        check(lib().gsplat_batch_image_device(self.ptr, view, ctypes.byref(p), ctypes.byref(n)))
+        return p.value, n.value
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        check(lib().gsplat_batch_get_stream(self.ptr, ctypes.byref(s)))
+        return s.value
 
 
 def sort_values_by_keys(keys, values):

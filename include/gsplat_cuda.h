@@ -170,6 +170,73 @@ int32_t gsplat_cuda_sort_pairs(uint32_t *keys, uint32_t *values, uint64_t len);
 int32_t gsplat_cuda_sort_values_by_keys_noalloc(const uint32_t *keys, uint32_t *values,
                                                 uint64_t len, void *stream);
 
+/* ---- batched frames -------------------------------------------------------
+ * No counterpart in the reference: its renderer draws one camera per call.
+ * A batch holds several HBM-resident scenes and renders many views (scene,
+ * camera, image size) in one call: the views are split into launch groups of
+ * up to 1024 views (one CUDA-graph launch each, with one shared sort over
+ * (view, tile, depth) keys), and every view's image equals, bit for bit, the
+ * image gsplat_context_render_frame gives for the same scene, camera, size,
+ * tile size and blend mode. A batch handle is confined to one thread at a
+ * time, like a context. */
+typedef struct GsplatBatch GsplatBatch;
+
+typedef struct GsplatBatchView {
+  uint32_t scene;       /* id returned by gsplat_batch_add_scene_* */
+  uint32_t width;
+  uint32_t height;
+  uint32_t reserved;    /* 0 */
+  GsplatCamera camera;
+} GsplatBatchView;      /* 56 bytes */
+
+typedef struct GsplatBatchViewStats {
+  uint32_t visible_count;  /* depth-visible splats (GsplatStats.visible_count) */
+  uint32_t drawn_count;    /* splats with a raster record */
+  uint32_t tile_pairs;     /* (tile, splat) pairs the view emitted */
+  uint32_t group;          /* launch group the view ran in */
+} GsplatBatchViewStats;
+
+typedef struct GsplatBatchTimes {
+  float device_ms;       /* CUDA-event time of all launch groups */
+  float wall_ms;         /* host time of the call */
+  uint32_t groups;       /* launch groups */
+  uint32_t reruns;       /* groups re-run after outgrowing their pair buffers */
+  uint32_t kernel_launches;
+  uint32_t reserved;
+  uint64_t tile_pairs;   /* over all views */
+} GsplatBatchTimes;
+
+/* Creates a batch on the current CUDA device (UNSUPPORTED without an sm_100
+ * device). Scenes are held under a budget of 150 GiB unless changed. */
+int32_t gsplat_batch_create(GsplatBatch **out_batch);
+void gsplat_batch_destroy(GsplatBatch *batch);
+int32_t gsplat_batch_set_scene_budget(GsplatBatch *batch, uint64_t bytes);
+/* Uploads a scene (validated like gsplat_context_load_scene_buffers); the id
+ * numbers scenes from 0 in the order they were added. UNSUPPORTED when the
+ * scene would exceed the budget. */
+int32_t gsplat_batch_add_scene_buffers(GsplatBatch *batch, const GsplatSceneDesc *scene,
+                                       uint32_t *out_scene);
+int32_t gsplat_batch_add_scene_path(GsplatBatch *batch, const char *path, uint32_t *out_scene);
+int32_t gsplat_batch_set_tile_size(GsplatBatch *batch, uint32_t tile);       /* 8 or 16 */
+int32_t gsplat_batch_set_blend_mode(GsplatBatch *batch, uint32_t mode);      /* GsplatBlendMode */
+/* Launch-group limits: views (1..1024), predicted tile pairs and splats per
+ * group (0 keeps the current value). */
+int32_t gsplat_batch_set_limits(GsplatBatch *batch, uint32_t max_views, uint64_t max_pairs,
+                                uint64_t max_splats);
+/* Renders all `count` views and waits until every image is in device memory. */
+int32_t gsplat_batch_render(GsplatBatch *batch, const GsplatBatchView *views, uint32_t count);
+int32_t gsplat_batch_get_times(const GsplatBatch *batch, GsplatBatchTimes *out_times);
+int32_t gsplat_batch_get_view_stats(const GsplatBatch *batch, uint32_t view,
+                                    GsplatBatchViewStats *out_stats);
+/* RGBA8 image of view `view` of the last render (row 0 = top, tight rows). */
+int32_t gsplat_batch_readback_rgba8(GsplatBatch *batch, uint32_t view, uint8_t *out,
+                                    uint64_t out_len);
+/* Device address and size of that image (valid until the next render or
+ * destroy), and the cudaStream_t the batch renders on. */
+int32_t gsplat_batch_image_device(const GsplatBatch *batch, uint32_t view, const void **out_ptr,
+                                  uint64_t *out_bytes);
+int32_t gsplat_batch_get_stream(const GsplatBatch *batch, void **out_stream);
+
 /* ---- host utilities ---- */
 
 /* Parsed PLY scene owned by the library (crates/gsplat-io-ply/src/lib.rs:178-235). */

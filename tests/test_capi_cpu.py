@@ -44,6 +44,9 @@ def test_abi_struct_sizes():
     assert ctypes.sizeof(ffi.GsplatStats) == 24
     assert ctypes.sizeof(ffi.GsplatCamera) == 40
     assert ffi.PROJECTED_DTYPE.itemsize == 64
+    assert ctypes.sizeof(ffi.GsplatBatchView) == 56
+    assert ctypes.sizeof(ffi.GsplatBatchViewStats) == 16
+    assert ctypes.sizeof(ffi.GsplatBatchTimes) == 32
 
 
 def test_versions_defaults_and_messages(oracle):
@@ -92,6 +95,24 @@ def test_null_context_arguments():
     assert L.gsplat_context_get_stats(None, ctypes.byref(st)) == 1
     L.gsplat_context_destroy(None)
     assert L.gsplat_context_readback_rgba8(None, None, 0) == 1
+
+
+def test_batch_null_and_no_gpu_errors():
+    L = ffi.lib()
+    assert L.gsplat_batch_create(None) == 1
+    assert "out_batch is null" in ffi.last_error()
+    L.gsplat_batch_destroy(None)
+    assert L.gsplat_batch_render(None, None, 0) == 1
+    assert "batch is null" in ffi.last_error()
+    t = ffi.GsplatBatchTimes()
+    assert L.gsplat_batch_get_times(None, ctypes.byref(t)) == 1
+    out = ctypes.c_void_p(1)
+    rc = L.gsplat_batch_create(ctypes.byref(out))
+    if rc == 4:
+        assert not out.value and "unavailable" in ffi.last_error()
+    else:
+        assert rc == 0
+        L.gsplat_batch_destroy(out)
 
 
 def test_surface_renderer_is_unsupported():

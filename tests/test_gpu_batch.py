@@ -1,0 +1,165 @@
+"""GPU tests of the batched form: many views over several resident scenes of
+uneven sizes in one call. Every view's image must equal, bit for bit, the
+plain one-frame render of the same scene, camera and size (the per-tile
+lists of a view are the same in the shared (view, tile, depth) key space),
+whatever the launch grouping, pair-buffer re-runs, tile size or blend mode;
+per-view counts must equal the oracle's."""
+
+import numpy as np
+import pytest
+
+import gsplat_ffi as ffi
+import gsplat_scenes
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(256, 256), (320, 200), (400, 300), (97, 61)]
+
+
+def _scenes():
+    rng = np.random.default_rng(77)
+    small = gsplat_scenes.make_scene(rng, gsplat_scenes.gmm_means(rng, 3000), -3.5, 0.6, 0.5, 1.5, 1)
+    mid, _, _, _ = gsplat_scenes.config1(seed=8)
+    big = gsplat_scenes.make_scene(rng, gsplat_scenes.gmm_means(rng, 20000), -4.2, 0.6, 0.5, 1.5, 3)
+    return [small, mid, big]
+
+
+def _views(rng, count, nscenes):
+    out = []
+    for k in range(count):
+        cam = gsplat_scenes.orbit_camera(rng, (3.0, 7.0))
+        w, h = SIZES[k % len(SIZES)]
+        out.append((int(rng.integers(nscenes)), cam, w, h))
+    return out
+
+
+def _plain(scene, cam, w, h, tile=16, blend=0):
+    ctx = ffi.Context(w, h)
+    ctx.set_tile_size(tile)
+    ctx.set_blend_mode(blend)
+    ctx.load_scene(scene)
+    ctx.set_camera(cam)
+    ctx.render_frame()
+    return ctx
+
+
+def _check_against_plain(batch, scenes, views, tile=16, blend=0, oracle=None):
+    for k, (sid, cam, w, h) in enumerate(views):
+        ctx = _plain(scenes[sid], cam, w, h, tile, blend)
+        img = batch.readback_rgba8(k)
+        assert np.array_equal(img, ctx.readback_rgba8()), f"view {k}"
+        st = batch.view_stats(k)
+        counts = ctx.frame_counts()
+        assert st.visible_count == counts.visible and st.drawn_count == counts.drawn
+        assert st.tile_pairs == counts.tile_keys
+        if oracle is not None and k < 3:
+            fr = oracle.Frame(oracle.SceneView(scenes[sid]), cam, w, h, tile=tile)
+            assert st.visible_count == fr.visible and st.tile_pairs == len(fr.pair_tiles)
+            ref = fr.raster_tiles_fp32() if blend == 0 else fr.raster_unorm8()
+            assert np.array_equal(img, ref), f"view {k} vs oracle"
+
+
+def test_batch_views_equal_plain_frames(oracle):
+    scenes = _scenes()
+    rng = np.random.default_rng(1)
+    views = _views(rng, 14, len(scenes))
+    with ffi.Batch() as b:
+        ids = [b.add_scene(s) for s in scenes]
+        assert ids == [0, 1, 2]
+        t = b.render(views)
+        assert t.groups == 1 and t.kernel_launches > 0 and t.device_ms > 0
+        _check_against_plain(b, scenes, views, oracle=oracle)
+        # a second call with other cameras reuses the workspace (graph replay
+        # where the layout repeats) and stays exact
+        views2 = _views(rng, 14, len(scenes))
+        b.render(views2)
+        _check_against_plain(b, scenes, views2)
+        assert sum(b.view_stats(k).tile_pairs for k in range(14)) == b.times().tile_pairs
+
+
+def test_batch_grouping_and_pair_reruns():
+    scenes = _scenes()
+    rng = np.random.default_rng(2)
+    # Large splats close to the camera: far more pairs per splat than the
+    # first prediction, so groups overflow and are re-run with larger buffers.
+    r2 = np.random.default_rng(9)
+    means = r2.uniform(-2, 2, (3000, 3)).astype(np.float32)
+    scenes.append(gsplat_scenes.make_scene(r2, means, -0.5, 0.3, 2.0, 0.5, 0))
+    views = _views(rng, 10, len(scenes))
+    views += [(3, gsplat_scenes.camera((0.0, 0.0, -3.0), (0, 0, 0), 70.0), 640, 480)]
+    with ffi.Batch() as b:
+        for s in scenes:
+            b.add_scene(s)
+        b.set_limits(max_views=3)
+        b.set_tile_size(8)
+        t = b.render(views)
+        assert t.groups == 4
+        assert t.reruns >= 1
+        groups = [b.view_stats(k).group for k in range(len(views))]
+        assert groups == sorted(groups) and groups[0] == 0 and groups[-1] == 3
+        _check_against_plain(b, scenes, views, tile=8)
+        t = b.render(views)  # predictions learned: no re-run the second time
+        assert t.reruns == 0
+        _check_against_plain(b, scenes, views, tile=8)
+
+
+@pytest.mark.parametrize("tile,blend", [(8, 0), (16, 1)])
+def test_batch_tile_size_and_blend_mode(oracle, tile, blend):
+    scenes = _scenes()
+    rng = np.random.default_rng(3 + tile)
+    views = _views(rng, 6, len(scenes))
+    with ffi.Batch() as b:
+        for s in scenes:
+            b.add_scene(s)
+        b.set_tile_size(tile)
+        b.set_blend_mode(blend)
+        b.render(views)
+        _check_against_plain(b, scenes, views, tile, blend, oracle=oracle)
+
+
+def test_batch_more_than_one_launch_of_views():
+    """More views than one launch group holds (1024): split, still exact."""
+    scenes = _scenes()[:2]
+    rng = np.random.default_rng(4)
+    views = []
+    for k in range(1100):
+        cam = gsplat_scenes.orbit_camera(rng, (3.0, 7.0))
+        views.append((k % 2, cam, 48, 32))
+    with ffi.Batch() as b:
+        for s in scenes:
+            b.add_scene(s)
+        t = b.render(views)
+        assert t.groups == 2
+        pick = [0, 1, 511, 1023, 1024, 1099]
+        for k in pick:
+            sid, cam, w, h = views[k]
+            ctx = _plain(scenes[sid], cam, w, h)
+            assert np.array_equal(b.readback_rgba8(k), ctx.readback_rgba8()), k
+
+
+def test_batch_errors():
+    scenes = _scenes()
+    with ffi.Batch() as b:
+        b.add_scene(scenes[0])
+        cam = gsplat_scenes.default_camera()
+        with pytest.raises(ffi.GsplatError) as e:
+            b.render([(5, cam, 32, 32)])
+        assert e.value.code == ffi.INVALID_ARGUMENT and "unknown scene" in e.value.message
+        arr = b.make_views([(0, cam, 32, 32)])
+        arr[0].reserved = 1
+        with pytest.raises(ffi.GsplatError) as e:
+            b.render(arr)
+        assert e.value.code == ffi.INVALID_ARGUMENT
+        with pytest.raises(ffi.GsplatError) as e:
+            b.render([(0, dict(cam, near_plane=5.0, far_plane=1.0), 32, 32)])
+        assert e.value.code == ffi.INVALID_ARGUMENT
+        with pytest.raises(ffi.GsplatError) as e:
+            b.readback_rgba8(0)
+        assert e.value.code == ffi.INVALID_ARGUMENT
+        b.set_scene_budget(1 << 20)
+        with pytest.raises(ffi.GsplatError) as e:
+            b.add_scene(scenes[2])
+        assert e.value.code == ffi.UNSUPPORTED and "budget" in e.value.message
+        with pytest.raises(ffi.GsplatError) as e:
+            b.set_limits(max_views=2000)
+        assert e.value.code == ffi.INVALID_ARGUMENT
