@@ -21,13 +21,20 @@ constexpr uint64_t kMaxPairs = (1u << 30) - 1;
 
 // ---- SceneStore ------------------------------------------------------------
 
+void SceneStore::check_budget(uint64_t bytes) const {
+  if (bytes_ + bytes > budget_)
+    throw Error(Code::Unsupported, "scene memory budget exceeded: " + std::to_string(bytes_ + bytes) +
+                                       " > " + std::to_string(budget_) + " bytes");
+}
+
 uint32_t SceneStore::add(const HostScene &s, cudaStream_t stream) {
   if (scene_validate(s) != Code::Ok) throw Error(Code::InvalidArgument, "invalid scene buffers");
-  const uint64_t need = scene_device_bytes(s);
-  if (bytes_ + need > budget_)
-    throw Error(Code::Unsupported, "scene memory budget exceeded: " + std::to_string(bytes_ + need) +
-                                       " > " + std::to_string(budget_) + " bytes");
-  auto sc = upload_scene(s, stream);
+  check_budget(scene_device_bytes(s));
+  return insert(upload_scene(s, stream));
+}
+
+uint32_t SceneStore::insert(std::unique_ptr<DeviceScene> sc) {
+  check_budget(sc->bytes());
   bytes_ += sc->bytes();
   scenes_.push_back(std::move(sc));
   return (uint32_t)scenes_.size() - 1;

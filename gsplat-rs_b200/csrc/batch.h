@@ -30,6 +30,10 @@ class SceneStore {
   // Uploads and returns the new scene's id; Unsupported if the budget would
   // be exceeded.
   uint32_t add(const HostScene &s, cudaStream_t stream);
+  // Throws Unsupported if `bytes` more would exceed the budget.
+  void check_budget(uint64_t bytes) const;
+  // Takes an uploaded scene (budget checked again).
+  uint32_t insert(std::unique_ptr<DeviceScene> sc);
   const DeviceScene &get(uint32_t id) const;
   uint32_t count() const { return (uint32_t)scenes_.size(); }
   uint64_t bytes() const { return bytes_; }

@@ -13,6 +13,7 @@
 #include "gsr_host.h"
 #include "batch.h"
 #include "renderer.h"
+#include "server.h"
 #include "sort_api.h"
 
 using gsr::Code;
@@ -27,6 +28,10 @@ struct GsplatContext {
 
 struct GsplatBatch {
   std::unique_ptr<gsr::Batch> batch;
+};
+
+struct GsplatServer {
+  std::unique_ptr<gsr::Server> server;
 };
 
 struct GsplatHostScene {
@@ -724,6 +729,139 @@ int32_t gsplat_batch_get_stream(const GsplatBatch *batch, void **out_stream) {
     if (!out_stream)
       return fail(Code::InvalidArgument, "gsplat_batch_get_stream: out_stream is null");
     *out_stream = (void *)batch->batch->stream();
+    return ok();
+  });
+}
+
+// ---- served rendering (gsplat_cuda.h) ----------------------------------------
+
+int32_t gsplat_server_create(const GsplatServeConfig *config, GsplatServer **out_server) {
+  return guarded("gsplat_server_create", [&]() -> int32_t {
+    if (!out_server) return fail(Code::InvalidArgument, "gsplat_server_create: out_server is null");
+    *out_server = nullptr;
+    gsr::ServeConfig c;
+    if (config) {
+      if (config->reserved != 0)
+        return fail(Code::InvalidArgument, "gsplat_server_create: reserved field must be 0");
+      if (config->scene_budget_bytes) c.scene_budget = config->scene_budget_bytes;
+      if (config->work_budget_bytes) c.work_budget = config->work_budget_bytes;
+      if (config->lanes) c.lanes = config->lanes;
+      if (config->max_views_per_batch) c.max_views = config->max_views_per_batch;
+      if (config->tile_size) c.tile = config->tile_size;
+    }
+    auto s = std::make_unique<GsplatServer>();
+    s->server = std::make_unique<gsr::Server>(c);
+    *out_server = s.release();
+    return ok();
+  });
+}
+
+void gsplat_server_destroy(GsplatServer *server) {
+  try {
+    delete server;
+  } catch (...) {
+  }
+}
+
+#define GSR_SERVER_CHECK(op) \
+  if (!server || !server->server) return fail(Code::InvalidArgument, op ": server is null")
+
+int32_t gsplat_server_add_scene_buffers(GsplatServer *server, const GsplatSceneDesc *scene,
+                                        uint32_t *out_scene) {
+  return guarded("gsplat_server_add_scene_buffers", [&]() -> int32_t {
+    GSR_SERVER_CHECK("gsplat_server_add_scene_buffers");
+    if (!scene || !out_scene)
+      return fail(Code::InvalidArgument, "gsplat_server_add_scene_buffers: null argument");
+    *out_scene = server->server->add_scene(host_scene_from_desc(*scene));
+    return ok();
+  });
+}
+
+int32_t gsplat_server_add_scene_path(GsplatServer *server, const char *path, uint32_t *out_scene) {
+  return guarded("gsplat_server_add_scene_path", [&]() -> int32_t {
+    GSR_SERVER_CHECK("gsplat_server_add_scene_path");
+    if (!path || !out_scene)
+      return fail(Code::InvalidArgument, "gsplat_server_add_scene_path: null argument");
+    std::string p(path);
+    if (!valid_utf8(p))
+      return fail(Code::InvalidArgument, "gsplat_server_add_scene_path: path is not valid UTF-8");
+    *out_scene = server->server->add_scene(gsr::load_ply(p));
+    return ok();
+  });
+}
+
+int32_t gsplat_server_submit(GsplatServer *server, const GsplatBatchView *view,
+                             uint64_t *out_request) {
+  return guarded("gsplat_server_submit", [&]() -> int32_t {
+    GSR_SERVER_CHECK("gsplat_server_submit");
+    if (!view || !out_request)
+      return fail(Code::InvalidArgument, "gsplat_server_submit: null argument");
+    if (view->reserved != 0)
+      return fail(Code::InvalidArgument, "gsplat_server_submit: reserved field must be 0");
+    *out_request =
+        server->server->submit(gsr::BatchView{view->scene, view->camera, view->width, view->height});
+    return ok();
+  });
+}
+
+static GsplatRequestInfo to_c_info(const gsr::RequestInfo &i) {
+  return GsplatRequestInfo{(uint32_t)i.status, i.error_code, i.batch_views, i.counters.visible,
+                           i.counters.drawn, i.counters.pairs, i.latency_ms, i.queue_ms};
+}
+
+int32_t gsplat_server_poll(GsplatServer *server, uint64_t request, GsplatRequestInfo *out_info) {
+  return guarded("gsplat_server_poll", [&]() -> int32_t {
+    GSR_SERVER_CHECK("gsplat_server_poll");
+    if (!out_info) return fail(Code::InvalidArgument, "gsplat_server_poll: out_info is null");
+    *out_info = to_c_info(server->server->poll(request));
+    return ok();
+  });
+}
+
+int32_t gsplat_server_wait(GsplatServer *server, uint64_t request, uint32_t timeout_ms,
+                           GsplatRequestInfo *out_info) {
+  return guarded("gsplat_server_wait", [&]() -> int32_t {
+    GSR_SERVER_CHECK("gsplat_server_wait");
+    if (!out_info) return fail(Code::InvalidArgument, "gsplat_server_wait: out_info is null");
+    *out_info = to_c_info(server->server->wait(request, timeout_ms));
+    return ok();
+  });
+}
+
+int32_t gsplat_server_read_rgba8(GsplatServer *server, uint64_t request, uint8_t *out,
+                                 uint64_t out_len) {
+  return guarded("gsplat_server_read_rgba8", [&]() -> int32_t {
+    GSR_SERVER_CHECK("gsplat_server_read_rgba8");
+    if (!out) return fail(Code::InvalidArgument, "gsplat_server_read_rgba8: out is null");
+    server->server->read_rgba8(request, out, out_len);
+    return ok();
+  });
+}
+
+int32_t gsplat_server_release(GsplatServer *server, uint64_t request) {
+  return guarded("gsplat_server_release", [&]() -> int32_t {
+    GSR_SERVER_CHECK("gsplat_server_release");
+    server->server->release(request);
+    return ok();
+  });
+}
+
+int32_t gsplat_server_get_stats(GsplatServer *server, GsplatServeStats *out_stats) {
+  return guarded("gsplat_server_get_stats", [&]() -> int32_t {
+    GSR_SERVER_CHECK("gsplat_server_get_stats");
+    if (!out_stats) return fail(Code::InvalidArgument, "gsplat_server_get_stats: out_stats is null");
+    const gsr::ServeStats s = server->server->stats();
+    *out_stats = GsplatServeStats{s.submitted, s.completed, s.failed, s.batches, s.reruns,
+                                  s.peak_admitted_bytes, s.p50_ms, s.p99_ms, s.mean_ms, s.max_ms,
+                                  s.views_per_s, s.mean_batch_views};
+    return ok();
+  });
+}
+
+int32_t gsplat_server_reset_stats(GsplatServer *server) {
+  return guarded("gsplat_server_reset_stats", [&]() -> int32_t {
+    GSR_SERVER_CHECK("gsplat_server_reset_stats");
+    server->server->reset_stats();
     return ok();
   });
 }

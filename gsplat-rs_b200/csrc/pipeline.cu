@@ -132,6 +132,7 @@ void Pipeline::record(int k) {
 void Pipeline::drop_graph() {
   for (auto &g : graphs_) cudaGraphExecDestroy(g.exec);
   graphs_.clear();
+  seen_keys_.clear();
 }
 
 Pipeline::Layout Pipeline::plan_views(const ViewSpec *views, uint32_t count,
@@ -351,7 +352,21 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
     GraphEntry *hit = nullptr;
     for (auto &g : graphs_)
       if (g.key == key) hit = &g;
+    // A layout is captured the second time it is seen: one-off layouts (a
+    // served batch of a new size) launch directly instead of paying for a
+    // capture they would never replay.
+    bool seen = false;
     if (!hit) {
+      for (auto &k : seen_keys_)
+        if (k == key) seen = true;
+      if (!seen) {
+        if (seen_keys_.size() >= kGraphCacheSize) seen_keys_.erase(seen_keys_.begin());
+        seen_keys_.push_back(key);
+      }
+    }
+    if (!hit && !seen) {
+      launch_all(l, images, sinks);
+    } else if (!hit) {
       if (graphs_.size() >= kGraphCacheSize) {
         auto lru = std::min_element(graphs_.begin(), graphs_.end(),
                                     [](const GraphEntry &a, const GraphEntry &b) {
@@ -383,8 +398,10 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
       graphs_.push_back(GraphEntry{key, exec, 0});
       hit = &graphs_.back();
     }
-    hit->last_use = ++graph_clock_;
-    GSR_CUDA(cudaGraphLaunch(hit->exec, stream_));
+    if (hit) {
+      hit->last_use = ++graph_clock_;
+      GSR_CUDA(cudaGraphLaunch(hit->exec, stream_));
+    }
   }
   GSR_CUDA(cudaGetLastError());
   last_layout_ = l;

@@ -204,6 +204,7 @@ class Pipeline {
   };
   static constexpr size_t kGraphCacheSize = 32;
   std::vector<GraphEntry> graphs_;
+  std::vector<GraphKey> seen_keys_;  // layouts launched once without a graph
   uint64_t graph_clock_ = 0;
 };
 

@@ -107,6 +107,30 @@ class GsplatBatchTimes(ctypes.Structure):
                 ("tile_pairs", ctypes.c_uint64)]
 
 
+class GsplatServeConfig(ctypes.Structure):
+    _fields_ = [("scene_budget_bytes", ctypes.c_uint64), ("work_budget_bytes", ctypes.c_uint64),
+                ("lanes", ctypes.c_uint32), ("max_views_per_batch", ctypes.c_uint32),
+                ("tile_size", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class GsplatRequestInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_uint32), ("error_code", ctypes.c_int32),
+                ("batch_views", ctypes.c_uint32), ("visible_count", ctypes.c_uint32),
+                ("drawn_count", ctypes.c_uint32), ("tile_pairs", ctypes.c_uint32),
+                ("latency_ms", ctypes.c_float), ("queue_ms", ctypes.c_float)]
+
+
+class GsplatServeStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("failed", ctypes.c_uint64), ("batches", ctypes.c_uint64),
+                ("reruns", ctypes.c_uint64), ("peak_admitted_bytes", ctypes.c_uint64),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
+                ("views_per_s", ctypes.c_double), ("mean_batch_views", ctypes.c_double)]
+
+
+REQUEST_QUEUED, REQUEST_RUNNING, REQUEST_DONE, REQUEST_FAILED = 0, 1, 2, 3
+
 PROJECTED_DTYPE = np.dtype([("center_ndc", "<f4", 2), ("axis_u", "<f4", 2), ("axis_v", "<f4", 2),
                             ("color", "<f4", 4), ("extent_scale", "<f4"), ("depth", "<f4"),
                             ("flags", "<u4"), ("tile_x0", "<u2"), ("tile_y0", "<u2"),
@@ -210,6 +234,23 @@ _SIGS = [
      [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p),
       ctypes.POINTER(ctypes.c_uint64)]),
     ("gsplat_batch_get_stream", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    ("gsplat_server_create", ctypes.c_int32,
+     [ctypes.POINTER(GsplatServeConfig), ctypes.POINTER(ctypes.c_void_p)]),
+    ("gsplat_server_destroy", None, [ctypes.c_void_p]),
+    ("gsplat_server_add_scene_buffers", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.POINTER(GsplatSceneDesc), _u32p]),
+    ("gsplat_server_add_scene_path", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_char_p, _u32p]),
+    ("gsplat_server_submit", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.POINTER(GsplatBatchView), ctypes.POINTER(ctypes.c_uint64)]),
+    ("gsplat_server_poll", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(GsplatRequestInfo)]),
+    ("gsplat_server_wait", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(GsplatRequestInfo)]),
+    ("gsplat_server_read_rgba8", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_uint64, _u8p, ctypes.c_uint64]),
+    ("gsplat_server_release", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64]),
+    ("gsplat_server_get_stats", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(GsplatServeStats)]),
+    ("gsplat_server_reset_stats", ctypes.c_int32, [ctypes.c_void_p]),
     ("gsplat_ply_load", ctypes.c_int32, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
     ("gsplat_host_scene_destroy", None, [ctypes.c_void_p]),
     ("gsplat_host_scene_view", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(GsplatSceneDesc)]),
@@ -505,6 +546,77 @@ class Batch:
         s = ctypes.c_void_p()
         check(lib().gsplat_batch_get_stream(self.ptr, ctypes.byref(s)))
         return s.value
+
+
+class Server:
+    """One GsplatServer: resident scenes and a continuous-batching request loop."""
+
+    def __init__(self, lanes=0, max_views=0, tile=0, scene_budget=0, work_budget=0):
+        cfg = GsplatServeConfig(scene_budget, work_budget, lanes, max_views, tile, 0)
+        self.ptr = ctypes.c_void_p()
+        check(lib().gsplat_server_create(ctypes.byref(cfg), ctypes.byref(self.ptr)))
+        self.sizes = {}
+
+    def close(self):
+        if self.ptr:
+            lib().gsplat_server_destroy(self.ptr)
+            self.ptr = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_scene(self, scene):
+        sd = SceneDesc(scene)
+        sid = ctypes.c_uint32()
+        check(lib().gsplat_server_add_scene_buffers(self.ptr, ctypes.byref(sd.desc), ctypes.byref(sid)))
+        return sid.value
+
+    def submit(self, scene, cam, width, height):
+        v = GsplatBatchView()
+        v.scene, v.width, v.height, v.reserved = scene, width, height, 0
+        v.camera = cam if isinstance(cam, GsplatCamera) else GsplatCamera.from_dict(cam)
+        rid = ctypes.c_uint64()
+        check(lib().gsplat_server_submit(self.ptr, ctypes.byref(v), ctypes.byref(rid)))
+        self.sizes[rid.value] = (width, height)
+        return rid.value
+
+    def poll(self, rid):
+        i = GsplatRequestInfo()
+        check(lib().gsplat_server_poll(self.ptr, rid, ctypes.byref(i)))
+        return i
+
+    def wait(self, rid, timeout_ms=60000):
+        i = GsplatRequestInfo()
+        check(lib().gsplat_server_wait(self.ptr, rid, timeout_ms, ctypes.byref(i)))
+        return i
+
+    def read_rgba8(self, rid, out=None):
+        w, h = self.sizes.get(rid, (1, 1))
+        if out is None:
+            out = np.empty(w * h * 4, np.uint8)
+        check(lib().gsplat_server_read_rgba8(self.ptr, rid, out.ctypes.data_as(_u8p), out.nbytes))
+        return out.reshape(h, w, 4)
+
+    def release(self, rid):
+        check(lib().gsplat_server_release(self.ptr, rid))
+        self.sizes.pop(rid, None)
+
+    def stats(self):
+        s = GsplatServeStats()
+        check(lib().gsplat_server_get_stats(self.ptr, ctypes.byref(s)))
+        return s
+
+    def reset_stats(self):
+        check(lib().gsplat_server_reset_stats(self.ptr))
 
 
 def sort_values_by_keys(keys, values):

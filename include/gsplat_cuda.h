@@ -237,6 +237,75 @@ int32_t gsplat_batch_image_device(const GsplatBatch *batch, uint32_t view, const
                                   uint64_t *out_bytes);
 int32_t gsplat_batch_get_stream(const GsplatBatch *batch, void **out_stream);
 
+/* ---- served rendering --------------------------------------------------------
+ * No counterpart in the reference. A server keeps scenes resident in HBM and
+ * renders requests (one GsplatBatchView each) with continuous batching: a
+ * scheduler thread takes the queued requests into a batch whenever one of
+ * its lanes (a CUDA stream with its own workspace) is free, admitting them in
+ * arrival order while the batch's predicted memory -- tile-pair buffers sized
+ * from predicted tile-overlap counts, splat workspace and images -- fits the
+ * lane's share of the work budget. Batches on different lanes overlap on the
+ * device. A request is done when its RGBA8 image is in host memory; it is
+ * identical, bit for bit, to gsplat_context_render_frame's image for the same
+ * scene, camera and size at the server's tile size. Every call except create
+ * and destroy may be made from any thread. */
+typedef struct GsplatServer GsplatServer;
+
+typedef struct GsplatServeConfig {
+  uint64_t scene_budget_bytes;  /* resident scenes; 0 = 150 GiB */
+  uint64_t work_budget_bytes;   /* workspace over all lanes; 0 = 24 GiB */
+  uint32_t lanes;               /* batches in flight, 1..8; 0 = 2 */
+  uint32_t max_views_per_batch; /* 1..1024; 0 = 256 */
+  uint32_t tile_size;           /* 8 or 16; 0 = 16 */
+  uint32_t reserved;            /* 0 */
+} GsplatServeConfig;            /* 32 bytes */
+
+typedef enum GsplatRequestStatus {
+  GSPLAT_REQUEST_QUEUED = 0,
+  GSPLAT_REQUEST_RUNNING = 1,
+  GSPLAT_REQUEST_DONE = 2,
+  GSPLAT_REQUEST_FAILED = 3
+} GsplatRequestStatus;
+
+typedef struct GsplatRequestInfo {
+  uint32_t status;          /* GsplatRequestStatus */
+  int32_t error_code;       /* GsplatErrorCode of a failed request */
+  uint32_t batch_views;     /* requests in the batch it ran in */
+  uint32_t visible_count;
+  uint32_t drawn_count;
+  uint32_t tile_pairs;
+  float latency_ms;         /* submit -> image in host memory */
+  float queue_ms;           /* submit -> batch launch */
+} GsplatRequestInfo;        /* 32 bytes */
+
+typedef struct GsplatServeStats {
+  uint64_t submitted, completed, failed, batches, reruns;
+  uint64_t peak_admitted_bytes;  /* predicted workspace of the batches in flight */
+  double p50_ms, p99_ms, mean_ms, max_ms;  /* request latency, nearest rank */
+  double views_per_s;        /* completed / (last completion - first submit) */
+  double mean_batch_views;
+} GsplatServeStats;          /* 96 bytes */
+
+int32_t gsplat_server_create(const GsplatServeConfig *config, GsplatServer **out_server);
+/* Finishes the batches in flight, fails queued requests and frees everything. */
+void gsplat_server_destroy(GsplatServer *server);
+int32_t gsplat_server_add_scene_buffers(GsplatServer *server, const GsplatSceneDesc *scene,
+                                        uint32_t *out_scene);
+int32_t gsplat_server_add_scene_path(GsplatServer *server, const char *path, uint32_t *out_scene);
+/* Validates the view (scene id, camera, size) and queues it. */
+int32_t gsplat_server_submit(GsplatServer *server, const GsplatBatchView *view,
+                             uint64_t *out_request);
+int32_t gsplat_server_poll(GsplatServer *server, uint64_t request, GsplatRequestInfo *out_info);
+/* Waits up to timeout_ms for the request to finish; *out_info tells whether it did. */
+int32_t gsplat_server_wait(GsplatServer *server, uint64_t request, uint32_t timeout_ms,
+                           GsplatRequestInfo *out_info);
+int32_t gsplat_server_read_rgba8(GsplatServer *server, uint64_t request, uint8_t *out,
+                                 uint64_t out_len);
+/* Forgets a finished request and recycles its image buffer. */
+int32_t gsplat_server_release(GsplatServer *server, uint64_t request);
+int32_t gsplat_server_get_stats(GsplatServer *server, GsplatServeStats *out_stats);
+int32_t gsplat_server_reset_stats(GsplatServer *server);
+
 /* ---- host utilities ---- */
 
 /* Parsed PLY scene owned by the library (crates/gsplat-io-ply/src/lib.rs:178-235). */

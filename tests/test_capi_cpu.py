@@ -47,6 +47,9 @@ def test_abi_struct_sizes():
     assert ctypes.sizeof(ffi.GsplatBatchView) == 56
     assert ctypes.sizeof(ffi.GsplatBatchViewStats) == 16
     assert ctypes.sizeof(ffi.GsplatBatchTimes) == 32
+    assert ctypes.sizeof(ffi.GsplatServeConfig) == 32
+    assert ctypes.sizeof(ffi.GsplatRequestInfo) == 32
+    assert ctypes.sizeof(ffi.GsplatServeStats) == 96
 
 
 def test_versions_defaults_and_messages(oracle):
@@ -113,6 +116,26 @@ def test_batch_null_and_no_gpu_errors():
     else:
         assert rc == 0
         L.gsplat_batch_destroy(out)
+
+
+def test_server_null_and_no_gpu_errors():
+    L = ffi.lib()
+    assert L.gsplat_server_create(None, None) == 1
+    L.gsplat_server_destroy(None)
+    rid = ctypes.c_uint64()
+    assert L.gsplat_server_submit(None, None, ctypes.byref(rid)) == 1
+    assert "server is null" in ffi.last_error()
+    cfg = ffi.GsplatServeConfig(0, 0, 0, 0, 0, 1)
+    out = ctypes.c_void_p(1)
+    assert L.gsplat_server_create(ctypes.byref(cfg), ctypes.byref(out)) == 1
+    assert not out.value
+    cfg.reserved = 0
+    rc = L.gsplat_server_create(ctypes.byref(cfg), ctypes.byref(out))
+    if rc == 4:
+        assert not out.value and "unavailable" in ffi.last_error()
+    else:
+        assert rc == 0
+        L.gsplat_server_destroy(out)
 
 
 def test_surface_renderer_is_unsupported():
