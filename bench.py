@@ -214,6 +214,10 @@ def measure_batched(ffi, torch, steps, warmup):
     for s in scenes:
         b.add_scene(s)
     arr = ffi.Batch.make_views(specs)
+    # launch shape from the autotuner, searched on every 8th view
+    tune_views = ffi.Batch.make_views(specs[::8])
+    tuned = b.autotune(tune_views, os.path.join(tempfile.gettempdir(), "gsplat_bench_tune.txt"),
+                       reps=2)
     for _ in range(max(warmup, 2)):
         b.render(arr)
     dev, wall = [], []
@@ -280,6 +284,10 @@ def measure_batched(ffi, torch, steps, warmup):
             "views": n, "views_per_s": batched_vps,
             "ms_per_batch": float(np.median(dev)), "wall_ms_per_batch": float(np.median(wall)),
             "groups": t.groups, "kernel_launches": t.kernel_launches, "tile_pairs": int(t.tile_pairs),
+            "autotune": {"tile": tuned.tile_size, "chunk": tuned.chunk,
+                         "blocks_per_sm": tuned.blocks_per_sm, "candidates": tuned.candidates,
+                         "from_cache": bool(tuned.from_cache),
+                         "subset_best_ms": tuned.best_ms, "subset_default_ms": tuned.default_ms},
             "e2e_views_per_s": n / float(np.median(e2e)),
             "e2e_d2h_bytes": int(pixels * 4),
             "plain_views_per_s": n / (plain_dev_total / 1000.0),
@@ -288,6 +296,107 @@ def measure_batched(ffi, torch, steps, warmup):
             "per_scene": per_scene,
             "timing": "device ms from CUDA events around all launch groups (batched) and the "
                       "per-phase CUDA events of each plain frame; scenes exceed L2"}
+
+
+def _spin_until(t):
+    while True:
+        d = t - time.perf_counter()
+        if d <= 0:
+            return
+        if d > 0.002:
+            time.sleep(d - 0.001)
+
+
+def measure_served(ffi, rates, seconds, max_requests):
+    """Served stream: 8 resident scenes (sizes log-uniform in [50k, 3M], SH
+    degree 0-3 mixed), Poisson arrivals at each offered rate, each request a
+    random scene, orbit camera and resolution from {512^2, 720p, 1080p}.
+    Latency is submit -> RGBA8 image in host memory. The plain drop-in call
+    serves the same arrival sequence one gsplat_context_render_frame +
+    readback at a time, in arrival order."""
+    scenes = gsplat_scenes.config5_scenes()
+    srv = ffi.Server(lanes=2, max_views=256)
+    for sc in scenes:
+        srv.add_scene(sc)
+    ctxs = {}
+    for sid, sc in enumerate(scenes):
+        ctx = ffi.Context(512, 512)
+        ctx.load_scene(sc)
+        ctxs[sid] = ctx
+    # warm-up: every (scene, size) once through both paths
+    warm = []
+    for sid in range(len(scenes)):
+        for w, h in gsplat_scenes.RESOLUTIONS:
+            cam = gsplat_scenes.camera((0.0, 0.5, -5.0), (0, 0, 0), 50.0)
+            warm.append(srv.submit(sid, cam, w, h))
+            ctxs[sid].set_size(w, h)
+            ctxs[sid].set_camera(cam)
+            ctxs[sid].render_frame()
+    for rid in warm:
+        srv.wait(rid)
+        srv.release(rid)
+    out = []
+    for rate in rates:
+        count = int(min(max_requests, max(50, rate * seconds)))
+        reqs = gsplat_scenes.config5_requests(int(rate), rate, count, len(scenes))
+        srv.reset_stats()
+        done = threading.Event()
+        ids = []
+
+        def consumer():
+            k = 0
+            while k < count:
+                if k >= len(ids):
+                    time.sleep(0.0002)
+                    continue
+                srv.wait(ids[k])
+                srv.release(ids[k])
+                k += 1
+            done.set()
+
+        th = threading.Thread(target=consumer)
+        th.start()
+        t0 = time.perf_counter()
+        for r in reqs:
+            _spin_until(t0 + r["arrival_s"])
+            ids.append(srv.submit(r["scene"], r["camera"], r["width"], r["height"]))
+        done.wait()
+        th.join()
+        st = srv.stats()
+        # plain: one request at a time, in arrival order
+        lat = []
+        busy = 0.0
+        t0 = time.perf_counter()
+        for r in reqs:
+            _spin_until(t0 + r["arrival_s"])
+            ctx = ctxs[r["scene"]]
+            if (ctx.width, ctx.height) != (r["width"], r["height"]):
+                ctx.set_size(r["width"], r["height"])
+            ts = time.perf_counter()
+            ctx.set_camera(r["camera"])
+            ctx.render_frame()
+            ctx.readback_rgba8()
+            te = time.perf_counter()
+            busy += te - ts
+            lat.append((te - (t0 + r["arrival_s"])) * 1000.0)
+        lat = np.sort(np.array(lat))
+        plain_span = time.perf_counter() - t0
+        out.append({"offered_req_per_s": rate, "requests": count,
+                    "views_per_s": st.views_per_s, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
+                    "mean_batch_views": st.mean_batch_views, "batches": int(st.batches),
+                    "reruns": int(st.reruns), "peak_admitted_gb": st.peak_admitted_bytes / 1e9,
+                    "plain_views_per_s": count / plain_span,
+                    "plain_capacity_views_per_s": count / busy,
+                    "plain_p50_ms": float(lat[int(math.ceil(0.5 * len(lat))) - 1]),
+                    "plain_p99_ms": float(lat[int(math.ceil(0.99 * len(lat))) - 1])})
+    srv.close()
+    for c in ctxs.values():
+        c.close()
+    return {"workload": "8 resident scenes, sizes log-uniform in [50k, 3M] splats, SH degree 0-3 "
+                        "mixed; Poisson arrivals; each request a random scene, orbit camera and "
+                        "resolution from 512^2/720p/1080p; 2 lanes, <=256 views per batch",
+            "latency": "submit -> RGBA8 image in pinned host memory (host clock)",
+            "rates": out}
 
 
 def run_cuda(args, world, rank, local):
@@ -412,6 +521,9 @@ def run_cuda(args, world, rank, local):
     ctx.close()
     if not args.no_batched:
         line["batched"] = measure_batched(ffi, torch, args.batch_steps, 2)
+    if not args.no_served:
+        line["served"] = measure_served(ffi, [float(x) for x in args.serve_rates.split(",")],
+                                        args.serve_seconds, 4000)
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:
@@ -428,6 +540,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=3)
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--serve-rates", default="500,2000,8000,20000")
+    ap.add_argument("--serve-seconds", type=float, default=1.0)
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":

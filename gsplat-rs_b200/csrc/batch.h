@@ -143,6 +143,10 @@ class Batch {
   uint32_t tile() const { return tile_; }
   void set_blend_mode(uint32_t mode);
   void set_use_graph(bool on) { lane_->pipe().set_use_graph(on); }
+  void set_raster_config(const RasterConfig &c) { lane_->pipe().set_raster_config(c); }
+  const RasterConfig &raster_config() { return lane_->pipe().raster_config(); }
+  uint32_t blend_mode() { return lane_->pipe().blend_mode(); }
+  int device() const { return device_; }
   void set_limits(const GroupLimits &l);
   const GroupLimits &limits() const { return limits_; }
 

@@ -11,6 +11,7 @@
 #include "../../include/gsplat.h"
 #include "../../include/gsplat_cuda.h"
 #include "gsr_host.h"
+#include "autotune.h"
 #include "batch.h"
 #include "renderer.h"
 #include "server.h"
@@ -361,6 +362,17 @@ int32_t gsplat_context_set_cuda_graph(GsplatContext *ctx, uint32_t enabled) {
   });
 }
 
+int32_t gsplat_context_set_raster_config(GsplatContext *ctx, uint32_t chunk, uint32_t blocks_per_sm) {
+  return guarded("gsplat_context_set_raster_config", [&]() -> int32_t {
+    if (!ctx) return fail(Code::InvalidArgument, "gsplat_context_set_raster_config: ctx is null");
+    gsr::RasterConfig c;
+    c.chunk = chunk;
+    c.blocks_per_sm = blocks_per_sm;
+    ctx->renderer->set_raster_config(c);
+    return ok();
+  });
+}
+
 int32_t gsplat_context_load_scene_buffers(GsplatContext *ctx, const GsplatSceneDesc *scene) {
   return guarded("gsplat_context_load_scene_buffers", [&]() -> int32_t {
     if (!ctx || !scene)
@@ -665,17 +677,46 @@ int32_t gsplat_batch_set_limits(GsplatBatch *batch, uint32_t max_views, uint64_t
   });
 }
 
+int32_t gsplat_batch_set_raster_config(GsplatBatch *batch, uint32_t chunk, uint32_t blocks_per_sm) {
+  return guarded("gsplat_batch_set_raster_config", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_set_raster_config");
+    gsr::RasterConfig c;
+    c.chunk = chunk;
+    c.blocks_per_sm = blocks_per_sm;
+    batch->batch->set_raster_config(c);
+    return ok();
+  });
+}
+
+static std::vector<gsr::BatchView> to_batch_views(const GsplatBatchView *views, uint32_t count) {
+  std::vector<gsr::BatchView> v(count);
+  for (uint32_t i = 0; i < count; ++i) {
+    if (views[i].reserved != 0) throw Error(Code::InvalidArgument, "reserved field must be 0");
+    v[i] = gsr::BatchView{views[i].scene, views[i].camera, views[i].width, views[i].height};
+  }
+  return v;
+}
+
+int32_t gsplat_batch_autotune(GsplatBatch *batch, const GsplatBatchView *views, uint32_t count,
+                              const char *cache_path, uint32_t reps, GsplatTuneResult *out_result) {
+  return guarded("gsplat_batch_autotune", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_autotune");
+    if (!views || count == 0 || !out_result)
+      return fail(Code::InvalidArgument, "gsplat_batch_autotune: null argument or no views");
+    gsr::TuneResult r = gsr::autotune(*batch->batch, to_batch_views(views, count),
+                                      cache_path ? std::string(cache_path) : std::string(), reps);
+    *out_result = GsplatTuneResult{r.best.tile, r.best.raster.chunk, r.best.raster.blocks_per_sm,
+                                   (uint32_t)r.tried.size(), r.best.ms, r.default_ms,
+                                   r.from_cache ? 1u : 0u, 0};
+    return ok();
+  });
+}
+
 int32_t gsplat_batch_render(GsplatBatch *batch, const GsplatBatchView *views, uint32_t count) {
   return guarded("gsplat_batch_render", [&]() -> int32_t {
     GSR_BATCH_CHECK("gsplat_batch_render");
     if (!views || count == 0) return fail(Code::InvalidArgument, "gsplat_batch_render: no views");
-    std::vector<gsr::BatchView> v(count);
-    for (uint32_t i = 0; i < count; ++i) {
-      if (views[i].reserved != 0)
-        return fail(Code::InvalidArgument, "gsplat_batch_render: reserved field must be 0");
-      v[i] = gsr::BatchView{views[i].scene, views[i].camera, views[i].width, views[i].height};
-    }
-    batch->batch->render(v);
+    batch->batch->render(to_batch_views(views, count));
     return ok();
   });
 }
@@ -748,6 +789,8 @@ int32_t gsplat_server_create(const GsplatServeConfig *config, GsplatServer **out
       if (config->lanes) c.lanes = config->lanes;
       if (config->max_views_per_batch) c.max_views = config->max_views_per_batch;
       if (config->tile_size) c.tile = config->tile_size;
+      c.raster.chunk = config->raster_chunk;
+      c.raster.blocks_per_sm = config->raster_blocks_per_sm;
     }
     auto s = std::make_unique<GsplatServer>();
     s->server = std::make_unique<gsr::Server>(c);

@@ -61,7 +61,7 @@ struct FrameCounters {
   uint32_t error;
   uint32_t overflow;
   uint32_t pairs;  // pairs written: min(keys, capacity)
-  uint32_t pad0;
+  uint32_t raster_ticket;  // persistent raster tile queue
   unsigned long long keys;  // pairs emitted (may exceed the capacity)
   uint32_t sort_tickets[16];
 };

@@ -20,6 +20,8 @@
 //   UNORM8 mode: back to front, dst = src + dst * (1 - w) rounded to UNORM8
 //     after every splat (the reference's Rgba8Unorm premultiplied blend).
 
+#include <algorithm>
+
 #include "device_common.cuh"
 #include "kernels.h"
 
@@ -34,55 +36,47 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// UNORM8 parity mode: back to front over the tile list, the reference
-// fragment rule with the quad clip, rounding to UNORM8 after every blend.
-// Per-block prologue shared by both raster kernels: fold the frame's error
-// bits into the sticky word (block 0) and find the view of this global tile.
-__device__ __forceinline__ uint32_t raster_view(const ViewDev *__restrict__ views,
-                                                uint32_t num_views,
-                                                const FrameCounters *__restrict__ counters,
-                                                uint32_t *sticky, uint32_t *s_view) {
-  if (threadIdx.x == 0) {
-    if (blockIdx.x == 0) {
-      uint32_t bits = counters->error | (counters->overflow ? 0x80000000u : 0u);
-      if (bits) atomicOr(sticky, bits);
-    }
-    *s_view = find_view(num_views, blockIdx.x, [&](uint32_t v) { return views[v].tile_base; });
+// Block 0 folds the frame's error and overflow bits into the sticky word
+// that gsplat_context_sync reports for enqueued frames.
+__device__ __forceinline__ void fold_errors(const RasterArgs &a) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    uint32_t bits = a.counters->error | (a.counters->overflow ? 0x80000000u : 0u);
+    if (bits) atomicOr(a.sticky, bits);
   }
-  __syncthreads();
-  return *s_view;
 }
 
+// UNORM8 parity mode: back to front over the tile list, the reference
+// fragment rule with the quad clip, rounding to UNORM8 after every blend.
 template <int kTile>
-__global__ void __launch_bounds__(kTile *kTile) raster_unorm8_kernel(
-    const ViewDev *__restrict__ views, uint32_t num_views, const uint2 *__restrict__ ranges,
-    const SortPlan *__restrict__ plan, const uint32_t *__restrict__ ids0,
-    const uint32_t *__restrict__ ids1, const Record *__restrict__ records,
-    uint32_t *__restrict__ images, const FrameCounters *__restrict__ counters, uint32_t *sticky) {
+__global__ void __launch_bounds__(kTile *kTile) raster_unorm8_kernel(RasterArgs a) {
   constexpr int kN = kTile * kTile;
   __shared__ float4 s_a[2][kN];
   __shared__ float4 s_b[2][kN];
   __shared__ float4 s_c[2][kN];
   __shared__ uint32_t s_view;
-  const uint32_t view = raster_view(views, num_views, counters, sticky, &s_view);
-  const FrameParams p = views[view].p;
-  uint32_t *__restrict__ image = images + views[view].image_base;
+  fold_errors(a);
   const uint32_t tile = blockIdx.x;
-  const uint32_t local_tile = tile - views[view].tile_base;
+  if (threadIdx.x == 0)
+    s_view = find_view(a.num_views, tile, [&](uint32_t v) { return a.views[v].tile_base; });
+  __syncthreads();
+  const uint32_t view = s_view;
+  const FrameParams p = a.views[view].p;
+  uint32_t *__restrict__ image = a.images + a.views[view].image_base;
+  const uint32_t local_tile = tile - a.views[view].tile_base;
   const uint32_t tx = local_tile % p.tiles_x, ty = local_tile / p.tiles_x;
   const uint32_t tid = threadIdx.x;
   const uint32_t px = tx * kTile + (tid % kTile);
   const uint32_t py = ty * kTile + (tid / kTile);
   const bool inside = px < p.width && py < p.height;
   const float fpx = (float)px, fpy = (float)py;
-  const uint32_t *__restrict__ ids = plan->final_buffer == 0 ? ids0 : ids1;
-  const uint2 range = ranges[tile];
+  const uint32_t *__restrict__ ids = a.plan->final_buffer == 0 ? a.ids0 : a.ids1;
+  const uint2 range = a.ranges[tile];
   const uint32_t count = range.y - range.x;
   const uint32_t chunks = (count + kN - 1) / kN;
   auto issue = [&](uint32_t c, int buf) {
     uint32_t k = c * kN + tid;
     if (k < count) {
-      const Record *r = &records[ids[range.x + k]];
+      const Record *r = &a.records[ids[range.x + k]];
       cp_async16(&s_a[buf][tid], &r->a);
       cp_async16(&s_b[buf][tid], &r->b);
       cp_async16(&s_c[buf][tid], &r->c);
@@ -100,15 +94,15 @@ __global__ void __launch_bounds__(kTile *kTile) raster_unorm8_kernel(
     const uint32_t n_in = min((uint32_t)kN, count - c * kN);
     if (inside) {
       for (uint32_t j = 0; j < n_in; ++j) {
-        const float4 a = s_a[buf][j], b = s_b[buf][j], col = s_c[buf][j];
-        float dpx = fpx - a.x, dpy = fpy - a.y;
-        float lx = fmaf(a.z, dpx, a.w * dpy);
-        float ly = fmaf(b.x, dpx, b.y * dpy);
-        if (!(fabsf(lx) <= b.z && fabsf(ly) <= b.z)) continue;
+        const float4 ra = s_a[buf][j], rb = s_b[buf][j], col = s_c[buf][j];
+        float dpx = fpx - ra.x, dpy = fpy - ra.y;
+        float lx = fmaf(ra.z, dpx, ra.w * dpy);
+        float ly = fmaf(rb.x, dpx, rb.y * dpy);
+        if (!(fabsf(lx) <= rb.z && fabsf(ly) <= rb.z)) continue;
         float r2 = fmaf(lx, lx, ly * ly);
         if (!(r2 <= 1.0f)) continue;
         float g = exp_neg(-4.5f * r2);
-        float w = b.w * g;
+        float w = rb.w * g;
         if (!(w > 1.0f / 256.0f)) continue;
         float om = 1.0f - w;
         d0 = to_unorm8(fmaf((float)d0 / 255.0f, om, col.x * g));
@@ -125,39 +119,44 @@ __global__ void __launch_bounds__(kTile *kTile) raster_unorm8_kernel(
 
 // FP32 front-to-back mode. Threads map to 8x4-pixel warp blocks (lane l of
 // warp w covers column (w % (kTile/8))*8 + (l & 7), row (w / (kTile/8))*4 +
-// (l >> 3)). Per chunk of kN list entries:
+// (l >> 3)). Per chunk of kChunk list entries:
 //   1. raw records arrive by cp.async (double-buffered, next chunk in flight);
-//   2. each thread derives, for its entry and this tile, the tile-local
-//      offsets ox, oy (local = (ax*lx + ay*ly + ox, bx*lx + by*ly + oy) for
-//      tile-local pixel coordinates), s^2, and a bit mask of the warp blocks
-//      the splat's ellipse bounding box (plus one pixel) touches;
+//   2. one thread per entry derives, for this tile, the local offsets ox, oy
+//      (local = (ax*lx + ay*ly + ox, bx*lx + by*ly + oy) for pixel coordinates
+//      relative to the 16-pixel grid corner), s^2, and a bit mask of the warp
+//      blocks the ellipse |local| <= s reaches (band intervals plus half a
+//      pixel);
 //   3. each warp compacts the entries whose mask has its bit (ballots keep the
 //      list order) and blends only those; a pixel stops at T < 1e-4, a warp
 //      when all 32 pixels have, the block when all pixels have.
-// Culling is conservative, so results equal the unculled per-pixel walk.
-template <int kTile>
-__global__ void __launch_bounds__(kTile *kTile) raster_fp32_kernel(
-    const ViewDev *__restrict__ views, uint32_t num_views, const uint2 *__restrict__ ranges,
-    const SortPlan *__restrict__ plan, const uint32_t *__restrict__ ids0,
-    const uint32_t *__restrict__ ids1, const Record *__restrict__ records,
-    uint32_t *__restrict__ images, const FrameCounters *__restrict__ counters, uint32_t *sticky) {
-  constexpr int kN = kTile * kTile;
-  constexpr int kWarps = kN / 32;
-  constexpr int kBlocksX = kTile / 8;
-  __shared__ uint32_t s_view;
-  __shared__ float4 s_raw[2][3][kN];
-  __shared__ float4 s_d0[kN];  // ax, ay, ox, s2
-  __shared__ float4 s_d1[kN];  // bx, by, oy, alpha
-  __shared__ float4 s_d2[kN];  // r*alpha, g*alpha, b*alpha, -
-  __shared__ uint8_t s_mask[kN];
-  __shared__ uint16_t s_list[kWarps][kN];
+// Culling is conservative, so results equal the unculled per-pixel walk, and
+// neither the chunk size nor the tile order changes any pixel.
+template <int kTile, int kChunk>
+struct Fp32Smem {
+  static constexpr int kWarps = kTile * kTile / 32;
+  float4 raw[2][3][kChunk];
+  float4 d0[kChunk];  // ax, ay, ox, s2
+  float4 d1[kChunk];  // bx, by, oy, alpha
+  float4 d2[kChunk];  // r*alpha, g*alpha, b*alpha, -
+  uint8_t mask[kChunk];
+  uint16_t list[kWarps][kChunk];
+  uint32_t view;
+  uint32_t next;
+};
 
-  const uint32_t view = raster_view(views, num_views, counters, sticky, &s_view);
-  const uint32_t width = views[view].p.width, height = views[view].p.height;
-  const uint32_t tiles_x = views[view].p.tiles_x;
-  uint32_t *__restrict__ image = images + views[view].image_base;
-  const uint32_t tile = blockIdx.x;
-  const uint32_t local_tile = tile - views[view].tile_base;
+template <int kTile, int kChunk>
+__device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t tile,
+                                                 Fp32Smem<kTile, kChunk> &sm) {
+  constexpr int kBlocksX = kTile / 8;
+  constexpr int kWarps = Fp32Smem<kTile, kChunk>::kWarps;
+  if (threadIdx.x == 0)
+    sm.view = find_view(a.num_views, tile, [&](uint32_t v) { return a.views[v].tile_base; });
+  __syncthreads();
+  const uint32_t view = sm.view;
+  const uint32_t width = a.views[view].p.width, height = a.views[view].p.height;
+  const uint32_t tiles_x = a.views[view].p.tiles_x;
+  uint32_t *__restrict__ image = a.images + a.views[view].image_base;
+  const uint32_t local_tile = tile - a.views[view].tile_base;
   const uint32_t tx = local_tile % tiles_x, ty = local_tile / tiles_x;
   const uint32_t x0 = tx * kTile, y0 = ty * kTile;
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -171,18 +170,18 @@ __global__ void __launch_bounds__(kTile *kTile) raster_fp32_kernel(
   const float fx = (float)(px - ax0), fy = (float)(py - ay0);
   const float fax = (float)ax0, fay = (float)ay0;
   const float ftx = (float)x0, fty = (float)y0;
-  const uint32_t *__restrict__ ids = plan->final_buffer == 0 ? ids0 : ids1;
-  const uint2 range = ranges[tile];
+  const uint32_t *__restrict__ ids = a.plan->final_buffer == 0 ? a.ids0 : a.ids1;
+  const uint2 range = a.ranges[tile];
   const uint32_t count = range.y - range.x;
-  const uint32_t chunks = (count + kN - 1) / kN;
+  const uint32_t chunks = (count + kChunk - 1) / kChunk;
 
   auto issue = [&](uint32_t c, int buf) {
-    uint32_t k = c * kN + tid;
-    if (k < count) {
-      const Record *r = &records[ids[range.y - 1 - k]];
-      cp_async16(&s_raw[buf][0][tid], &r->a);
-      cp_async16(&s_raw[buf][1][tid], &r->b);
-      cp_async16(&s_raw[buf][2][tid], &r->c);
+    uint32_t k = c * kChunk + tid;
+    if (tid < (uint32_t)kChunk && k < count) {
+      const Record *r = &a.records[ids[range.y - 1 - k]];
+      cp_async16(&sm.raw[buf][0][tid], &r->a);
+      cp_async16(&sm.raw[buf][1][tid], &r->b);
+      cp_async16(&sm.raw[buf][2][tid], &r->c);
     }
     cp_async_commit();
   };
@@ -195,24 +194,24 @@ __global__ void __launch_bounds__(kTile *kTile) raster_fp32_kernel(
     if (c + 1 < chunks) issue(c + 1, buf ^ 1);
     else cp_async_commit();
     cp_async_wait_1();
-    const uint32_t n_in = min((uint32_t)kN, count - c * kN);
+    const uint32_t n_in = min((uint32_t)kChunk, count - c * kChunk);
     if (tid < n_in) {
-      const float4 a = s_raw[buf][0][tid], b = s_raw[buf][1][tid], col = s_raw[buf][2][tid];
-      float cxa = a.x - fax, cya = a.y - fay;
-      float ox = -fmaf(a.z, cxa, a.w * cya);
-      float oy = -fmaf(b.x, cxa, b.y * cya);
-      float cxl = a.x - ftx, cyl = a.y - fty;
-      s_d0[tid] = make_float4(a.z, a.w, ox, b.z * b.z);
-      s_d1[tid] = make_float4(b.x, b.y, oy, b.w);
-      s_d2[tid] = col;
+      const float4 ra = sm.raw[buf][0][tid], rb = sm.raw[buf][1][tid], col = sm.raw[buf][2][tid];
+      float cxa = ra.x - fax, cya = ra.y - fay;
+      float ox = -fmaf(ra.z, cxa, ra.w * cya);
+      float oy = -fmaf(rb.x, cxa, rb.y * cya);
+      float cxl = ra.x - ftx, cyl = ra.y - fty;
+      sm.d0[tid] = make_float4(ra.z, ra.w, ox, rb.z * rb.z);
+      sm.d1[tid] = make_float4(rb.x, rb.y, oy, rb.w);
+      sm.d2[tid] = col;
       // Which 8x4 warp blocks the ellipse |local| <= s reaches: for each
       // 4-row band, the x-interval the ellipse spans within the band (plus
-      // half a pixel on every side), tested against the two 8-column blocks.
+      // half a pixel on every side), tested against the 8-column blocks.
       // q(dx, dy) = A dx^2 + 2B dx dy + C dy^2 is |local|^2 in pixel units.
-      const float qa = fmaf(a.z, a.z, b.x * b.x);
-      const float qb = fmaf(a.z, a.w, b.x * b.y);
-      const float qc = fmaf(a.w, a.w, b.y * b.y);
-      const float s2 = b.z * b.z;
+      const float qa = fmaf(ra.z, ra.z, rb.x * rb.x);
+      const float qb = fmaf(ra.z, ra.w, rb.x * rb.y);
+      const float qc = fmaf(ra.w, ra.w, rb.y * rb.y);
+      const float s2 = rb.z * rb.z;
       const float det = fmaf(qa, qc, -qb * qb);
       const float inv_a = 1.0f / qa;
       const float hx = sqrtf(s2 * qc / det);
@@ -231,33 +230,33 @@ __global__ void __launch_bounds__(kTile *kTile) raster_fp32_kernel(
         float xmax = fmaxf((-qb * lo + r_lo) * inv_a, (-qb * hi + r_hi) * inv_a);
         if (dy_left >= lo && dy_left <= hi) xmin = -hx;
         if (-dy_left >= lo && -dy_left <= hi) xmax = hx;
-        const float x0 = cxl + xmin - 0.5f, x1 = cxl + xmax + 0.5f;
+        const float bx0f = cxl + xmin - 0.5f, bx1f = cxl + xmax + 0.5f;
 #pragma unroll
-        for (int col = 0; col < kBlocksX; ++col)
-          if (x1 >= (float)(8 * col) && x0 <= (float)(8 * col + 7))
-            mask |= 1u << (band * kBlocksX + col);
+        for (int colb = 0; colb < kBlocksX; ++colb)
+          if (bx1f >= (float)(8 * colb) && bx0f <= (float)(8 * colb + 7))
+            mask |= 1u << (band * kBlocksX + colb);
       }
       // A degenerate conic (never expected: axes are clamped to an
       // anisotropy of 64) falls back to every block.
       if (!(det > 0.0f) || !(hx < 3.0e38f) || !(hy < 3.0e38f)) mask = (1u << kWarps) - 1u;
-      s_mask[tid] = (uint8_t)mask;
+      sm.mask[tid] = (uint8_t)mask;
     }
     __syncthreads();
     // Ordered compaction of this warp's entries.
     uint32_t n_w = 0;
     for (uint32_t k0 = 0; k0 < n_in; k0 += 32) {
       uint32_t k = k0 + lane;
-      bool hit = k < n_in && ((s_mask[k] >> warp) & 1u);
+      bool hit = k < n_in && ((sm.mask[k] >> warp) & 1u);
       uint32_t bal = __ballot_sync(0xffffffffu, hit);
-      if (hit) s_list[warp][n_w + __popc(bal & lanemask_lt())] = (uint16_t)k;
+      if (hit) sm.list[warp][n_w + __popc(bal & lanemask_lt())] = (uint16_t)k;
       n_w += __popc(bal);
     }
     __syncwarp();
     for (uint32_t i = 0; i < n_w; ++i) {
       if (__all_sync(0xffffffffu, done)) break;
-      const uint32_t j = s_list[warp][i];
-      const float4 d0 = s_d0[j];
-      const float4 d1 = s_d1[j];
+      const uint32_t j = sm.list[warp][i];
+      const float4 d0 = sm.d0[j];
+      const float4 d1 = sm.d1[j];
       float lx = fmaf(d0.x, fx, fmaf(d0.y, fy, d0.z));
       float ly = fmaf(d1.x, fx, fmaf(d1.y, fy, d1.z));
       float r2 = fmaf(lx, lx, ly * ly);
@@ -265,7 +264,7 @@ __global__ void __launch_bounds__(kTile *kTile) raster_fp32_kernel(
       float g = gauss_weight(r2);
       float w = d1.w * g;
       if (!(w > 1.0f / 256.0f)) continue;
-      const float4 col = s_d2[j];
+      const float4 col = sm.d2[j];
       float gT = g * T;
       c0 = fmaf(col.x, gT, c0);
       c1 = fmaf(col.y, gT, c1);
@@ -273,7 +272,7 @@ __global__ void __launch_bounds__(kTile *kTile) raster_fp32_kernel(
       T = T * (1.0f - w);
       if (T < 1e-4f) done = true;
     }
-    if (__syncthreads_count(done) == kN) break;
+    if (__syncthreads_count(done) == kTile * kTile) break;
   }
   cp_async_wait_all();
   if (inside)
@@ -281,25 +280,64 @@ __global__ void __launch_bounds__(kTile *kTile) raster_fp32_kernel(
                                        (to_unorm8(c2) << 16) | (to_unorm8(1.0f - T) << 24);
 }
 
+// One block per tile (kPersistent false), or a fixed grid of blocks that take
+// tiles from a global queue (an atomic ticket over the batch's tiles) until
+// it is empty.
+template <int kTile, int kChunk, bool kPersistent>
+__global__ void __launch_bounds__(kTile *kTile) raster_fp32_kernel(RasterArgs a) {
+  __shared__ Fp32Smem<kTile, kChunk> sm;
+  fold_errors(a);
+  if constexpr (!kPersistent) {
+    raster_fp32_tile<kTile, kChunk>(a, blockIdx.x, sm);
+  } else {
+    for (;;) {
+      if (threadIdx.x == 0) sm.next = atomicAdd(&a.counters->raster_ticket, 1u);
+      __syncthreads();
+      const uint32_t tile = sm.next;
+      if (tile >= a.total_tiles) break;
+      raster_fp32_tile<kTile, kChunk>(a, tile, sm);
+      __syncthreads();  // shared memory is reused by the next tile
+    }
+  }
+}
+
 }  // namespace
 
-void launch_raster(const ViewDev *views, uint32_t num_views, uint32_t total_tiles, uint32_t tile,
-                   const uint2 *ranges, const SortPlan *tile_plan, const uint32_t *ids0,
-                   const uint32_t *ids1, const Record *records, uint32_t *images,
-                   uint32_t blend_mode, const FrameCounters *counters, uint32_t *sticky,
-                   cudaStream_t stream) {
-  if (total_tiles == 0) return;
-  if (tile == 16) {
-    if (blend_mode == 1)
-      raster_unorm8_kernel<16><<<total_tiles, 256, 0, stream>>>(views, num_views, ranges, tile_plan, ids0, ids1, records, images, counters, sticky);
+void launch_raster(const RasterArgs &a, uint32_t tile, uint32_t blend_mode,
+                   const RasterConfig &cfg, uint32_t sm_count, cudaStream_t stream) {
+  if (a.total_tiles == 0) return;
+  if (blend_mode == 1) {
+    if (tile == 16)
+      raster_unorm8_kernel<16><<<a.total_tiles, 256, 0, stream>>>(a);
     else
-      raster_fp32_kernel<16><<<total_tiles, 256, 0, stream>>>(views, num_views, ranges, tile_plan, ids0, ids1, records, images, counters, sticky);
-  } else {
-    if (blend_mode == 1)
-      raster_unorm8_kernel<8><<<total_tiles, 64, 0, stream>>>(views, num_views, ranges, tile_plan, ids0, ids1, records, images, counters, sticky);
-    else
-      raster_fp32_kernel<8><<<total_tiles, 64, 0, stream>>>(views, num_views, ranges, tile_plan, ids0, ids1, records, images, counters, sticky);
+      raster_unorm8_kernel<8><<<a.total_tiles, 64, 0, stream>>>(a);
+    return;
   }
+  const bool persistent = cfg.blocks_per_sm > 0;
+  const uint32_t grid =
+      persistent ? std::min<uint32_t>(a.total_tiles, cfg.blocks_per_sm * sm_count) : a.total_tiles;
+#define GSR_FP32(T, C)                                                           \
+  do {                                                                           \
+    if (persistent)                                                              \
+      raster_fp32_kernel<T, C, true><<<grid, T * T, 0, stream>>>(a);             \
+    else                                                                         \
+      raster_fp32_kernel<T, C, false><<<grid, T * T, 0, stream>>>(a);            \
+  } while (0)
+  if (tile == 16) {
+    if (cfg.chunk == 64) GSR_FP32(16, 64);
+    else if (cfg.chunk == 128) GSR_FP32(16, 128);
+    else GSR_FP32(16, 256);
+  } else {
+    if (cfg.chunk == 32) GSR_FP32(8, 32);
+    else GSR_FP32(8, 64);
+  }
+#undef GSR_FP32
+}
+
+bool raster_config_valid(uint32_t tile, const RasterConfig &cfg) {
+  const bool chunk_ok = tile == 16 ? (cfg.chunk == 64 || cfg.chunk == 128 || cfg.chunk == 256)
+                                   : (cfg.chunk == 32 || cfg.chunk == 64);
+  return chunk_ok && cfg.blocks_per_sm <= 32;
 }
 
 }  // namespace gsr

@@ -258,13 +258,18 @@ inline uint32_t tiles_for(uint32_t capacity) {
 }  // namespace
 
 // Scratch layout: [tickets: 64 words][hist: 4*256][status: passes*tiles*256].
+// A workspace sized for `capacity` serves every sort of up to `capacity`
+// items: smaller sorts may run 8 items per thread where a larger one runs 16,
+// and so use more tiles, so the bound takes the 8-per-thread tile count.
 uint64_t sort_work_words(uint32_t capacity, uint32_t passes) {
-  return 64ull + 4ull * 256ull + (uint64_t)passes * tiles_for(capacity) * 256ull;
+  const uint64_t max_tiles = ((uint64_t)capacity + kThreads * 8 - 1) / (kThreads * 8);
+  return 64ull + 4ull * 256ull + (uint64_t)passes * max_tiles * 256ull;
 }
 
 void launch_sort(const SortBuffers &b, cudaStream_t stream) {
   const uint32_t tiles = tiles_for(b.capacity);
-  const uint64_t words = sort_work_words(b.capacity, b.passes);
+  // the words this launch uses (at most sort_work_words(b.capacity, b.passes))
+  const uint64_t words = 64ull + 4ull * 256ull + (uint64_t)b.passes * tiles * 256ull;
   cudaMemsetAsync(b.work, 0, words * sizeof(uint32_t), stream);
   uint32_t *tickets = b.work;
   uint32_t *hist = b.work + 64;

@@ -80,13 +80,34 @@ void launch_ranges(const SortPlan *tile_plan, const uint32_t *keys0, const uint3
                    cudaStream_t stream);
 
 // ---- K4: tile raster ------------------------------------------------------
-// One block per global tile of the batch; images holds every view's RGBA8
-// pixels at views[v].image_base.
-void launch_raster(const ViewDev *views, uint32_t num_views, uint32_t total_tiles, uint32_t tile,
-                   const uint2 *ranges, const SortPlan *tile_plan, const uint32_t *ids0,
-                   const uint32_t *ids1, const Record *records, uint32_t *images,
-                   uint32_t blend_mode, const FrameCounters *counters, uint32_t *sticky,
-                   cudaStream_t stream);
+// images holds every view's RGBA8 pixels at views[v].image_base.
+struct RasterArgs {
+  const ViewDev *views;
+  uint32_t num_views;
+  uint32_t total_tiles;            // global tiles over the views
+  const uint2 *ranges;             // [total_tiles] list ranges
+  const SortPlan *plan;            // selects the buffer holding the sorted ids
+  const uint32_t *ids0, *ids1;
+  const Record *records;
+  uint32_t *images;
+  FrameCounters *counters;         // raster_ticket is the persistent tile queue
+  uint32_t *sticky;
+};
+// Raster launch shape: records staged per step (tile 16: 64/128/256; tile 8:
+// 32/64) and persistent blocks per SM pulling tiles from a global queue
+// (0 = one block per tile). The FP32 mode honours both; UNORM8 parity mode
+// always runs one block per tile with full-tile chunks. No setting changes a
+// pixel.
+struct RasterConfig {
+  uint32_t chunk = 256;
+  uint32_t blocks_per_sm = 0;
+  bool operator==(const RasterConfig &o) const {
+    return chunk == o.chunk && blocks_per_sm == o.blocks_per_sm;
+  }
+};
+bool raster_config_valid(uint32_t tile, const RasterConfig &cfg);
+void launch_raster(const RasterArgs &a, uint32_t tile, uint32_t blend_mode,
+                   const RasterConfig &cfg, uint32_t sm_count, cudaStream_t stream);
 
 // ---- small helpers ----------------------------------------------------------
 void launch_fill_u32(uint32_t *dst, uint32_t value, uint64_t count, cudaStream_t stream);

@@ -84,6 +84,9 @@ std::unique_ptr<DeviceScene> upload_scene(const HostScene &s, cudaStream_t strea
 }
 
 Pipeline::Pipeline(int device, cudaStream_t stream) : device_(device), stream_(stream) {
+  int sms = 0;
+  GSR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
+  sm_count_ = (uint32_t)sms;
   for (auto &ev : ev_) GSR_CUDA(cudaEventCreate(&ev));
   for (auto &ev : slot_ev_) GSR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   GSR_CUDA(cudaMallocHost(&counters_host_, sizeof(FrameCounters)));
@@ -127,6 +130,19 @@ void Pipeline::record(int k) {
     GSR_CUDA(cudaEventRecordWithFlags(ev_[k], stream_, cudaEventRecordExternal));
   else
     GSR_CUDA(cudaEventRecord(ev_[k], stream_));
+}
+
+void Pipeline::set_tile(uint32_t tile) {
+  tile_ = tile;
+  if (!raster_config_valid(tile_, raster_cfg_)) raster_cfg_.chunk = tile_ * tile_;
+}
+
+void Pipeline::set_raster_config(const RasterConfig &c) {
+  if (!raster_config_valid(tile_, c))
+    throw Error(Code::InvalidArgument, "raster chunk " + std::to_string(c.chunk) +
+                                           " or blocks per SM " + std::to_string(c.blocks_per_sm) +
+                                           " not valid for tile size " + std::to_string(tile_));
+  raster_cfg_ = c;
 }
 
 void Pipeline::drop_graph() {
@@ -319,8 +335,9 @@ void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &si
   launch_ranges(tile_plan_, tile_keys0_, tile_keys1_, counters_, (uint32_t)key_cap_, ranges_,
                 stream_);
   record(5);
-  launch_raster(views_dev_, l.views, l.total_tiles, tile_, ranges_, tile_plan_, tile_vals0_,
-                tile_vals1_, records_, images, blend_mode_, counters_, sticky_, stream_);
+  RasterArgs ra{views_dev_, l.views,  l.total_tiles, ranges_,   tile_plan_,
+                tile_vals0_, tile_vals1_, records_,  images, counters_, sticky_};
+  launch_raster(ra, tile_, blend_mode_, raster_cfg_, sm_count_, stream_);
   record(6);
   GSR_CUDA(cudaMemcpyAsync(sinks.counters, counters_, sizeof(FrameCounters),
                            cudaMemcpyDeviceToHost, stream_));
@@ -348,7 +365,8 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
   if (!use_graph_) {
     launch_all(l, images, sinks);
   } else {
-    const GraphKey key{l, images, key_cap_, tile_, blend_mode_, debug_, sinks.counters, sinks.views};
+    const GraphKey key{l,     images,         key_cap_,       tile_,       blend_mode_,
+                       debug_, raster_cfg_, sinks.counters, sinks.views};
     GraphEntry *hit = nullptr;
     for (auto &g : graphs_)
       if (g.key == key) hit = &g;

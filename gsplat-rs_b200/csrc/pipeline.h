@@ -9,6 +9,7 @@
 
 #include "device_types.h"
 #include "gsr_host.h"
+#include "kernels.h"
 
 namespace gsr {
 
@@ -73,13 +74,17 @@ class Pipeline {
   Pipeline(int device, cudaStream_t stream);
   ~Pipeline();
 
-  void set_tile(uint32_t tile) { tile_ = tile; }
+  // Tile size 8 or 16; the raster chunk follows to the nearest valid size.
+  void set_tile(uint32_t tile);
   uint32_t tile() const { return tile_; }
   void set_blend_mode(uint32_t mode) { blend_mode_ = mode; }
   uint32_t blend_mode() const { return blend_mode_; }
   void set_debug(bool on) { debug_ = on; }
   bool debug() const { return debug_; }
   void set_use_graph(bool on) { use_graph_ = on; }
+  // Throws InvalidArgument unless valid for the current tile size.
+  void set_raster_config(const RasterConfig &c);
+  const RasterConfig &raster_config() const { return raster_cfg_; }
 
   // Renders `count` views into `images` (device, RGBA8 words) at the given
   // pixel offsets and waits. Grows the pair buffers and re-runs on overflow.
@@ -139,7 +144,8 @@ class Pipeline {
   int device_;
   cudaStream_t stream_;
   cudaEvent_t ev_[kPhaseCount + 1] = {};
-  uint32_t tile_ = 16, blend_mode_ = 0;
+  uint32_t tile_ = 16, blend_mode_ = 0, sm_count_ = 148;
+  RasterConfig raster_cfg_;
   bool debug_ = false, use_graph_ = true, has_run_ = false, capturing_ = false;
   Layout last_layout_;
   HostSinks last_sinks_;
@@ -189,11 +195,12 @@ class Pipeline {
     uint64_t key_cap;
     uint32_t tile, blend;
     bool debug;
+    RasterConfig raster;
     FrameCounters *host_counters;
     ViewCounters *host_views;
     bool operator==(const GraphKey &o) const {
       return layout == o.layout && images == o.images && key_cap == o.key_cap &&
-             tile == o.tile && blend == o.blend && debug == o.debug &&
+             tile == o.tile && blend == o.blend && debug == o.debug && raster == o.raster &&
              host_counters == o.host_counters && host_views == o.host_views;
     }
   };

@@ -33,6 +33,7 @@ class Renderer {
   uint32_t blend_mode() const { return pipe_->blend_mode(); }
   void set_debug(bool on) { pipe_->set_debug(on); }
   void set_use_graph(bool on) { pipe_->set_use_graph(on); }
+  void set_raster_config(const RasterConfig &c) { pipe_->set_raster_config(c); }
 
   void load_scene(const HostScene &s);
   bool has_scene() const { return scene_ != nullptr; }

@@ -60,6 +60,9 @@ Server::Server(const ServeConfig &cfg) : cfg_(cfg), scenes_(cfg.scene_budget) {
     auto ls = std::make_unique<LaneState>();
     ls->lane = std::make_unique<Lane>(device_);
     ls->lane->pipe().set_tile(cfg.tile);
+    RasterConfig rc = cfg.raster;
+    if (rc.chunk == 0) rc.chunk = cfg.tile * cfg.tile;
+    ls->lane->pipe().set_raster_config(rc);
     ls->server = this;
     lanes_.push_back(std::move(ls));
   }

@@ -32,6 +32,7 @@ struct ServeConfig {
   uint32_t lanes = 2;                    // batches in flight
   uint32_t max_views = 256;              // per batch
   uint32_t tile = 16;
+  RasterConfig raster;  // chunk 0 = full tile
 };
 
 enum class RequestStatus : uint32_t { Queued = 0, Running = 1, Done = 2, Failed = 3 };

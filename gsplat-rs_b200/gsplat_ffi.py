@@ -110,7 +110,15 @@ class GsplatBatchTimes(ctypes.Structure):
 class GsplatServeConfig(ctypes.Structure):
     _fields_ = [("scene_budget_bytes", ctypes.c_uint64), ("work_budget_bytes", ctypes.c_uint64),
                 ("lanes", ctypes.c_uint32), ("max_views_per_batch", ctypes.c_uint32),
-                ("tile_size", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("tile_size", ctypes.c_uint32), ("raster_chunk", ctypes.c_uint32),
+                ("raster_blocks_per_sm", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class GsplatTuneResult(ctypes.Structure):
+    _fields_ = [("tile_size", ctypes.c_uint32), ("chunk", ctypes.c_uint32),
+                ("blocks_per_sm", ctypes.c_uint32), ("candidates", ctypes.c_uint32),
+                ("best_ms", ctypes.c_float), ("default_ms", ctypes.c_float),
+                ("from_cache", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class GsplatRequestInfo(ctypes.Structure):
@@ -190,6 +198,8 @@ _SIGS = [
     ("gsplat_context_set_tile_size", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
     ("gsplat_context_set_debug_taps", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
     ("gsplat_context_set_cuda_graph", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
+    ("gsplat_context_set_raster_config", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]),
     ("gsplat_context_load_scene_buffers", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.POINTER(GsplatSceneDesc)]),
     ("gsplat_context_readback_rgba8", ctypes.c_int32, [ctypes.c_void_p, _u8p, ctypes.c_uint64]),
@@ -223,6 +233,11 @@ _SIGS = [
     ("gsplat_batch_set_blend_mode", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
     ("gsplat_batch_set_limits", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64]),
+    ("gsplat_batch_set_raster_config", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]),
+    ("gsplat_batch_autotune", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.POINTER(GsplatBatchView), ctypes.c_uint32, ctypes.c_char_p,
+      ctypes.c_uint32, ctypes.POINTER(GsplatTuneResult)]),
     ("gsplat_batch_render", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.POINTER(GsplatBatchView), ctypes.c_uint32]),
     ("gsplat_batch_get_times", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(GsplatBatchTimes)]),
@@ -372,6 +387,9 @@ class Context:
     def set_cuda_graph(self, on=True):
         check(lib().gsplat_context_set_cuda_graph(self.ptr, 1 if on else 0))
 
+    def set_raster_config(self, chunk, blocks_per_sm=0):
+        check(lib().gsplat_context_set_raster_config(self.ptr, chunk, blocks_per_sm))
+
     def load_scene_path(self, path):
         check(lib().gsplat_context_load_scene_path(self.ptr, os.fsencode(path)))
 
@@ -504,6 +522,17 @@ class Batch:
     def set_limits(self, max_views=0, max_pairs=0, max_splats=0):
         check(lib().gsplat_batch_set_limits(self.ptr, max_views, max_pairs, max_splats))
 
+    def set_raster_config(self, chunk, blocks_per_sm=0):
+        check(lib().gsplat_batch_set_raster_config(self.ptr, chunk, blocks_per_sm))
+
+    def autotune(self, views, cache_path=None, reps=3):
+        arr = views if isinstance(views, ctypes.Array) else self.make_views(views)
+        r = GsplatTuneResult()
+        check(lib().gsplat_batch_autotune(self.ptr, arr, len(arr),
+                                          os.fsencode(cache_path) if cache_path else None, reps,
+                                          ctypes.byref(r)))
+        return r
+
     @staticmethod
     def make_views(views):
         """views: iterable of (scene, camera, width, height)."""
@@ -551,8 +580,10 @@ class Batch:
 class Server:
     """One GsplatServer: resident scenes and a continuous-batching request loop."""
 
-    def __init__(self, lanes=0, max_views=0, tile=0, scene_budget=0, work_budget=0):
-        cfg = GsplatServeConfig(scene_budget, work_budget, lanes, max_views, tile, 0)
+    def __init__(self, lanes=0, max_views=0, tile=0, scene_budget=0, work_budget=0,
+                 raster_chunk=0, raster_blocks_per_sm=0):
+        cfg = GsplatServeConfig(scene_budget, work_budget, lanes, max_views, tile, raster_chunk,
+                                raster_blocks_per_sm, 0)
         self.ptr = ctypes.c_void_p()
         check(lib().gsplat_server_create(ctypes.byref(cfg), ctypes.byref(self.ptr)))
         self.sizes = {}

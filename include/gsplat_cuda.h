@@ -94,6 +94,12 @@ int32_t gsplat_context_set_debug_taps(GsplatContext *ctx, uint32_t enabled);
  * taps and pair capacity stay the same; disabled, every launch is issued
  * separately. Images are identical either way. */
 int32_t gsplat_context_set_cuda_graph(GsplatContext *ctx, uint32_t enabled);
+/* Raster launch shape of the FP32 mode: records staged per step (`chunk`:
+ * 64, 128 or 256 at tile size 16; 32 or 64 at tile size 8) and persistent
+ * blocks per SM that pull tiles from a global queue (0 = one block per tile,
+ * at most 32). Changing the tile size resets an invalid chunk to the full
+ * tile. Images do not depend on either setting. */
+int32_t gsplat_context_set_raster_config(GsplatContext *ctx, uint32_t chunk, uint32_t blocks_per_sm);
 
 /* Load a scene from host memory (validated like SceneBuffers::validate,
  * crates/gsplat-core/src/lib.rs:224-276). Replaces any loaded scene. */
@@ -223,6 +229,30 @@ int32_t gsplat_batch_set_blend_mode(GsplatBatch *batch, uint32_t mode);      /* 
  * group (0 keeps the current value). */
 int32_t gsplat_batch_set_limits(GsplatBatch *batch, uint32_t max_views, uint64_t max_pairs,
                                 uint64_t max_splats);
+/* As gsplat_context_set_raster_config. */
+int32_t gsplat_batch_set_raster_config(GsplatBatch *batch, uint32_t chunk, uint32_t blocks_per_sm);
+
+typedef struct GsplatTuneResult {
+  uint32_t tile_size;      /* chosen launch shape, now set on the batch */
+  uint32_t chunk;
+  uint32_t blocks_per_sm;
+  uint32_t candidates;     /* shapes timed (0 when taken from the cache) */
+  float best_ms;           /* median device time of the views with it */
+  float default_ms;        /* the same with tile 16, chunk 256, one block per tile */
+  uint32_t from_cache;
+  uint32_t reserved;
+} GsplatTuneResult;        /* 32 bytes */
+
+/* Autotunes the batch's launch shape on `views`: renders them with every
+ * candidate (tile 16 with chunks 256/128/64, tile 8 with chunks 64/32, each
+ * with one block per tile or 2/4 resp. 8/16 persistent blocks per SM), keeps
+ * the fastest by median device time over `reps` renders and sets it on the
+ * batch. With a `cache_path`, results are kept in that text file keyed by GPU
+ * name, blend mode, image sizes and scene-size class, and a later call with
+ * the same key takes the stored shape without rendering. Images are the same
+ * under every candidate. */
+int32_t gsplat_batch_autotune(GsplatBatch *batch, const GsplatBatchView *views, uint32_t count,
+                              const char *cache_path, uint32_t reps, GsplatTuneResult *out_result);
 /* Renders all `count` views and waits until every image is in device memory. */
 int32_t gsplat_batch_render(GsplatBatch *batch, const GsplatBatchView *views, uint32_t count);
 int32_t gsplat_batch_get_times(const GsplatBatch *batch, GsplatBatchTimes *out_times);
@@ -257,8 +287,10 @@ typedef struct GsplatServeConfig {
   uint32_t lanes;               /* batches in flight, 1..8; 0 = 2 */
   uint32_t max_views_per_batch; /* 1..1024; 0 = 256 */
   uint32_t tile_size;           /* 8 or 16; 0 = 16 */
+  uint32_t raster_chunk;        /* as gsplat_context_set_raster_config; 0 = full tile */
+  uint32_t raster_blocks_per_sm;/* 0 = one block per tile */
   uint32_t reserved;            /* 0 */
-} GsplatServeConfig;            /* 32 bytes */
+} GsplatServeConfig;            /* 40 bytes */
 
 typedef enum GsplatRequestStatus {
   GSPLAT_REQUEST_QUEUED = 0,

@@ -163,3 +163,34 @@ def test_batch_errors():
         with pytest.raises(ffi.GsplatError) as e:
             b.set_limits(max_views=2000)
         assert e.value.code == ffi.INVALID_ARGUMENT
+
+
+def test_batch_autotune_and_cache(tmp_path):
+    scenes = _scenes()
+    rng = np.random.default_rng(21)
+    views = _views(rng, 8, len(scenes))
+    cache = str(tmp_path / "tune.txt")
+    with ffi.Batch() as b:
+        for s in scenes:
+            b.add_scene(s)
+        b.render(views)
+        before = [b.readback_rgba8(k).copy() for k in range(len(views))]
+        r = b.autotune(views, cache, reps=1)
+        assert r.candidates == 15 and not r.from_cache
+        assert 0 < r.best_ms <= r.default_ms * 1.0001
+        assert r.tile_size in (8, 16)
+        b.render(views)
+        for k in range(len(views)):
+            assert np.array_equal(b.readback_rgba8(k), before[k]), k
+        text = open(cache).read().splitlines()
+        assert text[0] == "gsplat-cuda-autotune v1" and len(text) == 2
+        assert "|blend0|" in text[1]
+    with ffi.Batch() as b:
+        for s in scenes:
+            b.add_scene(s)
+        r2 = b.autotune(views, cache)
+        assert r2.from_cache and r2.candidates == 0
+        assert (r2.tile_size, r2.chunk, r2.blocks_per_sm) == (r.tile_size, r.chunk, r.blocks_per_sm)
+        b.render(views)
+        for k in range(len(views)):
+            assert np.array_equal(b.readback_rgba8(k), before[k]), k

@@ -321,6 +321,60 @@ def test_cuda_graph_replay_matches_direct_launches(oracle):
     assert np.array_equal(graph.readback_rgba8(), direct.readback_rgba8())
 
 
+def test_smaller_scene_after_larger_reuses_workspace(oracle):
+    """A workspace sized by a sort above 2M keys (16 keys per thread) must
+    also serve a later, smaller sort that runs 8 keys per thread and so has
+    more tiles: plain context and batch lane alike."""
+    rng = np.random.default_rng(31)
+    big = gsplat_scenes.make_scene(rng, gsplat_scenes.gmm_means(rng, 2_300_000), -5.0, 0.5, 0.5,
+                                   1.5, 0)
+    small = gsplat_scenes.make_scene(rng, gsplat_scenes.gmm_means(rng, 1_200_000), -5.0, 0.5, 0.5,
+                                     1.5, 0)
+    cam = gsplat_scenes.camera((0.0, 0.5, -5.0), (0, 0, 0), 50.0)
+    w, h = 320, 240
+    ref = oracle.Frame(oracle.SceneView(small), cam, w, h).raster_tiles_fp32()
+    ctx = _ctx(w, h)
+    ctx.load_scene(big)
+    ctx.set_camera(cam)
+    ctx.render_frame()
+    ctx.load_scene(small)
+    ctx.render_frame()
+    assert np.array_equal(ctx.readback_rgba8(), ref)
+    with ffi.Batch() as b:
+        b.add_scene(big)
+        b.add_scene(small)
+        b.render([(0, cam, w, h)])
+        b.render([(1, cam, w, h)])
+        assert np.array_equal(b.readback_rgba8(0), ref)
+
+
+RASTER_SHAPES = [(16, c, b) for c in (256, 128, 64) for b in (0, 2, 4)] + \
+    [(8, c, b) for c in (64, 32) for b in (0, 8, 16)]
+
+
+def test_raster_launch_shapes_do_not_change_pixels(oracle):
+    """Every tile size, chunk size and persistent-queue setting the autotuner
+    may pick gives the oracle's image bit for bit."""
+    scene, cam, w, h = gsplat_scenes.config1(seed=12)
+    ref = oracle.Frame(oracle.SceneView(scene), cam, w + 37, h + 5).raster_tiles_fp32()
+    ctx = _ctx(w + 37, h + 5)
+    ctx.load_scene(scene)
+    ctx.set_camera(cam)
+    for tile, chunk, bps in RASTER_SHAPES:
+        ctx.set_tile_size(tile)
+        ctx.set_raster_config(chunk, bps)
+        ctx.render_frame()
+        assert np.array_equal(ctx.readback_rgba8(), ref), (tile, chunk, bps)
+    with pytest.raises(ffi.GsplatError) as e:
+        ctx.set_raster_config(256, 0)  # tile size is 8 now
+    assert e.value.code == ffi.INVALID_ARGUMENT
+    ctx.set_tile_size(16)
+    with pytest.raises(ffi.GsplatError):
+        ctx.set_raster_config(96, 0)
+    with pytest.raises(ffi.GsplatError):
+        ctx.set_raster_config(256, 33)
+
+
 def test_c_smoke_programs_run():
     exe = os.path.join(ROOT, "tests", "ffi", "_build_smoke")
     subprocess.run(["gcc", "-O2", "-I", os.path.join(ROOT, "include"),
