@@ -221,10 +221,12 @@ def measure_batched(ffi, torch, steps, warmup):
     for _ in range(max(warmup, 2)):
         b.render(arr)
     dev, wall = [], []
+    torch.cuda.nvtx.range_push("batched_timed")  # ncu --nvtx-include batched_timed/
     for _ in range(steps):
         t = b.render(arr)
         dev.append(t.device_ms)
         wall.append(t.wall_ms)
+    torch.cuda.nvtx.range_pop()
     t = b.times()
     pixels = sum(w * h for _, _, w, h in specs)
     # e2e: cameras in, all images read back into pinned host memory
@@ -399,12 +401,27 @@ def measure_served(ffi, rates, seconds, max_requests):
             "rates": out}
 
 
+def run_sections_only(args, ffi, torch):
+    """The batched and/or served sections alone (no plain-frame line), for
+    profiling those workloads by themselves."""
+    out = {"metric": METRIC, "sections": args.only}
+    if "batched" in args.only:
+        out["batched"] = measure_batched(ffi, torch, args.batch_steps, args.warmup)
+    if "served" in args.only:
+        out["served"] = measure_served(ffi, [float(x) for x in args.serve_rates.split(",")],
+                                       args.serve_seconds, 4000)
+    print(json.dumps(out), flush=True)
+
+
 def run_cuda(args, world, rank, local):
     import torch
 
     import gsplat_ffi as ffi
 
     torch.cuda.set_device(local)
+    if args.only:
+        run_sections_only(args, ffi, torch)
+        return
     if world > 1:
         import datetime
 
@@ -506,7 +523,9 @@ def run_cuda(args, world, rank, local):
         b = algorithmic_bytes(k, counts, scene["positions"].shape[0], planes, w, h, tile_passes)
         phase_rooflines[k] = {"ms": ms, "bytes": b, "gbs": b / (ms * 1e-3) / 1e9 if ms > 0 else None}
 
-    launches_per_frame = 1 + (2 + 4) + 1 + (2 + tile_passes) + 1 + 1
+    # preprocess; depth sort: plan + 4 passes (histograms from K1); emit; tile
+    # sort: plan + passes (histograms from K2); ranges; raster
+    launches_per_frame = 1 + (1 + 4) + 1 + (1 + tile_passes) + 1 + 1
     line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_frame,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -519,9 +538,9 @@ def run_cuda(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(scene, cam, w, h, budget_s=args.cpu_budget)
     ctx.close()
-    if not args.no_batched:
+    if not args.no_batched and world == 1:
         line["batched"] = measure_batched(ffi, torch, args.batch_steps, 2)
-    if not args.no_served:
+    if not args.no_served and world == 1:
         line["served"] = measure_served(ffi, [float(x) for x in args.serve_rates.split(",")],
                                         args.serve_seconds, 4000)
     if world > 1:
@@ -543,7 +562,10 @@ def main():
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--serve-rates", default="500,2000,8000,20000")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
+    ap.add_argument("--only", default="",
+                    help="comma list of batched,served: run just those sections (profiling)")
     args = ap.parse_args()
+    args.only = [x for x in args.only.split(",") if x]
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)

@@ -254,13 +254,27 @@ void Batch::set_limits(const GroupLimits &l) {
   limits_ = l;
 }
 
-BatchResult Batch::render(const std::vector<BatchView> &views) {
+BatchResult Batch::render(const std::vector<BatchView> &in) {
   auto t0 = std::chrono::steady_clock::now();
-  if (views.empty()) throw Error(Code::InvalidArgument, "no views to render");
+  if (in.empty()) throw Error(Code::InvalidArgument, "no views to render");
   has_images_ = false;
-  const uint64_t pixels = make_view_specs(scenes_, views.data(), (uint32_t)views.size(), specs_, bases_);
-  std::vector<uint64_t> predicted(views.size());
-  for (size_t v = 0; v < views.size(); ++v)
+  // Views of one scene render next to each other, so the pipeline's view
+  // sets read each scene once for all of them; results keep the caller's
+  // order through pos_.
+  const uint32_t n = (uint32_t)in.size();
+  std::vector<uint32_t> order(n);
+  for (uint32_t v = 0; v < n; ++v) order[v] = v;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](uint32_t a, uint32_t b) { return in[a].scene < in[b].scene; });
+  std::vector<BatchView> views(n);
+  pos_.resize(n);
+  for (uint32_t j = 0; j < n; ++j) {
+    views[j] = in[order[j]];
+    pos_[order[j]] = j;
+  }
+  const uint64_t pixels = make_view_specs(scenes_, views.data(), n, specs_, bases_);
+  std::vector<uint64_t> predicted(n);
+  for (uint32_t v = 0; v < n; ++v)
     predicted[v] = predictor_.predict(views[v].scene, specs_[v].scene->n, views[v].width,
                                       views[v].height, tile_);
   groups_ = plan_groups(specs_, predicted, tile_, limits_);
@@ -272,8 +286,8 @@ BatchResult Batch::render(const std::vector<BatchView> &views) {
   r.device_ms = lane_->device_ms();
   r.groups = (uint32_t)groups_.size();
   r.launches = r.groups * lane_->pipe().launches_per_run();
-  stats_.assign(lane_->view_counters(), lane_->view_counters() + views.size());
-  for (size_t v = 0; v < views.size(); ++v) {
+  stats_.assign(lane_->view_counters(), lane_->view_counters() + n);
+  for (uint32_t v = 0; v < n; ++v) {
     predictor_.observe(views[v].scene, specs_[v].scene->n, views[v].width, views[v].height, tile_,
                        stats_[v].pairs);
     r.pairs += stats_[v].pairs;
@@ -284,23 +298,25 @@ BatchResult Batch::render(const std::vector<BatchView> &views) {
   return r;
 }
 
-const ViewCounters &Batch::view_stats(uint32_t view) const {
-  if (!has_images_ || view >= stats_.size())
+uint32_t Batch::position(uint32_t view) const {
+  if (!has_images_ || view >= pos_.size())
     throw Error(Code::InvalidArgument, "no rendered view " + std::to_string(view));
-  return stats_[view];
+  return pos_[view];
 }
 
+const ViewCounters &Batch::view_stats(uint32_t view) const { return stats_[position(view)]; }
+
 uint32_t Batch::view_group(uint32_t view) const {
+  const uint32_t j = position(view);
   for (uint32_t g = 0; g < groups_.size(); ++g)
-    if (view >= groups_[g].first && view < groups_[g].first + groups_[g].count) return g;
+    if (j >= groups_[g].first && j < groups_[g].first + groups_[g].count) return g;
   throw Error(Code::InvalidArgument, "no rendered view " + std::to_string(view));
 }
 
 const uint32_t *Batch::image_device(uint32_t view, uint64_t *bytes) const {
-  if (!has_images_ || view >= specs_.size())
-    throw Error(Code::InvalidArgument, "no rendered view " + std::to_string(view));
-  if (bytes) *bytes = 4ull * specs_[view].width * specs_[view].height;
-  return lane_->images() + bases_[view];
+  const uint32_t j = position(view);
+  if (bytes) *bytes = 4ull * specs_[j].width * specs_[j].height;
+  return lane_->images() + bases_[j];
 }
 
 void Batch::readback_rgba8(uint32_t view, uint8_t *out, uint64_t len) {

@@ -153,6 +153,7 @@ class Batch {
   // Renders every view; blocks until all images are in HBM.
   BatchResult render(const std::vector<BatchView> &views);
   uint32_t view_count() const { return (uint32_t)specs_.size(); }
+  // Per-view results by the caller's view index.
   const ViewCounters &view_stats(uint32_t view) const;
   uint32_t view_group(uint32_t view) const;
   // Device pointer to a view's RGBA8 image (valid until the next render).
@@ -168,8 +169,10 @@ class Batch {
   SceneStore scenes_;
   PairPredictor predictor_;
   std::unique_ptr<Lane> lane_;
-  std::vector<ViewSpec> specs_;
+  uint32_t position(uint32_t view) const;  // caller index -> render position
+  std::vector<ViewSpec> specs_;            // render order (views grouped by scene)
   std::vector<uint64_t> bases_;
+  std::vector<uint32_t> pos_;
   std::vector<ViewGroup> groups_;
   std::vector<ViewCounters> stats_;
   BatchResult last_;

@@ -72,11 +72,21 @@ struct ViewDev {
   FrameParams p;       // per-view uniforms (camera, image size, tile grid)
   SceneDev sc;         // the view's scene
   uint32_t splat_base; // first gid of the view
-  uint32_t block_base; // first preprocess block of the view
+  uint32_t set;        // the view set (views of one scene) the view belongs to
   uint32_t tile_base;  // first global tile id of the view
   uint32_t pad;
   unsigned long long image_base;  // first pixel of the view's image
 };
+
+// Consecutive views of one scene that the preprocess kernel handles together
+// (one read of the scene planes for all of them).
+struct ViewSetDev {
+  uint32_t first_view;  // index into the view table
+  uint32_t count;       // 1..kMaxSetViews
+  uint32_t block_base;  // first preprocess block of the set
+  uint32_t pad;
+};
+constexpr uint32_t kMaxSetViews = 16;
 
 // Per-view counters of a batch (zeroed per batch).
 struct ViewCounters {

@@ -254,86 +254,107 @@ __device__ __forceinline__ bool project(const SceneDev &sc, const FrameParams &p
 }
 
 constexpr int kK1Threads = 256;
+constexpr int kK1Warps = kK1Threads / 32;
+// Resident blocks per SM the register allocation must allow (tuning knob).
+#ifndef GSR_K1_MIN_BLOCKS
+#define GSR_K1_MIN_BLOCKS 3
+#endif
 
+// One block covers 256 consecutive splats of one scene for every view of a
+// view set (up to kMaxSetViews views of that scene), so the scene planes are
+// read from HBM once per set instead of once per view (the later views of
+// the set find them in L1/L2). Per view, the arithmetic is exactly the
+// single-view sequence. Visible entries are compacted in (block, view, id)
+// order, which keeps every view's entries in ascending id order.
 template <int kPlanes, bool kDebug>
-__global__ void __launch_bounds__(kK1Threads) preprocess_kernel(const ViewDev *__restrict__ views,
-                                                                uint32_t num_views,
-                                                                uint32_t total_blocks,
-                                                                K1Buffers b) {
+__global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
+    preprocess_kernel(const ViewDev *__restrict__ views, const ViewSetDev *__restrict__ sets,
+                      uint32_t num_sets, uint32_t total_blocks, K1Buffers b) {
   __shared__ uint32_t s_block;
-  __shared__ uint32_t s_view;
-  __shared__ uint32_t s_warp[kK1Threads / 32];
+  __shared__ uint32_t s_set;
+  __shared__ uint32_t s_cnt[kMaxSetViews][kK1Warps];  // visible per view and warp
   __shared__ uint32_t s_hist[4][256];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) {
     const uint32_t blk = atomicAdd(&b.counters->k1_ticket, 1u);
     s_block = blk;
-    s_view = find_view(num_views, blk, [&](uint32_t v) { return views[v].block_base; });
+    s_set = find_view(num_sets, blk, [&](uint32_t v) { return sets[v].block_base; });
   }
   for (uint32_t k = threadIdx.x; k < 4 * 256; k += kK1Threads) (&s_hist[0][0])[k] = 0;
   __syncthreads();
   const uint32_t block = s_block;
-  const uint32_t view = s_view;
-  const FrameParams p = views[view].p;
-  const SceneDev sc = views[view].sc;
-  const uint32_t i = (block - views[view].block_base) * kK1Threads + threadIdx.x;
-  const uint32_t gid = views[view].splat_base + i;
+  const ViewSetDev set = sets[s_set];
+  const SceneDev sc = views[set.first_view].sc;
+  const uint32_t i = (block - set.block_base) * kK1Threads + threadIdx.x;
   const bool valid = i < sc.n;
+  const float4 pa = valid ? sc.pos_alpha[i] : make_float4(0.f, 0.f, 0.f, 0.f);
 
-  float4 pa = valid ? sc.pos_alpha[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-  float rel[3] = {pa.x - p.cam[0], pa.y - p.cam[1], pa.z - p.cam[2]};
-  float depth = p.r2[0] * rel[0] + p.r2[1] * rel[1] + p.r2[2] * rel[2];
-  const bool vis = valid && depth >= p.near_plane && depth <= p.far_plane;
-
-  // The block's visible count is known right after the depth test: publish
-  // it for the successors' look-back before doing the heavy vertex stage.
-  const uint32_t ballot = __ballot_sync(0xffffffffu, vis);
-  const uint32_t rank = __popc(ballot & lanemask_lt());
-  if (lane == 0) s_warp[warp] = __popc(ballot);
+  // Depth test for every view of the set. The block's visible count is
+  // known right after it: publish it for the successors' look-back before
+  // doing the heavy vertex stage.
+  uint32_t vis_bits = 0;
+  for (uint32_t k = 0; k < set.count; ++k) {
+    const FrameParams &p = views[set.first_view + k].p;
+    const float rx = pa.x - p.cam[0], ry = pa.y - p.cam[1], rz = pa.z - p.cam[2];
+    const float depth = p.r2[0] * rx + p.r2[1] * ry + p.r2[2] * rz;
+    const bool vis = valid && depth >= p.near_plane && depth <= p.far_plane;
+    const uint32_t ballot = __ballot_sync(0xffffffffu, vis);
+    if (lane == 0) s_cnt[k][warp] = __popc(ballot);
+    vis_bits |= (vis ? 1u : 0u) << k;
+  }
   __syncthreads();
-  uint32_t warp_prefix = 0, block_total = 0;
+  uint32_t block_total = 0;
+  for (uint32_t k = 0; k < set.count; ++k)
 #pragma unroll
-  for (int w = 0; w < kK1Threads / 32; ++w) {
-    uint32_t c = s_warp[w];
-    warp_prefix += (w < (int)warp) ? c : 0u;
-    block_total += c;
-  }
-  if (threadIdx.x == 0) {
-    lookback_publish_aggregate(b.status, block, block_total);
-    if (block_total) atomicAdd(&b.view_counters[view].visible, block_total);
+    for (int w = 0; w < kK1Warps; ++w) block_total += s_cnt[k][w];
+  if (threadIdx.x == 0) lookback_publish_aggregate(b.status, block, block_total);
+  if (threadIdx.x < set.count) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int w = 0; w < kK1Warps; ++w) c += s_cnt[threadIdx.x][w];
+    if (c) atomicAdd(&b.view_counters[set.first_view + threadIdx.x].visible, c);
   }
 
-  ProjectedDev *dbg = nullptr;
-  if (kDebug && valid) {
-    dbg = &b.projected[gid];
-    ProjectedDev z = {};
-    z.depth = depth;
-    z.flags = vis ? 1u : 0u;
-    *dbg = z;
-  }
-  const uint32_t key = ~__float_as_uint(fmaxf(depth, 0.0f));
-  uint32_t area = 0;  // tile pairs this splat will emit
-  if (vis) {
-    Record rec;
-    uint2 rect = make_uint2(0u, 0u);
-    bool drawn = project<kPlanes>(sc, p, i, pa, rel, depth, rec, rect, dbg);
-    b.rects[gid] = rect;
-    area = ((rect.y & 0xffffu) - (rect.x & 0xffffu)) * ((rect.y >> 16) - (rect.x >> 16));
-    if (drawn) {
-      b.records[gid] = rec;
-      uint32_t dmask = __ballot_sync(__activemask(), true);
-      if (lane == __ffs(dmask) - 1) {
+  for (uint32_t k = 0; k < set.count; ++k) {
+    const uint32_t view = set.first_view + k;
+    const FrameParams &p = views[view].p;
+    const uint32_t gid = views[view].splat_base + i;
+    const bool vis = (vis_bits >> k) & 1u;
+    float rel[3] = {pa.x - p.cam[0], pa.y - p.cam[1], pa.z - p.cam[2]};
+    const float depth = p.r2[0] * rel[0] + p.r2[1] * rel[1] + p.r2[2] * rel[2];
+    ProjectedDev *dbg = nullptr;
+    if (kDebug && valid) {
+      dbg = &b.projected[gid];
+      ProjectedDev z = {};
+      z.depth = depth;
+      z.flags = vis ? 1u : 0u;
+      *dbg = z;
+    }
+    uint32_t area = 0;  // tile pairs this splat will emit for the view
+    bool drawn = false;
+    if (vis) {
+      Record rec;
+      uint2 rect = make_uint2(0u, 0u);
+      drawn = project<kPlanes>(sc, p, i, pa, rel, depth, rec, rect, dbg);
+      b.rects[gid] = rect;
+      if (drawn) b.records[gid] = rec;
+      area = ((rect.y & 0xffffu) - (rect.x & 0xffffu)) * ((rect.y >> 16) - (rect.x >> 16));
+      // Digit histograms of the depth keys for every radix pass.
+      const uint32_t key = ~__float_as_uint(fmaxf(depth, 0.0f));
+#pragma unroll
+      for (int d = 0; d < 4; ++d) atomicAdd(&s_hist[d][(key >> (8 * d)) & 255u], 1u);
+    }
+    const uint32_t dmask = __ballot_sync(0xffffffffu, drawn);
+    area = warp_sum(area);
+    if (lane == 0) {
+      if (dmask) {
         atomicAdd(&b.counters->drawn, __popc(dmask));
         atomicAdd(&b.view_counters[view].drawn, __popc(dmask));
       }
+      if (area) atomicAdd(&b.view_counters[view].pairs, area);
     }
-    // Digit histograms of the depth keys for every radix pass.
-#pragma unroll
-    for (int d = 0; d < 4; ++d) atomicAdd(&s_hist[d][(key >> (8 * d)) & 255u], 1u);
   }
-  // Per-view pair count (what K2 will emit for this view), one add per warp.
-  area = warp_sum(area);
-  if (lane == 0 && area) atomicAdd(&b.view_counters[view].pairs, area);
+
   // Every warp resolves the block's offset on its own (no second block
   // barrier); warp 0 publishes the inclusive prefix.
   const unsigned long long prefix = lookback_resolve(b.status, block, &b.counters->error);
@@ -341,10 +362,27 @@ __global__ void __launch_bounds__(kK1Threads) preprocess_kernel(const ViewDev *_
     lookback_publish_inclusive(b.status, block, prefix + block_total);
     if (block == total_blocks - 1) b.counters->visible = (uint32_t)(prefix + block_total);
   }
-  if (vis) {
-    const uint32_t slot = (uint32_t)prefix + warp_prefix + rank;
-    b.vis_keys[slot] = key;
-    b.vis_ids[slot] = gid;
+  uint32_t slot = (uint32_t)prefix;
+  for (uint32_t k = 0; k < set.count; ++k) {
+    uint32_t warp_prefix = 0, view_total = 0;
+#pragma unroll
+    for (int w = 0; w < kK1Warps; ++w) {
+      const uint32_t c = s_cnt[k][w];
+      warp_prefix += (w < (int)warp) ? c : 0u;
+      view_total += c;
+    }
+    const bool vis = (vis_bits >> k) & 1u;
+    const uint32_t bal = __ballot_sync(0xffffffffu, vis);
+    if (vis) {
+      const uint32_t view = set.first_view + k;
+      const FrameParams &p = views[view].p;
+      const float rx = pa.x - p.cam[0], ry = pa.y - p.cam[1], rz = pa.z - p.cam[2];
+      const float depth = p.r2[0] * rx + p.r2[1] * ry + p.r2[2] * rz;
+      const uint32_t at = slot + warp_prefix + __popc(bal & lanemask_lt());
+      b.vis_keys[at] = ~__float_as_uint(fmaxf(depth, 0.0f));
+      b.vis_ids[at] = views[view].splat_base + i;
+    }
+    slot += view_total;
   }
   __syncthreads();
   for (uint32_t k = threadIdx.x; k < 4 * 256; k += kK1Threads) {
@@ -354,28 +392,29 @@ __global__ void __launch_bounds__(kK1Threads) preprocess_kernel(const ViewDev *_
 }
 
 template <int kPlanes>
-void launch_k1(const ViewDev *views, uint32_t num_views, uint32_t total_blocks, const K1Buffers &b,
-               bool debug, cudaStream_t stream) {
+void launch_k1(const ViewDev *views, const ViewSetDev *sets, uint32_t num_sets,
+               uint32_t total_blocks, const K1Buffers &b, bool debug, cudaStream_t stream) {
   if (total_blocks == 0) return;
   if (debug)
-    preprocess_kernel<kPlanes, true><<<total_blocks, kK1Threads, 0, stream>>>(views, num_views,
-                                                                              total_blocks, b);
+    preprocess_kernel<kPlanes, true>
+        <<<total_blocks, kK1Threads, 0, stream>>>(views, sets, num_sets, total_blocks, b);
   else
-    preprocess_kernel<kPlanes, false><<<total_blocks, kK1Threads, 0, stream>>>(views, num_views,
-                                                                               total_blocks, b);
+    preprocess_kernel<kPlanes, false>
+        <<<total_blocks, kK1Threads, 0, stream>>>(views, sets, num_sets, total_blocks, b);
 }
 
 }  // namespace
 
 uint32_t preprocess_blocks(uint32_t splats) { return (splats + kK1Threads - 1) / kK1Threads; }
 
-void launch_preprocess(const ViewDev *views, uint32_t num_views, uint32_t total_blocks,
-                       uint32_t max_planes, const K1Buffers &b, bool debug, cudaStream_t stream) {
-  if (max_planes <= 1) launch_k1<1>(views, num_views, total_blocks, b, debug, stream);
-  else if (max_planes <= 3) launch_k1<3>(views, num_views, total_blocks, b, debug, stream);
-  else if (max_planes <= 7) launch_k1<7>(views, num_views, total_blocks, b, debug, stream);
-  else if (max_planes <= 12) launch_k1<12>(views, num_views, total_blocks, b, debug, stream);
-  else launch_k1<19>(views, num_views, total_blocks, b, debug, stream);
+void launch_preprocess(const ViewDev *views, const ViewSetDev *sets, uint32_t num_sets,
+                       uint32_t total_blocks, uint32_t max_planes, const K1Buffers &b, bool debug,
+                       cudaStream_t stream) {
+  if (max_planes <= 1) launch_k1<1>(views, sets, num_sets, total_blocks, b, debug, stream);
+  else if (max_planes <= 3) launch_k1<3>(views, sets, num_sets, total_blocks, b, debug, stream);
+  else if (max_planes <= 7) launch_k1<7>(views, sets, num_sets, total_blocks, b, debug, stream);
+  else if (max_planes <= 12) launch_k1<12>(views, sets, num_sets, total_blocks, b, debug, stream);
+  else launch_k1<19>(views, sets, num_sets, total_blocks, b, debug, stream);
 }
 
 }  // namespace gsr

@@ -27,6 +27,15 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+// Tuning knobs: resident pass blocks per SM the register allocation must
+// allow, and predecessor tiles read per look-back step.
+#ifndef GSR_SORT_MIN_BLOCKS
+#define GSR_SORT_MIN_BLOCKS 3
+#endif
+#ifndef GSR_LOOKBACK_WIDTH
+#define GSR_LOOKBACK_WIDTH 4
+#endif
+constexpr int kLookback = GSR_LOOKBACK_WIDTH;
 constexpr uint32_t kFlagA = 1u << 30;
 constexpr uint32_t kFlagP = 2u << 30;
 constexpr uint32_t kMask = (1u << 30) - 1;
@@ -110,7 +119,7 @@ __global__ void __launch_bounds__(kThreads) plan_kernel(const uint32_t *__restri
 }
 
 template <int kIpt>
-__global__ void __launch_bounds__(kThreads) pass_kernel(const SortPlan *__restrict__ plan,
+__global__ void __launch_bounds__(kThreads, GSR_SORT_MIN_BLOCKS) pass_kernel(const SortPlan *__restrict__ plan,
                                                         uint32_t pass, uint32_t shift,
                                                         uint32_t *k0, uint32_t *v0, uint32_t *k1,
                                                         uint32_t *v1, uint32_t *status,
@@ -183,23 +192,23 @@ __global__ void __launch_bounds__(kThreads) pass_kernel(const SortPlan *__restri
   uint32_t total;
   s_block_start[d] = block_exclusive_scan(block_count, s_wsum, total);
 
-  // Look back over the predecessor tiles, four status words per step: add
-  // aggregates until the nearest inclusive prefix; restart a step when one
-  // of the words it needs is not published yet.
+  // Look back over the predecessor tiles, kLookback status words per step:
+  // add aggregates until the nearest inclusive prefix; restart a step when
+  // one of the words it needs is not published yet.
   uint32_t exclusive = 0;
   if (tile > 0) {
     int32_t t = (int32_t)tile - 1;
     uint32_t spins = 0;
     while (t >= 0) {
-      uint32_t w[4];
+      uint32_t w[kLookback];
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
+      for (int q = 0; q < kLookback; ++q)
         w[q] = (t - q >= 0) ? ld_relaxed_u32(&status[(size_t)(t - q) * 256 + d]) : kFlagP;
       bool found = false, stalled = false;
       uint32_t add = 0;
       int used = 0;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < kLookback; ++q) {
         if (found || stalled) continue;
         uint32_t flag = w[q] & ~kMask;
         if (flag == 0) {
@@ -249,7 +258,12 @@ __global__ void __launch_bounds__(kThreads) pass_kernel(const SortPlan *__restri
 }
 
 // Keys per thread: 8 up to 2M keys, 16 above.
-inline uint32_t ipt_for(uint32_t capacity) { return capacity <= (1u << 21) ? 8u : 16u; }
+#ifndef GSR_SORT_IPT_LARGE
+#define GSR_SORT_IPT_LARGE 16
+#endif
+inline uint32_t ipt_for(uint32_t capacity) {
+  return capacity <= (1u << 21) ? 8u : (uint32_t)GSR_SORT_IPT_LARGE;
+}
 inline uint32_t tiles_for(uint32_t capacity) {
   uint32_t tile = kThreads * ipt_for(capacity);
   return (capacity + tile - 1) / tile;

@@ -10,6 +10,7 @@ namespace gsr {
 
 struct SceneDev;
 struct ViewDev;
+struct ViewSetDev;
 struct ViewCounters;
 struct Record;
 struct ProjectedDev;
@@ -29,9 +30,12 @@ struct K1Buffers {
   ViewCounters *view_counters; // [views], zeroed
   ProjectedDev *projected;     // [gid] debug tap, or null
 };
-uint32_t preprocess_blocks(uint32_t splats);  // blocks one view of `splats` splats needs
-void launch_preprocess(const ViewDev *views, uint32_t num_views, uint32_t total_blocks,
-                       uint32_t max_planes, const K1Buffers &b, bool debug, cudaStream_t stream);
+uint32_t preprocess_blocks(uint32_t splats);  // blocks one view set of `splats` splats needs
+// One block per 256 splats of each view set (views of one scene handled
+// together); total_blocks = sum over sets of preprocess_blocks(scene splats).
+void launch_preprocess(const ViewDev *views, const ViewSetDev *sets, uint32_t num_sets,
+                       uint32_t total_blocks, uint32_t max_planes, const K1Buffers &b, bool debug,
+                       cudaStream_t stream);
 
 // ---- K3: onesweep LSD radix sort of (u32 key, u32 value) pairs -----------
 // Sorts ascending and stably over bits [begin_bit, begin_bit + 8*passes) of

@@ -123,6 +123,7 @@ Pipeline::~Pipeline() {
   if (counters_host_) cudaFreeHost(counters_host_);
   if (view_counters_pinned_) cudaFreeHost(view_counters_pinned_);
   if (views_pinned_) cudaFreeHost(views_pinned_);
+  if (sets_pinned_) cudaFreeHost(sets_pinned_);
 }
 
 void Pipeline::record(int k) {
@@ -159,6 +160,7 @@ Pipeline::Layout Pipeline::plan_views(const ViewSpec *views, uint32_t count,
   Layout l;
   l.views = count;
   views_host_.resize(count);
+  sets_host_.clear();
   uint64_t splats = 0, blocks = 0, tiles = 0;
   for (uint32_t v = 0; v < count; ++v) {
     const ViewSpec &vs = views[v];
@@ -171,11 +173,17 @@ Pipeline::Layout Pipeline::plan_views(const ViewSpec *views, uint32_t count,
                             vs.scene->n);
     d.sc = vs.scene->dev;
     d.splat_base = (uint32_t)splats;
-    d.block_base = (uint32_t)blocks;
     d.tile_base = (uint32_t)tiles;
     d.image_base = image_bases[v];
+    // Consecutive views of one scene form a view set (one scene read in K1).
+    if (sets_host_.empty() || views[v - 1].scene != vs.scene ||
+        sets_host_.back().count == kMaxSetViews) {
+      sets_host_.push_back(ViewSetDev{v, 0, (uint32_t)blocks, 0});
+      blocks += preprocess_blocks(vs.scene->n);
+    }
+    sets_host_.back().count++;
+    d.set = (uint32_t)sets_host_.size() - 1;
     splats += vs.scene->n;
-    blocks += preprocess_blocks(vs.scene->n);
     tiles += d.p.num_tiles;
     l.max_planes = std::max(l.max_planes, vs.scene->dev.planes);
   }
@@ -183,6 +191,7 @@ Pipeline::Layout Pipeline::plan_views(const ViewSpec *views, uint32_t count,
     throw Error(Code::Unsupported, "splats over the views of one run exceed 2^30 - 1");
   if (tiles > (1u << 24)) throw Error(Code::Unsupported, "too many tiles in one run");
   l.total_splats = (uint32_t)splats;
+  l.sets = (uint32_t)sets_host_.size();
   l.total_blocks = (uint32_t)blocks;
   l.total_tiles = (uint32_t)tiles;
   l.tile_passes = tile_sort_passes(l.total_tiles);
@@ -197,7 +206,7 @@ void Pipeline::ensure_workspace(const Layout &l) {
     const uint32_t vcap = std::max(l.views, view_cap_);
     const uint32_t ncap = std::max(n, splat_cap_);
     // view workspace: [view counters | K1 status | emit status] zeroed, then the table.
-    const uint64_t k1_words = (ncap + 255) / 256 + 1;  // + views: blocks round up per view
+    const uint64_t k1_words = (ncap + 255) / 256 + 1;  // + views: blocks round up per set
     const uint64_t k1_total = k1_words + vcap;
     const uint64_t emit_words = (ncap + 1023) / 1024;
     uint64_t off = 0;
@@ -206,7 +215,9 @@ void Pipeline::ensure_workspace(const Layout &l) {
     const uint64_t o_em = off; off += align256(8 * emit_words);
     view_zero_bytes_ = off;
     const uint64_t o_tab = off; off += align256(sizeof(ViewDev) * vcap);
+    const uint64_t o_sets = off; off += align256(sizeof(ViewSetDev) * vcap);
     view_ws_.reset(off);
+    sets_dev_ = view_ws_.as<ViewSetDev>(o_sets);
     view_counters_ = view_ws_.as<ViewCounters>(o_vc);
     k1_status_ = view_ws_.as<unsigned long long>(o_k1);
     emit_status_ = view_ws_.as<unsigned long long>(o_em);
@@ -217,10 +228,13 @@ void Pipeline::ensure_workspace(const Layout &l) {
       GSR_CUDA(cudaStreamSynchronize(stream_));
       if (view_counters_pinned_) cudaFreeHost(view_counters_pinned_);
       if (views_pinned_) cudaFreeHost(views_pinned_);
+      if (sets_pinned_) cudaFreeHost(sets_pinned_);
       view_counters_pinned_ = nullptr;
       views_pinned_ = nullptr;
+      sets_pinned_ = nullptr;
       GSR_CUDA(cudaMallocHost(&view_counters_pinned_, sizeof(ViewCounters) * vcap));
       GSR_CUDA(cudaMallocHost(&views_pinned_, sizeof(ViewDev) * vcap * kViewSlots));
+      GSR_CUDA(cudaMallocHost(&sets_pinned_, sizeof(ViewSetDev) * vcap * kViewSlots));
       view_counters_pinned_cap_ = vcap;
     }
     if (n > splat_cap_) {
@@ -308,7 +322,8 @@ void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &si
 
   K1Buffers k1{vis_keys0_, vis_vals0_, rects_, records_, k1_status_, counters_, key_hist_,
                view_counters_, debug_ ? projected_.as<ProjectedDev>() : nullptr};
-  launch_preprocess(views_dev_, l.views, l.total_blocks, l.max_planes, k1, debug_, stream_);
+  launch_preprocess(views_dev_, sets_dev_, l.sets, l.total_blocks, l.max_planes, k1, debug_,
+                    stream_);
   record(1);
 
   SortBuffers ds{vis_keys0_, vis_vals0_, vis_keys1_, vis_vals1_, &counters_->visible, n, 0, 4,
@@ -359,6 +374,10 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
   std::memcpy(staged, views_host_.data(), sizeof(ViewDev) * l.views);
   GSR_CUDA(cudaMemcpyAsync(views_dev_, staged, sizeof(ViewDev) * l.views, cudaMemcpyHostToDevice,
                            stream_));
+  ViewSetDev *staged_sets = sets_pinned_ + (uint64_t)slot_ * view_cap_;
+  std::memcpy(staged_sets, sets_host_.data(), sizeof(ViewSetDev) * l.sets);
+  GSR_CUDA(cudaMemcpyAsync(sets_dev_, staged_sets, sizeof(ViewSetDev) * l.sets,
+                           cudaMemcpyHostToDevice, stream_));
   GSR_CUDA(cudaEventRecord(slot_ev_[slot_], stream_));
   slot_ = (slot_ + 1) % kViewSlots;
 

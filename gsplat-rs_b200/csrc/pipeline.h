@@ -125,9 +125,9 @@ class Pipeline {
  private:
   struct Layout {
     uint32_t views = 0, total_splats = 0, total_blocks = 0, total_tiles = 0, max_planes = 1;
-    uint32_t tile_passes = 1;
+    uint32_t tile_passes = 1, sets = 0;
     bool operator==(const Layout &o) const {
-      return views == o.views && total_splats == o.total_splats &&
+      return views == o.views && sets == o.sets && total_splats == o.total_splats &&
              total_blocks == o.total_blocks && total_tiles == o.total_tiles &&
              max_planes == o.max_planes && tile_passes == o.tile_passes;
     }
@@ -151,6 +151,7 @@ class Pipeline {
   HostSinks last_sinks_;
   RunResult last_;
   std::vector<ViewDev> views_host_;
+  std::vector<ViewSetDev> sets_host_;
   std::vector<ViewCounters> view_counters_host_;
 
   // Fixed-size scratch: counters, plans, histograms, sticky word; zeroed
@@ -164,6 +165,7 @@ class Pipeline {
   DeviceBuffer view_ws_;  // view table + view counters + look-back words (zeroed part)
   uint64_t view_zero_bytes_ = 0;
   ViewDev *views_dev_ = nullptr;
+  ViewSetDev *sets_dev_ = nullptr;
   ViewCounters *view_counters_ = nullptr;
   unsigned long long *k1_status_ = nullptr, *emit_status_ = nullptr;
   uint32_t view_cap_ = 0, splat_cap_ = 0, tile_cap_ = 0;
@@ -186,6 +188,7 @@ class Pipeline {
   // the copy that last read it has completed (slot_ev_[s]).
   static constexpr int kViewSlots = 4;
   ViewDev *views_pinned_ = nullptr;
+  ViewSetDev *sets_pinned_ = nullptr;
   cudaEvent_t slot_ev_[kViewSlots] = {};
   int slot_ = 0;
   // CUDA graphs of launch_all, one per layout, buffer set and setting.

@@ -237,6 +237,30 @@ bool Server::launch(LaneState &ls, std::unique_lock<std::mutex> &lk) {
     r.info.status = RequestStatus::Running;
     r.t_launch = now_ms();
   }
+  // Requests of one scene run next to each other (one scene read per view
+  // set in the preprocess kernel); image offsets follow the new order.
+  {
+    const size_t m = ls.ids.size();
+    std::vector<size_t> order(m);
+    for (size_t k = 0; k < m; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+      return requests_.at(ls.ids[a]).view.scene < requests_.at(ls.ids[b]).view.scene;
+    });
+    std::vector<uint64_t> ids(m), pred(m), bases(m);
+    std::vector<ViewSpec> specs(m);
+    uint64_t px = 0;
+    for (size_t k = 0; k < m; ++k) {
+      ids[k] = ls.ids[order[k]];
+      specs[k] = ls.specs[order[k]];
+      pred[k] = predicted[order[k]];
+      bases[k] = px;
+      px += (uint64_t)specs[k].width * specs[k].height;
+    }
+    ls.ids.swap(ids);
+    ls.specs.swap(specs);
+    ls.bases.swap(bases);
+    predicted.swap(pred);
+  }
   ls.admitted_bytes = bytes;
   peak_admitted_ = std::max<uint64_t>(peak_admitted_, bytes);
   for (auto &o : lanes_)

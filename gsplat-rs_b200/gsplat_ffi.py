@@ -16,7 +16,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libgsplat_ffi_c.so")
+# GSPLAT_FFI_LIB selects another build of the library (tuning variants).
+LIB_PATH = os.environ.get("GSPLAT_FFI_LIB") or os.path.join(HERE, "lib", "libgsplat_ffi_c.so")
 
 OK = 0
 INVALID_ARGUMENT = 1

@@ -96,7 +96,9 @@ def test_batch_grouping_and_pair_reruns():
         assert t.groups == 4
         assert t.reruns >= 1
         groups = [b.view_stats(k).group for k in range(len(views))]
-        assert groups == sorted(groups) and groups[0] == 0 and groups[-1] == 3
+        # views are grouped by scene, then split in render order
+        assert sorted(set(groups)) == [0, 1, 2, 3]
+        assert all(groups.count(g) <= 3 for g in range(4))
         _check_against_plain(b, scenes, views, tile=8)
         t = b.render(views)  # predictions learned: no re-run the second time
         assert t.reruns == 0
