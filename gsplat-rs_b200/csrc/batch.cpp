@@ -87,7 +87,7 @@ std::vector<ViewGroup> plan_groups(const std::vector<ViewSpec> &views,
     const uint64_t n = views[v].scene->n;
     const uint64_t t = (uint64_t)((views[v].width + tile - 1) / tile) * ((views[v].height + tile - 1) / tile);
     const bool fits = cur.count < max_views && splats + n <= std::min<uint64_t>(limits.max_splats, kMaxPairs) &&
-                      tiles + t <= (1u << 24) &&
+                      tiles + t <= std::min<uint64_t>(limits.max_tiles, 1u << 24) &&
                       cur.predicted_pairs + predicted[v] <= std::min<uint64_t>(limits.max_pairs, kMaxPairs);
     if (cur.count && !fits) {
       groups.push_back(cur);
@@ -249,7 +249,8 @@ void Batch::set_blend_mode(uint32_t mode) {
 }
 
 void Batch::set_limits(const GroupLimits &l) {
-  if (l.max_views == 0 || l.max_views > kMaxViewsPerLaunch || l.max_pairs == 0 || l.max_splats == 0)
+  if (l.max_views == 0 || l.max_views > kMaxViewsPerLaunch || l.max_pairs == 0 || l.max_splats == 0 ||
+      l.max_tiles == 0)
     throw Error(Code::InvalidArgument, "invalid batch limits");
   limits_ = l;
 }

@@ -64,6 +64,9 @@ struct GroupLimits {
   uint32_t max_views = 1024;
   uint64_t max_pairs = 1ull << 28;   // predicted tile pairs (sizes the key buffers)
   uint64_t max_splats = 1ull << 28;  // splats over the views (sizes the splat workspace)
+  // Tiles over the views: at most 2^16 keeps the tile sort at two passes,
+  // above that it takes three (limit 2^24).
+  uint64_t max_tiles = 1ull << 24;
 };
 
 struct ViewGroup {

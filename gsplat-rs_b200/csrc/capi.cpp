@@ -665,13 +665,14 @@ int32_t gsplat_batch_set_blend_mode(GsplatBatch *batch, uint32_t mode) {
 }
 
 int32_t gsplat_batch_set_limits(GsplatBatch *batch, uint32_t max_views, uint64_t max_pairs,
-                                uint64_t max_splats) {
+                                uint64_t max_splats, uint64_t max_tiles) {
   return guarded("gsplat_batch_set_limits", [&]() -> int32_t {
     GSR_BATCH_CHECK("gsplat_batch_set_limits");
     gsr::GroupLimits l = batch->batch->limits();
     if (max_views) l.max_views = max_views;
     if (max_pairs) l.max_pairs = max_pairs;
     if (max_splats) l.max_splats = max_splats;
+    if (max_tiles) l.max_tiles = max_tiles;
     batch->batch->set_limits(l);
     return ok();
   });

@@ -50,6 +50,7 @@ static_assert(sizeof(ProjectedDev) == 64, "projected splat layout");
 enum : uint32_t {
   kErrLookbackTimeout = 1u,  // a decoupled look-back wait hit its iteration limit
   kErrSortTooLarge = 2u,
+  kErrStageTimeout = 4u,     // a bulk-copy (TMA) completion wait hit its iteration limit
 };
 
 // Per-frame device counters; zeroed before each frame.

@@ -43,8 +43,12 @@ __device__ __forceinline__ float cov_bilinear(const Cov6 &c, const float *a, con
   return a[0] * bx + a[1] * by + a[2] * bz;
 }
 
+constexpr int kK1Threads = 256;
+
+// Float k of a splat's colour data; plane q of the splat is planes[q * kK1Threads]
+// (the block's shared-memory stage, one float4 per splat and plane).
 __device__ __forceinline__ float plane_float(const float4 *planes, int k) {
-  const float4 v = planes[k >> 2];
+  const float4 v = planes[(k >> 2) * kK1Threads];
   switch (k & 3) {
     case 0: return v.x;
     case 1: return v.y;
@@ -127,10 +131,12 @@ __device__ __forceinline__ void eval_sh(const float4 *f, uint32_t degree, float 
 // The per-splat vertex stage for a depth-visible splat. Returns false when
 // project_splat marks the splat invalid (behind near, beyond far, or outside
 // the frustum by its axis extents).
+// `ca`, `cb` are the splat's covariance planes and `col` its first colour
+// plane in the block's stage (planes kK1Threads float4 apart).
 template <int kPlanes>
-__device__ __forceinline__ bool project(const SceneDev &sc, const FrameParams &p, uint32_t i,
-                                        const float4 &pa, const float rel[3], float depth,
-                                        Record &rec, uint2 &rect, ProjectedDev *dbg) {
+__device__ __forceinline__ bool project(const FrameParams &p, const float4 &pa, const float4 &ca,
+                                        const float4 &cb, const float4 *col, const float rel[3],
+                                        float depth, Record &rec, uint2 &rect, ProjectedDev *dbg) {
   float px = p.r0[0] * rel[0] + p.r0[1] * rel[1] + p.r0[2] * rel[2];
   float py = p.r1[0] * rel[0] + p.r1[1] * rel[1] + p.r1[2] * rel[2];
   float z = depth;
@@ -139,8 +145,6 @@ __device__ __forceinline__ bool project(const SceneDev &sc, const FrameParams &p
   float x_ndc = (px * p.f) * inv_z / p.aspect;
   float y_ndc = (py * p.f) * inv_z;
 
-  const float4 ca = sc.cov_a[i];
-  const float4 cb = sc.cov_b[i];
   Cov6 wc{ca.x, ca.y, ca.z, ca.w, cb.x, cb.y};
   Cov6 cc{cov_quadratic(wc, p.r0[0], p.r0[1], p.r0[2]), cov_bilinear(wc, p.r0, p.r1),
           cov_bilinear(wc, p.r0, p.r2),                 cov_quadratic(wc, p.r1[0], p.r1[1], p.r1[2]),
@@ -198,12 +202,8 @@ __device__ __forceinline__ bool project(const SceneDev &sc, const FrameParams &p
     dy = rel[1] * inv;
     dz = rel[2] * inv;
   }
-  float4 fbuf[kPlanes];
-#pragma unroll
-  for (int k = 0; k < kPlanes; ++k)
-    fbuf[k] = k < (int)sc.planes ? sc.color[(size_t)k * sc.n + i] : make_float4(0.f, 0.f, 0.f, 0.f);
   float rgb[3];
-  eval_sh<kPlanes>(fbuf, p.sh_degree, dx, dy, dz, rgb);
+  eval_sh<kPlanes>(col, p.sh_degree, dx, dy, dz, rgb);
 #pragma unroll
   for (int ch = 0; ch < 3; ++ch) rgb[ch] = clampf(rgb[ch] + 0.5f, 0.0f, 1.0f);
   float pr = rgb[0] * al, pg = rgb[1] * al, pb = rgb[2] * al;
@@ -253,48 +253,93 @@ __device__ __forceinline__ bool project(const SceneDev &sc, const FrameParams &p
   return true;
 }
 
-constexpr int kK1Threads = 256;
 constexpr int kK1Warps = kK1Threads / 32;
 // Resident blocks per SM the register allocation must allow (tuning knob).
 #ifndef GSR_K1_MIN_BLOCKS
 #define GSR_K1_MIN_BLOCKS 3
 #endif
 
+// The block's slice of the scene planes in shared memory: 256 splats of
+// position/alpha, both covariance planes and kPlanes colour planes.
+template <int kPlanes>
+struct K1Stage {
+  float4 pos[kK1Threads];
+  float4 cov_a[kK1Threads];
+  float4 cov_b[kK1Threads];
+  float4 color[kPlanes][kK1Threads];
+  uint64_t bar[2];  // [0]: positions, [1]: covariance and colour
+};
+
 // One block covers 256 consecutive splats of one scene for every view of a
-// view set (up to kMaxSetViews views of that scene), so the scene planes are
-// read from HBM once per set instead of once per view (the later views of
-// the set find them in L1/L2). Per view, the arithmetic is exactly the
+// view set (up to kMaxSetViews views of that scene). One thread stages the
+// block's slice of every scene plane into shared memory with bulk copies
+// (cp.async.bulk, completion on an mbarrier), so all of the block's HBM
+// reads are in flight at once and every view of the set reads the slice
+// from shared memory: the scene is read from HBM once per set. Positions
+// arrive on their own barrier, so the depth tests start while covariance and
+// colour are still in flight. Per view, the arithmetic is exactly the
 // single-view sequence. Visible entries are compacted in (block, view, id)
 // order, which keeps every view's entries in ascending id order.
 template <int kPlanes, bool kDebug>
 __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
     preprocess_kernel(const ViewDev *__restrict__ views, const ViewSetDev *__restrict__ sets,
                       uint32_t num_sets, uint32_t total_blocks, K1Buffers b) {
+  extern __shared__ __align__(128) unsigned char k1_dyn[];
+  K1Stage<kPlanes> &st = *reinterpret_cast<K1Stage<kPlanes> *>(k1_dyn);
   __shared__ uint32_t s_block;
   __shared__ uint32_t s_set;
   __shared__ uint32_t s_cnt[kMaxSetViews][kK1Warps];  // visible per view and warp
   __shared__ uint32_t s_hist[4][256];
+  __shared__ FrameParams s_params[kMaxSetViews];  // the set's per-view uniforms
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) {
     const uint32_t blk = atomicAdd(&b.counters->k1_ticket, 1u);
     s_block = blk;
-    s_set = find_view(num_sets, blk, [&](uint32_t v) { return sets[v].block_base; });
+    const uint32_t si = find_view(num_sets, blk, [&](uint32_t v) { return sets[v].block_base; });
+    s_set = si;
+    const ViewSetDev set0 = sets[si];
+    const SceneDev sc0 = views[set0.first_view].sc;
+    const uint32_t i0 = (blk - set0.block_base) * kK1Threads;
+    const uint32_t bytes = min((uint32_t)kK1Threads, sc0.n - i0) * 16u;  // >= 16: i0 < n
+    mbar_init(&st.bar[0], 1);
+    mbar_init(&st.bar[1], 1);
+    fence_barrier_init();
+    mbar_arrive_expect_tx(&st.bar[0], bytes);
+    bulk_copy_g2s(st.pos, sc0.pos_alpha + i0, bytes, &st.bar[0]);
+    mbar_arrive_expect_tx(&st.bar[1], bytes * (2u + sc0.planes));
+    bulk_copy_g2s(st.cov_a, sc0.cov_a + i0, bytes, &st.bar[1]);
+    bulk_copy_g2s(st.cov_b, sc0.cov_b + i0, bytes, &st.bar[1]);
+    for (uint32_t q = 0; q < sc0.planes && q < (uint32_t)kPlanes; ++q)
+      bulk_copy_g2s(st.color[q], sc0.color + (size_t)q * sc0.n + i0, bytes, &st.bar[1]);
   }
   for (uint32_t k = threadIdx.x; k < 4 * 256; k += kK1Threads) (&s_hist[0][0])[k] = 0;
   __syncthreads();
   const uint32_t block = s_block;
   const ViewSetDev set = sets[s_set];
+  {
+    constexpr uint32_t kWords = sizeof(FrameParams) / 4;
+    static_assert(sizeof(FrameParams) % 4 == 0, "FrameParams is copied as words");
+    for (uint32_t w = threadIdx.x; w < set.count * kWords; w += kK1Threads) {
+      const uint32_t v = w / kWords, o = w % kWords;
+      reinterpret_cast<uint32_t *>(&s_params[v])[o] =
+          reinterpret_cast<const uint32_t *>(&views[set.first_view + v].p)[o];
+    }
+  }
+  __syncthreads();
   const SceneDev sc = views[set.first_view].sc;
   const uint32_t i = (block - set.block_base) * kK1Threads + threadIdx.x;
   const bool valid = i < sc.n;
-  const float4 pa = valid ? sc.pos_alpha[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  // A wait that expires leaves the error bit set (the frame reports an
+  // internal error) after a second bounded wait for the copies in flight.
+  if (!mbar_wait(&st.bar[0], 0, &b.counters->error)) mbar_wait(&st.bar[0], 0, &b.counters->error);
+  const float4 pa = valid ? st.pos[threadIdx.x] : make_float4(0.f, 0.f, 0.f, 0.f);
 
   // Depth test for every view of the set. The block's visible count is
   // known right after it: publish it for the successors' look-back before
   // doing the heavy vertex stage.
   uint32_t vis_bits = 0;
   for (uint32_t k = 0; k < set.count; ++k) {
-    const FrameParams &p = views[set.first_view + k].p;
+    const FrameParams &p = s_params[k];
     const float rx = pa.x - p.cam[0], ry = pa.y - p.cam[1], rz = pa.z - p.cam[2];
     const float depth = p.r2[0] * rx + p.r2[1] * ry + p.r2[2] * rz;
     const bool vis = valid && depth >= p.near_plane && depth <= p.far_plane;
@@ -315,9 +360,13 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
     if (c) atomicAdd(&b.view_counters[set.first_view + threadIdx.x].visible, c);
   }
 
+  if (!mbar_wait(&st.bar[1], 0, &b.counters->error)) mbar_wait(&st.bar[1], 0, &b.counters->error);
+  const float4 ca = st.cov_a[threadIdx.x];
+  const float4 cb = st.cov_b[threadIdx.x];
+  const float4 *col = &st.color[0][threadIdx.x];
   for (uint32_t k = 0; k < set.count; ++k) {
     const uint32_t view = set.first_view + k;
-    const FrameParams &p = views[view].p;
+    const FrameParams &p = s_params[k];
     const uint32_t gid = views[view].splat_base + i;
     const bool vis = (vis_bits >> k) & 1u;
     float rel[3] = {pa.x - p.cam[0], pa.y - p.cam[1], pa.z - p.cam[2]};
@@ -335,7 +384,7 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
     if (vis) {
       Record rec;
       uint2 rect = make_uint2(0u, 0u);
-      drawn = project<kPlanes>(sc, p, i, pa, rel, depth, rec, rect, dbg);
+      drawn = project<kPlanes>(p, pa, ca, cb, col, rel, depth, rec, rect, dbg);
       b.rects[gid] = rect;
       if (drawn) b.records[gid] = rec;
       area = ((rect.y & 0xffffu) - (rect.x & 0xffffu)) * ((rect.y >> 16) - (rect.x >> 16));
@@ -375,7 +424,7 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
     const uint32_t bal = __ballot_sync(0xffffffffu, vis);
     if (vis) {
       const uint32_t view = set.first_view + k;
-      const FrameParams &p = views[view].p;
+      const FrameParams &p = s_params[k];
       const float rx = pa.x - p.cam[0], ry = pa.y - p.cam[1], rz = pa.z - p.cam[2];
       const float depth = p.r2[0] * rx + p.r2[1] * ry + p.r2[2] * rz;
       const uint32_t at = slot + warp_prefix + __popc(bal & lanemask_lt());
@@ -385,10 +434,28 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
     slot += view_total;
   }
   __syncthreads();
+  if (threadIdx.x == 0) {  // every thread has passed both waits
+    mbar_inval(&st.bar[0]);
+    mbar_inval(&st.bar[1]);
+  }
   for (uint32_t k = threadIdx.x; k < 4 * 256; k += kK1Threads) {
     uint32_t c = (&s_hist[0][0])[k];
     if (c) atomicAdd(&b.key_hist[k], c);
   }
+}
+
+template <int kPlanes, bool kDebug>
+void launch_k1_t(const ViewDev *views, const ViewSetDev *sets, uint32_t num_sets,
+                 uint32_t total_blocks, const K1Buffers &b, cudaStream_t stream) {
+  constexpr size_t kSmem = sizeof(K1Stage<kPlanes>);
+  static const bool configured = [] {
+    cudaFuncSetAttribute(preprocess_kernel<kPlanes, kDebug>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+    return true;
+  }();
+  (void)configured;
+  preprocess_kernel<kPlanes, kDebug>
+      <<<total_blocks, kK1Threads, kSmem, stream>>>(views, sets, num_sets, total_blocks, b);
 }
 
 template <int kPlanes>
@@ -396,11 +463,9 @@ void launch_k1(const ViewDev *views, const ViewSetDev *sets, uint32_t num_sets,
                uint32_t total_blocks, const K1Buffers &b, bool debug, cudaStream_t stream) {
   if (total_blocks == 0) return;
   if (debug)
-    preprocess_kernel<kPlanes, true>
-        <<<total_blocks, kK1Threads, 0, stream>>>(views, sets, num_sets, total_blocks, b);
+    launch_k1_t<kPlanes, true>(views, sets, num_sets, total_blocks, b, stream);
   else
-    preprocess_kernel<kPlanes, false>
-        <<<total_blocks, kK1Threads, 0, stream>>>(views, sets, num_sets, total_blocks, b);
+    launch_k1_t<kPlanes, false>(views, sets, num_sets, total_blocks, b, stream);
 }
 
 }  // namespace

@@ -19,6 +19,8 @@
 // (crates/gsplat-sort/src/radix.rs:11-58: stable LSD passes, equal keys keep
 // their input order).
 
+#include <algorithm>
+
 #include "device_common.cuh"
 #include "kernels.h"
 
@@ -87,12 +89,24 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s
   return before + inc - v;
 }
 
+// Block 0 plans the passes; every block zeroes the look-back status words
+// of the tiles the actual item count needs (not the capacity's).
 __global__ void __launch_bounds__(kThreads) plan_kernel(const uint32_t *__restrict__ count,
                                                         const uint32_t *__restrict__ hist,
-                                                        uint32_t passes, SortPlan *plan) {
+                                                        uint32_t passes, SortPlan *plan,
+                                                        uint32_t *status, uint32_t tile_stride,
+                                                        uint32_t tile_items) {
+  const uint32_t n = *count;
+  const uint64_t used = (uint64_t)((n + tile_items - 1) / tile_items) * 256u;  // words per pass
+  for (uint32_t p = 0; p < passes; ++p) {
+    uint4 *dst = reinterpret_cast<uint4 *>(status + (size_t)p * tile_stride * 256u);
+    for (uint64_t k = blockIdx.x * (uint64_t)kThreads + threadIdx.x; k < used / 4;
+         k += (uint64_t)gridDim.x * kThreads)
+      dst[k] = make_uint4(0u, 0u, 0u, 0u);
+  }
+  if (blockIdx.x != 0) return;
   __shared__ uint32_t s_wsum[kWarps];
   __shared__ uint32_t s_trivial[4];
-  const uint32_t n = *count;
   const uint32_t d = threadIdx.x;
   if (d < 4) s_trivial[d] = 0;
   __syncthreads();
@@ -119,34 +133,33 @@ __global__ void __launch_bounds__(kThreads) plan_kernel(const uint32_t *__restri
 }
 
 template <int kIpt>
-__global__ void __launch_bounds__(kThreads, GSR_SORT_MIN_BLOCKS) pass_kernel(const SortPlan *__restrict__ plan,
-                                                        uint32_t pass, uint32_t shift,
-                                                        uint32_t *k0, uint32_t *v0, uint32_t *k1,
-                                                        uint32_t *v1, uint32_t *status,
-                                                        uint32_t *ticket, uint32_t *error) {
-  constexpr uint32_t kTile = kThreads * kIpt;
-  __shared__ uint32_t s_warp_hist[kWarps][256];
-  __shared__ uint32_t s_keys[kTile];
-  __shared__ uint32_t s_vals[kTile];
-  __shared__ uint32_t s_block_start[256];
-  __shared__ uint32_t s_global[256];
-  __shared__ uint32_t s_wsum[kWarps];
-  __shared__ uint32_t s_tile;
+struct PassSmem {
+  static constexpr uint32_t kTile = kThreads * kIpt;
+  uint32_t warp_hist[kWarps][256];
+  uint32_t keys[kTile];
+  uint32_t vals[kTile];
+  uint32_t block_start[256];
+  uint32_t global[256];
+  uint32_t wsum[kWarps];
+  uint32_t tile;
+};
 
-  if (plan->skip[pass]) return;
-  const uint32_t n = plan->n;
-  const bool from0 = plan->src[pass] == 0;
-  const uint32_t *__restrict__ in_k = from0 ? k0 : k1;
-  const uint32_t *__restrict__ in_v = from0 ? v0 : v1;
-  uint32_t *__restrict__ out_k = from0 ? k1 : k0;
-  uint32_t *__restrict__ out_v = from0 ? v1 : v0;
-
-  if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
-  for (uint32_t k = threadIdx.x; k < kWarps * 256; k += kThreads) (&s_warp_hist[0][0])[k] = 0;
-  __syncthreads();
-  const uint32_t tile = s_tile;
+// One tile of one pass: rank, publish, look back, reorder, scatter.
+template <int kIpt>
+__device__ __forceinline__ void pass_tile(const SortPlan *__restrict__ plan, uint32_t pass,
+                                          uint32_t shift, uint32_t n, uint32_t tile,
+                                          const uint32_t *__restrict__ in_k,
+                                          const uint32_t *__restrict__ in_v,
+                                          uint32_t *__restrict__ out_k,
+                                          uint32_t *__restrict__ out_v, uint32_t *status,
+                                          uint32_t *error, PassSmem<kIpt> &sm) {
+  constexpr uint32_t kTile = PassSmem<kIpt>::kTile;
+  auto &s_warp_hist = sm.warp_hist;
+  auto &s_keys = sm.keys;
+  auto &s_vals = sm.vals;
+  auto &s_block_start = sm.block_start;
+  auto &s_global = sm.global;
   const uint32_t base = tile * kTile;
-  if (base >= n) return;
 
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t warp_base = base + warp * 32 * kIpt;
@@ -190,7 +203,7 @@ __global__ void __launch_bounds__(kThreads, GSR_SORT_MIN_BLOCKS) pass_kernel(con
   uint32_t *my_status = &status[(size_t)tile * 256];
   st_relaxed_u32(&my_status[d], (tile == 0 ? kFlagP : kFlagA) | block_count);
   uint32_t total;
-  s_block_start[d] = block_exclusive_scan(block_count, s_wsum, total);
+  s_block_start[d] = block_exclusive_scan(block_count, sm.wsum, total);
 
   // Look back over the predecessor tiles, kLookback status words per step:
   // add aggregates until the nearest inclusive prefix; restart a step when
@@ -257,6 +270,33 @@ __global__ void __launch_bounds__(kThreads, GSR_SORT_MIN_BLOCKS) pass_kernel(con
   }
 }
 
+// Persistent pass: a fixed grid of blocks takes tiles from an atomic ticket
+// (so look-back only ever waits on tiles already taken by running blocks)
+// until the item count, read on the device, is covered.
+template <int kIpt>
+__global__ void __launch_bounds__(kThreads, GSR_SORT_MIN_BLOCKS)
+    pass_kernel(const SortPlan *__restrict__ plan, uint32_t pass, uint32_t shift, uint32_t *k0,
+                uint32_t *v0, uint32_t *k1, uint32_t *v1, uint32_t *status, uint32_t *ticket,
+                uint32_t *error) {
+  __shared__ PassSmem<kIpt> sm;
+  if (plan->skip[pass]) return;
+  const uint32_t n = plan->n;
+  const bool from0 = plan->src[pass] == 0;
+  const uint32_t *in_k = from0 ? k0 : k1;
+  const uint32_t *in_v = from0 ? v0 : v1;
+  uint32_t *out_k = from0 ? k1 : k0;
+  uint32_t *out_v = from0 ? v1 : v0;
+  for (;;) {
+    if (threadIdx.x == 0) sm.tile = atomicAdd(ticket, 1u);
+    for (uint32_t k = threadIdx.x; k < kWarps * 256; k += kThreads) (&sm.warp_hist[0][0])[k] = 0;
+    __syncthreads();
+    const uint32_t tile = sm.tile;
+    if ((uint64_t)tile * PassSmem<kIpt>::kTile >= n) break;
+    pass_tile<kIpt>(plan, pass, shift, n, tile, in_k, in_v, out_k, out_v, status, error, sm);
+    __syncthreads();  // shared memory is reused by the next tile
+  }
+}
+
 // Keys per thread: 8 up to 2M keys, 16 above.
 #ifndef GSR_SORT_IPT_LARGE
 #define GSR_SORT_IPT_LARGE 16
@@ -280,33 +320,51 @@ uint64_t sort_work_words(uint32_t capacity, uint32_t passes) {
   return 64ull + 4ull * 256ull + (uint64_t)passes * max_tiles * 256ull;
 }
 
+namespace {
+// Resident pass blocks on the device (the persistent grid).
+template <int kIpt>
+uint32_t resident_pass_blocks() {
+  static const uint32_t blocks = [] {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel<kIpt>, kThreads, 0);
+    return (uint32_t)std::max(1, sms * std::max(per_sm, 1));
+  }();
+  return blocks;
+}
+}  // namespace
+
 void launch_sort(const SortBuffers &b, cudaStream_t stream) {
   const uint32_t tiles = tiles_for(b.capacity);
-  // the words this launch uses (at most sort_work_words(b.capacity, b.passes))
-  const uint64_t words = 64ull + 4ull * 256ull + (uint64_t)b.passes * tiles * 256ull;
-  cudaMemsetAsync(b.work, 0, words * sizeof(uint32_t), stream);
+  const uint32_t ipt = ipt_for(b.capacity);
   uint32_t *tickets = b.work;
   uint32_t *hist = b.work + 64;
   uint32_t *status = b.work + 64 + 4 * 256;
+  // tickets and histograms; the status words are zeroed by the plan kernel
+  cudaMemsetAsync(b.work, 0, (64 + 4 * 256) * sizeof(uint32_t), stream);
   const uint32_t grid = tiles ? tiles : 1;
-  const uint32_t ipt = ipt_for(b.capacity);
   if (!b.hist) {
     if (ipt == 8)
       hist_kernel<8><<<grid, kThreads, 0, stream>>>(b.keys0, b.count, b.begin_bit, b.passes, hist);
     else
       hist_kernel<16><<<grid, kThreads, 0, stream>>>(b.keys0, b.count, b.begin_bit, b.passes, hist);
   }
-  plan_kernel<<<1, kThreads, 0, stream>>>(b.count, b.hist ? b.hist : hist, b.passes, b.plan);
+  const uint32_t zero_blocks = std::min<uint32_t>(grid, 296);
+  plan_kernel<<<zero_blocks, kThreads, 0, stream>>>(b.count, b.hist ? b.hist : hist, b.passes,
+                                                    b.plan, status, tiles, kThreads * ipt);
   for (uint32_t p = 0; p < b.passes; ++p) {
     uint32_t *st = status + (size_t)p * tiles * 256;
-    if (ipt == 8)
-      pass_kernel<8><<<grid, kThreads, 0, stream>>>(b.plan, p, b.begin_bit + 8 * p, b.keys0,
-                                                    b.vals0, b.keys1, b.vals1, st, tickets + p,
-                                                    b.error);
-    else
-      pass_kernel<16><<<grid, kThreads, 0, stream>>>(b.plan, p, b.begin_bit + 8 * p, b.keys0,
-                                                     b.vals0, b.keys1, b.vals1, st, tickets + p,
-                                                     b.error);
+    if (ipt == 8) {
+      const uint32_t g = std::min(grid, resident_pass_blocks<8>());
+      pass_kernel<8><<<g, kThreads, 0, stream>>>(b.plan, p, b.begin_bit + 8 * p, b.keys0, b.vals0,
+                                                 b.keys1, b.vals1, st, tickets + p, b.error);
+    } else {
+      const uint32_t g = std::min(grid, resident_pass_blocks<16>());
+      pass_kernel<16><<<g, kThreads, 0, stream>>>(b.plan, p, b.begin_bit + 8 * p, b.keys0,
+                                                  b.vals0, b.keys1, b.vals1, st, tickets + p,
+                                                  b.error);
+    }
   }
 }
 

@@ -233,7 +233,7 @@ _SIGS = [
     ("gsplat_batch_set_tile_size", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
     ("gsplat_batch_set_blend_mode", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
     ("gsplat_batch_set_limits", ctypes.c_int32,
-     [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64]),
+     [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
     ("gsplat_batch_set_raster_config", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]),
     ("gsplat_batch_autotune", ctypes.c_int32,
@@ -520,8 +520,8 @@ class Batch:
     def set_blend_mode(self, mode):
         check(lib().gsplat_batch_set_blend_mode(self.ptr, mode))
 
-    def set_limits(self, max_views=0, max_pairs=0, max_splats=0):
-        check(lib().gsplat_batch_set_limits(self.ptr, max_views, max_pairs, max_splats))
+    def set_limits(self, max_views=0, max_pairs=0, max_splats=0, max_tiles=0):
+        check(lib().gsplat_batch_set_limits(self.ptr, max_views, max_pairs, max_splats, max_tiles))
 
     def set_raster_config(self, chunk, blocks_per_sm=0):
         check(lib().gsplat_batch_set_raster_config(self.ptr, chunk, blocks_per_sm))

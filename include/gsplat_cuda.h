@@ -225,10 +225,11 @@ int32_t gsplat_batch_add_scene_buffers(GsplatBatch *batch, const GsplatSceneDesc
 int32_t gsplat_batch_add_scene_path(GsplatBatch *batch, const char *path, uint32_t *out_scene);
 int32_t gsplat_batch_set_tile_size(GsplatBatch *batch, uint32_t tile);       /* 8 or 16 */
 int32_t gsplat_batch_set_blend_mode(GsplatBatch *batch, uint32_t mode);      /* GsplatBlendMode */
-/* Launch-group limits: views (1..1024), predicted tile pairs and splats per
- * group (0 keeps the current value). */
+/* Launch-group limits: views (1..1024), predicted tile pairs, splats and
+ * image tiles per group (0 keeps the current value). Up to 65,536 tiles a
+ * group's tile sort takes two passes, above that three. */
 int32_t gsplat_batch_set_limits(GsplatBatch *batch, uint32_t max_views, uint64_t max_pairs,
-                                uint64_t max_splats);
+                                uint64_t max_splats, uint64_t max_tiles);
 /* As gsplat_context_set_raster_config. */
 int32_t gsplat_batch_set_raster_config(GsplatBatch *batch, uint32_t chunk, uint32_t blocks_per_sm);
 
