@@ -174,15 +174,38 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b) {
   }
 }
 
+// Tile boundaries of the sorted keys: four keys per thread (one 16-byte
+// load) plus the neighbour on each side.
 __global__ void ranges_kernel(const SortPlan *__restrict__ plan, const uint32_t *k0,
                               const uint32_t *k1, const FrameCounters *__restrict__ counters,
                               uint2 *__restrict__ ranges) {
   const uint32_t K = counters->pairs;
   const uint32_t *keys = plan->final_buffer == 0 ? k0 : k1;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < K; i += gridDim.x * blockDim.x) {
-    uint32_t t = keys[i];
-    if (i == 0 || keys[i - 1] != t) ranges[t].x = i;
-    if (i + 1 == K || keys[i + 1] != t) ranges[t].y = i + 1;
+  const uint32_t groups = (K + 3) / 4;
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < groups;
+       q += gridDim.x * blockDim.x) {
+    const uint32_t i0 = 4 * q;
+    uint32_t v[6];
+    if (i0 + 4 <= K) {
+      const uint4 x = *reinterpret_cast<const uint4 *>(keys + i0);
+      v[1] = x.x;
+      v[2] = x.y;
+      v[3] = x.z;
+      v[4] = x.w;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) v[1 + k] = i0 + k < K ? keys[i0 + k] : 0xffffffffu;
+    }
+    v[0] = i0 > 0 ? keys[i0 - 1] : 0xffffffffu;
+    v[5] = i0 + 4 < K ? keys[i0 + 4] : 0xffffffffu;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t i = i0 + k;
+      if (i >= K) break;
+      const uint32_t t = v[1 + k];
+      if (i == 0 || v[k] != t) ranges[t].x = i;
+      if (i + 1 == K || v[2 + k] != t) ranges[t].y = i + 1;
+    }
   }
 }
 
