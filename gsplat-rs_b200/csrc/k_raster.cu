@@ -252,25 +252,46 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
       n_w += __popc(bal);
     }
     __syncwarp();
-    for (uint32_t i = 0; i < n_w; ++i) {
-      if (__all_sync(0xffffffffu, done)) break;
-      const uint32_t j = sm.list[warp][i];
-      const float4 d0 = sm.d0[j];
-      const float4 d1 = sm.d1[j];
-      float lx = fmaf(d0.x, fx, fmaf(d0.y, fy, d0.z));
-      float ly = fmaf(d1.x, fx, fmaf(d1.y, fy, d1.z));
-      float r2 = fmaf(lx, lx, ly * ly);
-      if (done || !(r2 <= d0.w)) continue;
-      float g = gauss_weight(r2);
-      float w = d1.w * g;
-      if (!(w > 1.0f / 256.0f)) continue;
+    // Two list entries per step (one early-out vote, one packed index
+    // load); each pixel still takes them strictly in list order.
+    auto blend = [&](uint32_t j, float r2, float s2, float w_alpha) {
+      if (done || !(r2 <= s2)) return;
+      const float g = gauss_weight(r2);
+      const float w = w_alpha * g;
+      if (!(w > 1.0f / 256.0f)) return;
       const float4 col = sm.d2[j];
-      float gT = g * T;
+      const float gT = g * T;
       c0 = fmaf(col.x, gT, c0);
       c1 = fmaf(col.y, gT, c1);
       c2 = fmaf(col.z, gT, c2);
       T = T * (1.0f - w);
       if (T < 1e-4f) done = true;
+    };
+    auto local_r2 = [&](uint32_t j, float &s2, float &alpha) {
+      const float4 d0 = sm.d0[j];
+      const float4 d1 = sm.d1[j];
+      const float lx = fmaf(d0.x, fx, fmaf(d0.y, fy, d0.z));
+      const float ly = fmaf(d1.x, fx, fmaf(d1.y, fy, d1.z));
+      s2 = d0.w;
+      alpha = d1.w;
+      return fmaf(lx, lx, ly * ly);
+    };
+    uint32_t i = 0;
+    for (; i + 1 < n_w; i += 2) {
+      if (__all_sync(0xffffffffu, done)) break;
+      const uint32_t jj = *reinterpret_cast<const uint32_t *>(&sm.list[warp][i]);
+      const uint32_t ja = jj & 0xffffu, jb = jj >> 16;
+      float sa, aa, sb, ab;
+      const float r2a = local_r2(ja, sa, aa);
+      const float r2b = local_r2(jb, sb, ab);
+      blend(ja, r2a, sa, aa);
+      blend(jb, r2b, sb, ab);
+    }
+    if (i < n_w && !__all_sync(0xffffffffu, done)) {
+      const uint32_t ja = sm.list[warp][i];
+      float sa, aa;
+      const float r2a = local_r2(ja, sa, aa);
+      blend(ja, r2a, sa, aa);
     }
     if (__syncthreads_count(done) == kTile * kTile) break;
   }
