@@ -25,6 +25,7 @@
 #include "device_common.cuh"
 #include "kernels.h"
 
+
 namespace gsr {
 namespace {
 
@@ -213,24 +214,32 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
       const float qc = fmaf(ra.w, ra.w, rb.y * rb.y);
       const float s2 = rb.z * rb.z;
       const float det = fmaf(qa, qc, -qb * qb);
-      const float inv_a = 1.0f / qa;
-      const float hx = sqrtf(s2 * qc / det);
-      const float hy = sqrtf(s2 * qa / det);
-      const float dy_left = qb * hx / qc;  // dy of the leftmost point; rightmost at -dy_left
+      // The mask only culls: hardware reciprocal/rsqrt (a few ulp) plus an
+      // inflation of the extents far above their error keeps it conservative.
+      const float inv_a = __fdividef(1.0f, qa);
+      const float inv_det = __fdividef(1.0f, det);
+      const float hx2 = s2 * qc * inv_det, hy2 = s2 * qa * inv_det;
+      const float hx_raw = hx2 * rsqrtf(fmaxf(hx2, 1e-30f));
+      const float hx = fmaf(hx_raw, 1.0001f, 1e-3f);
+      const float hy = fmaf(hy2 * rsqrtf(fmaxf(hy2, 1e-30f)), 1.0001f, 1e-3f);
+      // dy of the leftmost point (rightmost at -dy_left), from the unpadded extent
+      const float dy_left = qb * hx_raw * __fdividef(1.0f, qc);
       const float s2a = s2 * qa;
+      constexpr float kPad = 0.5f + 1.0f / 64.0f;
       uint32_t mask = 0;
 #pragma unroll
       for (int band = 0; band < kTile / 4; ++band) {
         const float lo = fmaxf((float)(4 * band) - 0.5f - cyl, -hy);
         const float hi = fminf((float)(4 * band) + 3.5f - cyl, hy);
         if (!(lo <= hi)) continue;
-        const float r_lo = sqrtf(fmaxf(s2a - det * lo * lo, 0.0f));
-        const float r_hi = sqrtf(fmaxf(s2a - det * hi * hi, 0.0f));
+        const float qlo = fmaxf(s2a - det * lo * lo, 0.0f), qhi = fmaxf(s2a - det * hi * hi, 0.0f);
+        const float r_lo = fmaf(qlo * rsqrtf(fmaxf(qlo, 1e-30f)), 1.0001f, 1e-3f);
+        const float r_hi = fmaf(qhi * rsqrtf(fmaxf(qhi, 1e-30f)), 1.0001f, 1e-3f);
         float xmin = fminf((-qb * lo - r_lo) * inv_a, (-qb * hi - r_hi) * inv_a);
         float xmax = fmaxf((-qb * lo + r_lo) * inv_a, (-qb * hi + r_hi) * inv_a);
         if (dy_left >= lo && dy_left <= hi) xmin = -hx;
         if (-dy_left >= lo && -dy_left <= hi) xmax = hx;
-        const float bx0f = cxl + xmin - 0.5f, bx1f = cxl + xmax + 0.5f;
+        const float bx0f = cxl + xmin - kPad, bx1f = cxl + xmax + kPad;
 #pragma unroll
         for (int colb = 0; colb < kBlocksX; ++colb)
           if (bx1f >= (float)(8 * colb) && bx0f <= (float)(8 * colb + 7))
