@@ -130,7 +130,7 @@ T *PinnedArray<T>::ensure(size_t n) {
   if (p_) cudaFreeHost(p_);
   p_ = nullptr;
   cap_ = 0;
-  const size_t cap = std::max<size_t>(n, 64);
+  const size_t cap = std::max<size_t>(std::max<size_t>(n, 64), 2 * cap_);
   GSR_CUDA(cudaMallocHost(&p_, sizeof(T) * cap));
   std::memset(p_, 0, sizeof(T) * cap);
   cap_ = cap;

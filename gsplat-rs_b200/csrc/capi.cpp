@@ -897,7 +897,8 @@ int32_t gsplat_server_get_stats(GsplatServer *server, GsplatServeStats *out_stat
     const gsr::ServeStats s = server->server->stats();
     *out_stats = GsplatServeStats{s.submitted, s.completed, s.failed, s.batches, s.reruns,
                                   s.peak_admitted_bytes, s.p50_ms, s.p99_ms, s.mean_ms, s.max_ms,
-                                  s.views_per_s, s.mean_batch_views};
+                                  s.views_per_s, s.mean_batch_views, s.device_ms, s.launch_ms,
+                                  s.retire_ms};
     return ok();
   });
 }

@@ -203,8 +203,17 @@ void Pipeline::ensure_workspace(const Layout &l) {
   if (l.views > view_cap_ || n > splat_cap_ || !view_ws_.get()) {
     GSR_CUDA(cudaStreamSynchronize(stream_));  // earlier runs may still use the old buffers
     drop_graph();
-    const uint32_t vcap = std::max(l.views, view_cap_);
-    const uint32_t ncap = std::max(n, splat_cap_);
+    // Growth is geometric: a reallocation synchronises the device (cudaFree),
+    // so a stream of batches of varying size must not regrow every time.
+    const uint32_t vcap = l.views > view_cap_
+                              ? std::min<uint32_t>(std::max(l.views, view_cap_ + view_cap_ / 2),
+                                                   kMaxViewsPerLaunch)
+                              : view_cap_;
+    const uint32_t ncap = n > splat_cap_
+                              ? (uint32_t)std::min<uint64_t>(
+                                    std::max<uint64_t>(n, splat_cap_ + (uint64_t)splat_cap_ / 2),
+                                    kMaxSortItems)
+                              : splat_cap_;
     // view workspace: [view counters | K1 status | emit status] zeroed, then the table.
     const uint64_t k1_words = (ncap + 255) / 256 + 1;  // + views: blocks round up per set
     const uint64_t k1_total = k1_words + vcap;
@@ -263,7 +272,7 @@ void Pipeline::ensure_workspace(const Layout &l) {
   if (l.total_tiles > tile_cap_ || !tile_ws_.get()) {
     GSR_CUDA(cudaStreamSynchronize(stream_));
     drop_graph();
-    tile_cap_ = std::max(l.total_tiles, tile_cap_);
+    tile_cap_ = std::max(l.total_tiles, tile_cap_ + tile_cap_ / 2);
     tile_ws_.reset(align256(8ull * std::max<uint32_t>(tile_cap_, 1)));
     ranges_ = tile_ws_.as<uint2>();
   }
@@ -293,7 +302,9 @@ void Pipeline::ensure_key_workspace(uint64_t capacity) {
                                        " exceeds the renderer's limit of 2^30 - 1");
   GSR_CUDA(cudaStreamSynchronize(stream_));
   drop_graph();
-  const uint32_t cap = (uint32_t)capacity;
+  // geometric growth, as for the other workspaces
+  const uint32_t cap = (uint32_t)std::min<uint64_t>(
+      std::max<uint64_t>(capacity, key_cap_ + key_cap_ / 4), kMaxSortItems);
   const uint64_t words = sort_work_words(cap, passes);
   uint64_t off = 0;
   uint64_t o_k0 = off; off += align256(4ull * cap);

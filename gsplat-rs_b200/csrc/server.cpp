@@ -21,7 +21,7 @@ double now_ms() {
 // ---- PinnedPool --------------------------------------------------------------
 
 PinnedPool::~PinnedPool() {
-  for (uint8_t *p : all_) cudaFreeHost(p);
+  for (uint8_t *p : slabs_) cudaFreeHost(p);
 }
 
 uint8_t *PinnedPool::take(uint64_t bytes) {
@@ -34,11 +34,17 @@ uint8_t *PinnedPool::take(uint64_t bytes) {
       return p;
     }
   }
-  void *p = nullptr;
-  GSR_CUDA(cudaMallocHost(&p, bytes));
+  // Pinned allocations are slow (milliseconds): allocate a slab of many
+  // buffers of this size at once and hand out the rest later.
+  const uint64_t stride = (bytes + 255) & ~uint64_t(255);
+  const uint64_t count = std::max<uint64_t>(1, std::min<uint64_t>(64, (kSlabBytes + stride - 1) / stride));
+  void *slab = nullptr;
+  GSR_CUDA(cudaMallocHost(&slab, stride * count));
   std::lock_guard<std::mutex> g(mu_);
-  all_.push_back((uint8_t *)p);
-  return (uint8_t *)p;
+  slabs_.push_back((uint8_t *)slab);
+  auto &list = free_[bytes];
+  for (uint64_t k = 1; k < count; ++k) list.push_back((uint8_t *)slab + k * stride);
+  return (uint8_t *)slab;
 }
 
 void PinnedPool::give(uint8_t *p, uint64_t bytes) {
@@ -184,6 +190,9 @@ ServeStats Server::stats() {
       s.views_per_s = 1000.0 * l.size() / (last_done_ - first_submit_);
   }
   s.mean_batch_views = batches_ ? (double)batch_views_ / batches_ : 0.0;
+  s.device_ms = device_ms_;
+  s.launch_ms = launch_ms_;
+  s.retire_ms = retire_ms_;
   return s;
 }
 
@@ -194,6 +203,7 @@ void Server::reset_stats() {
   peak_admitted_ = 0;
   first_submit_ = -1;
   last_done_ = 0;
+  device_ms_ = launch_ms_ = retire_ms_ = 0;
 }
 
 uint64_t Server::view_bytes(const ViewSpec &s, uint64_t pairs) const {
@@ -274,6 +284,7 @@ bool Server::launch(LaneState &ls, std::unique_lock<std::mutex> &lk) {
   ls.busy = true;
   ls.completed.store(false);
   lk.unlock();
+  const double t_enqueue = now_ms();
   try {
     for (size_t k = 0; k < ls.ids.size(); ++k)
       ls.dst[k] = pool_.take(4ull * ls.specs[k].width * ls.specs[k].height);
@@ -298,20 +309,25 @@ bool Server::launch(LaneState &ls, std::unique_lock<std::mutex> &lk) {
     done_cv_.notify_all();
     return true;
   }
+  const double t_enqueued = now_ms();
   lk.lock();
   ++batches_;
   batch_views_ += ls.ids.size();
+  launch_ms_ += t_enqueued - t_enqueue;
   return true;
 }
 
 void Server::retire(LaneState &ls, std::unique_lock<std::mutex> &lk) {
   const double t_done = ls.t_complete.load();
   lk.unlock();
+  const double t_retire = now_ms();
   uint32_t reruns = 0;
+  float batch_device_ms = 0;
   std::string err;
   int32_t code = 0;
   try {
     reruns = ls.lane->finish(ls.specs, ls.bases, ls.groups);
+    batch_device_ms = ls.lane->device_ms();
     if (reruns) {
       // images were re-rendered: copy them again
       const uint32_t *img = ls.lane->images();
@@ -326,7 +342,10 @@ void Server::retire(LaneState &ls, std::unique_lock<std::mutex> &lk) {
     code = (int32_t)e.code;
   }
   const double t_final = reruns ? now_ms() : t_done;
+  const double t_retired = now_ms();
   lk.lock();
+  device_ms_ += batch_device_ms;
+  retire_ms_ += t_retired - t_retire;
   for (size_t k = 0; k < ls.ids.size(); ++k) {
     Request &r = requests_.at(ls.ids[k]);
     r.result = ls.dst[k];

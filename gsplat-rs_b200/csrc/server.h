@@ -53,9 +53,13 @@ struct ServeStats {
   double views_per_s = 0;      // completed / (last completion - first submit)
   double mean_batch_views = 0;
   uint64_t peak_admitted_bytes = 0;
+  double device_ms = 0;        // CUDA-event time of the batches' pipelines (sum)
+  double launch_ms = 0;        // host time spent enqueuing batches (sum)
+  double retire_ms = 0;        // host time spent retiring batches (sum)
 };
 
-// Pinned host buffers recycled by size.
+// Pinned host buffers recycled by size, carved from slabs of about 64 MB
+// (at most 64 buffers per slab).
 class PinnedPool {
  public:
   ~PinnedPool();
@@ -63,9 +67,10 @@ class PinnedPool {
   void give(uint8_t *p, uint64_t bytes);
 
  private:
+  static constexpr uint64_t kSlabBytes = 64ull << 20;
   std::mutex mu_;
   std::map<uint64_t, std::vector<uint8_t *>> free_;
-  std::vector<uint8_t *> all_;
+  std::vector<uint8_t *> slabs_;
 };
 
 class Server {
@@ -134,6 +139,7 @@ class Server {
   uint64_t submitted_ = 0, failed_ = 0, batches_ = 0, batch_views_ = 0, reruns_ = 0;
   uint64_t peak_admitted_ = 0;
   double first_submit_ = -1, last_done_ = 0;
+  double device_ms_ = 0, launch_ms_ = 0, retire_ms_ = 0;
   std::thread thread_;
 };
 

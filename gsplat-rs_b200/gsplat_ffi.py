@@ -135,7 +135,9 @@ class GsplatServeStats(ctypes.Structure):
                 ("reruns", ctypes.c_uint64), ("peak_admitted_bytes", ctypes.c_uint64),
                 ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
                 ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
-                ("views_per_s", ctypes.c_double), ("mean_batch_views", ctypes.c_double)]
+                ("views_per_s", ctypes.c_double), ("mean_batch_views", ctypes.c_double),
+                ("device_ms", ctypes.c_double), ("launch_ms", ctypes.c_double),
+                ("retire_ms", ctypes.c_double)]
 
 
 REQUEST_QUEUED, REQUEST_RUNNING, REQUEST_DONE, REQUEST_FAILED = 0, 1, 2, 3

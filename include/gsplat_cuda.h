@@ -317,7 +317,10 @@ typedef struct GsplatServeStats {
   double p50_ms, p99_ms, mean_ms, max_ms;  /* request latency, nearest rank */
   double views_per_s;        /* completed / (last completion - first submit) */
   double mean_batch_views;
-} GsplatServeStats;          /* 96 bytes */
+  double device_ms;          /* CUDA-event time of the batches' launch sequences, summed */
+  double launch_ms;          /* host time spent enqueuing batches, summed */
+  double retire_ms;          /* host time spent retiring batches, summed */
+} GsplatServeStats;          /* 120 bytes */
 
 int32_t gsplat_server_create(const GsplatServeConfig *config, GsplatServer **out_server);
 /* Finishes the batches in flight, fails queued requests and frees everything. */
