@@ -411,6 +411,82 @@ def measure_served(ffi, rates, seconds, max_requests):
             "rates": out}
 
 
+def write_plain_artifact(args, ffi, ctx, scene, cams, out, w, h):
+    """The plain frames as a benchmark artifact in the reference's v1 contract
+    (manifest.json, frames.jsonl, summary.json under args.artifact): one frame
+    per camera through the C ABI, per-frame host and device times."""
+    import platform
+    import uuid
+
+    import bench_artifact
+
+    run_id = "b200-plain-" + uuid.uuid4().hex[:12]
+    started = bench_artifact.utc_now()
+    for c in cams[:3]:
+        ctx.set_camera(c)
+        ctx.render_frame()
+    m_start = bench_artifact.utc_now()
+    frames = bench_artifact.record_frames(ctx, cams, out, run_id)
+    m_end = bench_artifact.utc_now()
+    commit, dirty = None, None
+    try:
+        commit = subprocess.run(["git", "-C", ROOT, "rev-parse", "HEAD"], capture_output=True,
+                                text=True, check=True).stdout.strip() or None
+        dirty = bool(subprocess.run(["git", "-C", ROOT, "status", "--porcelain"],
+                                    capture_output=True, text=True, check=True).stdout.strip())
+    except (OSError, subprocess.CalledProcessError):
+        commit, dirty = None, None
+    dev = ffi.device_info()
+    driver = None
+    try:
+        driver = subprocess.run(["nvidia-smi", "--query-gpu=driver_version", "--format=csv,noheader"],
+                                capture_output=True, text=True, check=True).stdout.strip().splitlines()[0]
+    except (OSError, subprocess.CalledProcessError, IndexError):
+        driver = None
+    arrays = [np.ascontiguousarray(scene[k], np.float32) for k in
+              ("positions", "opacity", "scale_xyz", "rotation_xyzw", "color_dc")]
+    if scene.get("sh_rest") is not None:
+        arrays.append(np.ascontiguousarray(scene["sh_rest"], np.float32))
+    trace = np.array([[*c.position, *c.rotation_xyzw, c.vertical_fov_radians] for c in cams],
+                     np.float32)
+    unavailable = ["environment.browser"]
+    if commit is None:
+        unavailable.append("build.repository_commit")
+    if dirty is None:
+        unavailable.append("build.dirty")
+    if driver is None:
+        unavailable.append("environment.driver")
+    manifest = {
+        "run_id": run_id,
+        "identity": {"series_id": "b200-plain-279k-sh3-1080p", "started_at_utc": started,
+                     "ended_at_utc": bench_artifact.utc_now(),
+                     "measurement_started_at_utc": m_start, "measurement_ended_at_utc": m_end},
+        "build": {"repository_commit": commit, "dirty": dirty, "profile": "release",
+                  "package_version": "0.1.0"},
+        "dataset": {"id": "synthetic-279199-sh3-gmm-seed1",
+                    "sha256": bench_artifact.sha256_of_arrays(arrays),
+                    "bytes": int(sum(a.nbytes for a in arrays)),
+                    "splat_count": int(scene["positions"].shape[0]),
+                    "sh_degree": int(scene["sh_degree"])},
+        "trace": {"id": "orbit-r4-yaw0.7-step0.002", "sha256": bench_artifact.sha256_of_arrays([trace])},
+        "renderer": {"implementation": "gsplat-rs-b200-cuda", "path": "sorted_alpha_cuda_tiles",
+                     "backend": "cuda-sm_100a", "sort_policy": "gpu_every_frame"},
+        "display": {"width": w, "height": h, "dpr": 1.0, "refresh_hz": 60.0,
+                    "frame_budget_ms": 1000.0 / 60.0, "refresh_hz_source": "configured",
+                    "frame_budget_source": "configured"},
+        "environment": {"platform": platform.machine(), "os": platform.platform(),
+                        "device": dev["name"], "browser": None, "adapter": dev["name"],
+                        "driver": driver},
+        "timing": {"frame_wall_source": "host time of set_camera + gsplat_context_render_frame + "
+                                        "RGBA8 readback into pinned memory (no presentation surface)",
+                   "device_timings": "CUDA events on the renderer's stream"},
+        "unavailable_fields": unavailable,
+    }
+    bench_artifact.write_artifact(args.artifact, manifest, frames, warmup_count=3,
+                                  frame_budget_ms=1000.0 / 60.0)
+    bench_artifact.validate(args.artifact)
+
+
 def run_sections_only(args, ffi, torch):
     """The batched and/or served sections alone (no plain-frame line), for
     profiling those workloads by themselves."""
@@ -508,6 +584,8 @@ def run_cuda(args, world, rank, local):
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
+    if args.artifact and rank == 0:
+        write_plain_artifact(args, ffi, ctx, scene, cams, out, w, h)
     clk = clocks.stop()
     e2e = {"value": world * args.steps / e2e_s, "unit": "frames/s",
            "h2d_bytes_per_step": 40, "d2h_bytes_per_step": w * h * 4 + 64}
@@ -575,6 +653,8 @@ def main():
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--serve-rates", default="500,2000,8000,20000")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
+    ap.add_argument("--artifact", default="",
+                    help="also write the plain frames as a v1 benchmark artifact into this folder")
     ap.add_argument("--only", default="",
                     help="comma list of batched,served: run just those sections (profiling)")
     args = ap.parse_args()

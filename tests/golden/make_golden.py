@@ -155,6 +155,18 @@ def main():
     }
     with open(os.path.join(HERE, "kats.json"), "w") as f:
         json.dump(kats, f, indent=1)
+
+    # Benchmark artifact v1 (tests/perf/benchmark-artifact-v1.md): the
+    # product's producer writes the fixture, the reference's own validator
+    # must accept it.
+    import subprocess
+
+    import artifact_fixture
+
+    art = os.path.join(HERE, "artifact_v1")
+    artifact_fixture.write(art)
+    subprocess.run([sys.executable, os.path.join(REF, "tests/perf/validate-benchmark-artifacts.py"),
+                    art], check=True)
     print("golden fixtures written to", HERE)
 
 

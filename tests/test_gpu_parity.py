@@ -375,6 +375,44 @@ def test_raster_launch_shapes_do_not_change_pixels(oracle):
         ctx.set_raster_config(256, 33)
 
 
+def test_benchmark_artifact_from_rendered_frames(tmp_path):
+    """Real frames through the C ABI recorded as a v1 benchmark artifact
+    (the reference's contract) pass the contract checks."""
+    import bench_artifact
+
+    scene, cam, w, h = gsplat_scenes.config1(seed=14)
+    ctx = _ctx(w, h)
+    ctx.load_scene(scene)
+    rng = np.random.default_rng(3)
+    cams = [gsplat_scenes.orbit_camera(rng, (4.0, 6.0)) for _ in range(12)]
+    out = np.empty(w * h * 4, np.uint8)
+    frames = bench_artifact.record_frames(ctx, cams, out, "gpu-test-run")
+    assert all(f["gpu_complete_ms"] > 0 and f["call_ms"] > 0 for f in frames)
+    assert all(f["visible"] > 0 for f in frames)
+    manifest = {
+        "run_id": "gpu-test-run",
+        "identity": {k: "2026-12-01T00:00:00Z" for k in (
+            "started_at_utc", "ended_at_utc", "measurement_started_at_utc",
+            "measurement_ended_at_utc")} | {"series_id": "gpu-test"},
+        "build": {"repository_commit": None, "dirty": None, "profile": "release",
+                  "package_version": "0.1.0"},
+        "dataset": {"id": "config1-seed14", "sha256": "2" * 64, "bytes": 1, "splat_count": 16384,
+                    "sh_degree": 0},
+        "trace": {"id": "orbit", "sha256": "3" * 64},
+        "renderer": {"implementation": "gsplat-rs-b200-cuda", "path": "sorted_alpha_cuda_tiles",
+                     "backend": "cuda-sm_100a", "sort_policy": "gpu_every_frame"},
+        "display": {"width": w, "height": h, "dpr": 1.0, "refresh_hz": 60.0,
+                    "frame_budget_ms": 16.7, "refresh_hz_source": "configured",
+                    "frame_budget_source": "configured"},
+        "environment": {"platform": "x", "os": "x", "device": "B200", "browser": None,
+                        "adapter": "B200", "driver": None},
+        "unavailable_fields": ["build.repository_commit", "build.dirty", "environment.browser",
+                               "environment.driver"],
+    }
+    bench_artifact.write_artifact(str(tmp_path), manifest, frames, 0, 16.7)
+    assert bench_artifact.validate(str(tmp_path))["frames"] == 12
+
+
 def test_c_smoke_programs_run():
     exe = os.path.join(ROOT, "tests", "ffi", "_build_smoke")
     subprocess.run(["gcc", "-O2", "-I", os.path.join(ROOT, "include"),
