@@ -22,7 +22,8 @@ Mapping of this renderer's frame onto the contract's fields:
   gpu_complete_ms     device time of the whole frame (all phases)
   geometry_submit_ms  null: the scene is resident, no geometry is submitted
   gpu_wait_ms         null: the call waits inside the library
-  sort_refreshed      true: every frame sorts
+  sort_refreshed      whether the frame sorted its depth order (always, unless
+                      a sort interval is set on the context)
 """
 
 import hashlib
@@ -239,7 +240,8 @@ def record_frames(ctx, cameras, out, run_id, t_origin_ns=None):
             run_id, k, te - t0, (tr - tc) / 1e6, (te - ts) / 1e6, st.visible_count,
             st.drawn_count, preprocess_ms=ph["preprocess"],
             sort_ms=ph["depth_sort"] + ph["emit"] + ph["tile_sort"] + ph["ranges"],
-            gpu_complete_ms=sum(ph.values())))
+            gpu_complete_ms=sum(ph.values()),
+            sort_refreshed=bool(ctx.frame_counts().sort_refreshed)))
     return frames
 
 

@@ -373,6 +373,14 @@ int32_t gsplat_context_set_raster_config(GsplatContext *ctx, uint32_t chunk, uin
   });
 }
 
+int32_t gsplat_context_set_sort_interval(GsplatContext *ctx, uint32_t interval) {
+  return guarded("gsplat_context_set_sort_interval", [&]() -> int32_t {
+    if (!ctx) return fail(Code::InvalidArgument, "gsplat_context_set_sort_interval: ctx is null");
+    ctx->renderer->set_sort_interval(interval);
+    return ok();
+  });
+}
+
 int32_t gsplat_context_load_scene_buffers(GsplatContext *ctx, const GsplatSceneDesc *scene) {
   return guarded("gsplat_context_load_scene_buffers", [&]() -> int32_t {
     if (!ctx || !scene)
@@ -410,6 +418,7 @@ int32_t gsplat_context_get_frame_counts(const GsplatContext *ctx, GsplatFrameCou
     out->raster_ms = f.raster_ms;
     out->frame_ms = f.frame_ms;
     out->frame_reruns = f.reruns;
+    out->sort_refreshed = f.sorted ? 1u : 0u;
     return ok();
   });
 }

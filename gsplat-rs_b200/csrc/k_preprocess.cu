@@ -389,9 +389,14 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
       if (drawn) b.records[gid] = rec;
       area = ((rect.y & 0xffffu) - (rect.x & 0xffffu)) * ((rect.y >> 16) - (rect.x >> 16));
       // Digit histograms of the depth keys for every radix pass.
-      const uint32_t key = ~__float_as_uint(fmaxf(depth, 0.0f));
+      if (!b.reuse_order) {
+        const uint32_t key = ~__float_as_uint(fmaxf(depth, 0.0f));
 #pragma unroll
-      for (int d = 0; d < 4; ++d) atomicAdd(&s_hist[d][(key >> (8 * d)) & 255u], 1u);
+        for (int d = 0; d < 4; ++d) atomicAdd(&s_hist[d][(key >> (8 * d)) & 255u], 1u);
+      }
+    } else if (b.reuse_order && valid) {
+      // The reused order may list this splat: it emits no tile this frame.
+      b.rects[gid] = make_uint2(0u, 0u);
     }
     const uint32_t dmask = __ballot_sync(0xffffffffu, drawn);
     area = warp_sum(area);
@@ -422,7 +427,7 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
     }
     const bool vis = (vis_bits >> k) & 1u;
     const uint32_t bal = __ballot_sync(0xffffffffu, vis);
-    if (vis) {
+    if (vis && !b.reuse_order) {
       const uint32_t view = set.first_view + k;
       const FrameParams &p = s_params[k];
       const float rx = pa.x - p.cam[0], ry = pa.y - p.cam[1], rz = pa.z - p.cam[2];

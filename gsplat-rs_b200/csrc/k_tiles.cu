@@ -44,7 +44,9 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b) {
     s_vtx[v] = b.views[v].p.tiles_x;
   }
   __syncthreads();
-  const uint32_t V = b.counters->visible;
+  // The sorted visible ids: this frame's, or the order reused from the last
+  // sort (the plan keeps its count).
+  const uint32_t V = b.depth_plan->n;
   const uint32_t block = s_block;
   const uint32_t start = block * kEmitItems;
   if (start >= V) return;

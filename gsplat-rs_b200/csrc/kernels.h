@@ -29,6 +29,9 @@ struct K1Buffers {
   uint32_t *key_hist;          // [4][256] digit histograms of the depth keys, zeroed
   ViewCounters *view_counters; // [views], zeroed
   ProjectedDev *projected;     // [gid] debug tap, or null
+  // Reuse of the last sorted order: project and count as usual, but write no
+  // keys, ids or histograms, and clear the rects of splats not visible now.
+  bool reuse_order;
 };
 uint32_t preprocess_blocks(uint32_t splats);  // blocks one view set of `splats` splats needs
 // One block per 256 splats of each view set (views of one scene handled
@@ -62,7 +65,7 @@ void launch_sort(const SortBuffers &b, cudaStream_t stream);
 
 // ---- K2: tile-pair emission over the depth-sorted visible ids ------------
 struct EmitBuffers {
-  const SortPlan *depth_plan;      // selects the buffer holding the sorted ids
+  const SortPlan *depth_plan;      // selects the buffer holding the sorted ids; n = their count
   const uint32_t *ids0, *ids1;     // depth-sorted gids, [visible]
   const uint2 *rects;              // [gid]
   uint32_t *tile_keys, *tile_vals; // [capacity] output pairs (global tile id, gid)

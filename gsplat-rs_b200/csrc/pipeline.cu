@@ -258,6 +258,7 @@ void Pipeline::ensure_workspace(const Layout &l) {
       uint64_t o_work = off; off += align256(4 * words);
       splat_ws_.reset(0);
       splat_ws_.reset(off);
+      sorted_valid_ = false;  // the sorted ids lived in the old buffers
       vis_keys0_ = splat_ws_.as<uint32_t>(o_k0);
       vis_vals0_ = splat_ws_.as<uint32_t>(o_v0);
       vis_keys1_ = splat_ws_.as<uint32_t>(o_k1b);
@@ -323,7 +324,8 @@ void Pipeline::ensure_key_workspace(uint64_t capacity) {
   debug_pairs_.reset(0);
 }
 
-void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &sinks) {
+void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &sinks,
+                          bool reuse) {
   const uint32_t n = std::max<uint32_t>(l.total_splats, 1);
   GSR_CUDA(cudaMemsetAsync(fixed_.get(), 0,
                            (char *)depth_plan_ - (char *)fixed_.get(), stream_));
@@ -331,15 +333,18 @@ void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &si
   GSR_CUDA(cudaMemsetAsync(ranges_, 0, 8ull * l.total_tiles, stream_));
   record(0);
 
-  K1Buffers k1{vis_keys0_, vis_vals0_, rects_, records_, k1_status_, counters_, key_hist_,
-               view_counters_, debug_ ? projected_.as<ProjectedDev>() : nullptr};
+  K1Buffers k1{vis_keys0_, vis_vals0_, rects_,         records_,
+               k1_status_, counters_,  key_hist_,      view_counters_,
+               debug_ ? projected_.as<ProjectedDev>() : nullptr, reuse};
   launch_preprocess(views_dev_, sets_dev_, l.sets, l.total_blocks, l.max_planes, k1, debug_,
                     stream_);
   record(1);
 
-  SortBuffers ds{vis_keys0_, vis_vals0_, vis_keys1_, vis_vals1_, &counters_->visible, n, 0, 4,
-                 depth_plan_, depth_sort_work_, &counters_->error, key_hist_};
-  launch_sort(ds, stream_);
+  if (!reuse) {  // a reused order keeps the last sort's ids and plan
+    SortBuffers ds{vis_keys0_, vis_vals0_, vis_keys1_, vis_vals1_, &counters_->visible, n, 0, 4,
+                   depth_plan_, depth_sort_work_, &counters_->error, key_hist_};
+    launch_sort(ds, stream_);
+  }
   record(2);
 
   EmitBuffers eb{depth_plan_, vis_vals0_, vis_vals1_, rects_, tile_keys0_, tile_vals0_, key_cap_,
@@ -378,6 +383,11 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
   ensure_workspace(l);
   if (!sinks.counters) sinks.counters = counters_host_;
   if (!sinks.views) sinks.views = view_counters_pinned_;
+  // The last sorted order can be reused only for the identical layout (same
+  // scenes, sizes and tile grid) and while its buffers are intact.
+  const bool reuse = reuse_request_ && sorted_valid_ && l == sorted_layout_ &&
+                     std::equal(views, views + count, sorted_scenes_.begin(), sorted_scenes_.end(),
+                                [](const ViewSpec &v, const DeviceScene *s) { return v.scene == s; });
   // The view table goes up from a pinned ring slot, asynchronously; the
   // slot's previous copy is long done in steady state.
   GSR_CUDA(cudaEventSynchronize(slot_ev_[slot_]));
@@ -393,10 +403,10 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
   slot_ = (slot_ + 1) % kViewSlots;
 
   if (!use_graph_) {
-    launch_all(l, images, sinks);
+    launch_all(l, images, sinks, reuse);
   } else {
-    const GraphKey key{l,     images,         key_cap_,       tile_,       blend_mode_,
-                       debug_, raster_cfg_, sinks.counters, sinks.views};
+    const GraphKey key{l,     images,      key_cap_,       tile_,       blend_mode_,
+                       debug_, raster_cfg_, sinks.counters, sinks.views, reuse};
     GraphEntry *hit = nullptr;
     for (auto &g : graphs_)
       if (g.key == key) hit = &g;
@@ -413,7 +423,7 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
       }
     }
     if (!hit && !seen) {
-      launch_all(l, images, sinks);
+      launch_all(l, images, sinks, reuse);
     } else if (!hit) {
       if (graphs_.size() >= kGraphCacheSize) {
         auto lru = std::min_element(graphs_.begin(), graphs_.end(),
@@ -427,7 +437,7 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
       GSR_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
       capturing_ = true;
       try {
-        launch_all(l, images, sinks);
+        launch_all(l, images, sinks, reuse);
       } catch (...) {
         capturing_ = false;
         cudaStreamEndCapture(stream_, &g);
@@ -455,6 +465,13 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
   last_layout_ = l;
   last_sinks_ = sinks;
   has_run_ = true;
+  last_reused_ = reuse;
+  if (!reuse) {
+    sorted_layout_ = l;
+    sorted_valid_ = true;
+    sorted_scenes_.clear();
+    for (uint32_t v = 0; v < count; ++v) sorted_scenes_.push_back(views[v].scene);
+  }
 }
 
 void Pipeline::collect(RunResult &r) {
@@ -464,6 +481,7 @@ void Pipeline::collect(RunResult &r) {
   r.preprocess_ms = t[kPhasePreprocess];
   r.sort_ms = t[kPhaseDepthSort] + t[kPhaseEmit] + t[kPhaseTileSort] + t[kPhaseRanges];
   r.raster_ms = t[kPhaseRaster];
+  r.sorted = !last_reused_;
   r.visible = last_sinks_.counters->visible;
   r.drawn = last_sinks_.counters->drawn;
   r.keys = last_sinks_.counters->keys;
@@ -535,7 +553,7 @@ SortPlan Pipeline::read_plan(int which) {
 std::vector<uint32_t> Pipeline::debug_order() {
   GSR_CUDA(cudaSetDevice(device_));
   SortPlan plan = read_plan(0);
-  std::vector<uint32_t> out(last_.visible);
+  std::vector<uint32_t> out(plan.n);
   if (!out.empty())
     GSR_CUDA(cudaMemcpy(out.data(), plan.final_buffer == 0 ? vis_vals0_ : vis_vals1_,
                         4 * out.size(), cudaMemcpyDeviceToHost));

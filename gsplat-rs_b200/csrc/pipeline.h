@@ -61,6 +61,7 @@ struct RunResult {
   float preprocess_ms = 0, sort_ms = 0, raster_ms = 0, frame_ms = 0;
   uint64_t visible = 0, drawn = 0, keys = 0;
   uint32_t reruns = 0;
+  bool sorted = true;  // false: the last sorted order was reused
 };
 
 // Pinned host destinations of a run's counters (default: the pipeline's own).
@@ -82,6 +83,12 @@ class Pipeline {
   void set_debug(bool on) { debug_ = on; }
   bool debug() const { return debug_; }
   void set_use_graph(bool on) { use_graph_ = on; }
+  // Asks the next runs to reuse the last sorted visible order instead of
+  // sorting (honoured only for a layout identical to the one last sorted):
+  // splats are projected with the new camera, but only those in the reused
+  // order can be drawn, in its order.
+  void set_reuse_order(bool on) { reuse_request_ = on; }
+  bool last_reused_order() const { return last_reused_; }
   // Throws InvalidArgument unless valid for the current tile size.
   void set_raster_config(const RasterConfig &c);
   const RasterConfig &raster_config() const { return raster_cfg_; }
@@ -135,7 +142,7 @@ class Pipeline {
   Layout plan_views(const ViewSpec *views, uint32_t count, const uint64_t *image_bases);
   void ensure_workspace(const Layout &l);
   void ensure_key_workspace(uint64_t capacity);
-  void launch_all(const Layout &l, uint32_t *images, const HostSinks &sinks);
+  void launch_all(const Layout &l, uint32_t *images, const HostSinks &sinks, bool reuse);
   void collect(RunResult &r);
   SortPlan read_plan(int which);
   void drop_graph();
@@ -147,6 +154,9 @@ class Pipeline {
   uint32_t tile_ = 16, blend_mode_ = 0, sm_count_ = 148;
   RasterConfig raster_cfg_;
   bool debug_ = false, use_graph_ = true, has_run_ = false, capturing_ = false;
+  bool reuse_request_ = false, last_reused_ = false, sorted_valid_ = false;
+  Layout sorted_layout_;
+  std::vector<const DeviceScene *> sorted_scenes_;  // scenes of the last sorted run
   Layout last_layout_;
   HostSinks last_sinks_;
   RunResult last_;
@@ -201,10 +211,11 @@ class Pipeline {
     RasterConfig raster;
     FrameCounters *host_counters;
     ViewCounters *host_views;
+    bool reuse;
     bool operator==(const GraphKey &o) const {
       return layout == o.layout && images == o.images && key_cap == o.key_cap &&
              tile == o.tile && blend == o.blend && debug == o.debug && raster == o.raster &&
-             host_counters == o.host_counters && host_views == o.host_views;
+             host_counters == o.host_counters && host_views == o.host_views && reuse == o.reuse;
     }
   };
   struct GraphEntry {

@@ -1,5 +1,6 @@
 // Plain frames: one view of the frame pipeline (no device code in this file).
 
+#include <cstring>
 #include <string>
 
 #include "cuda_check.h"
@@ -48,6 +49,7 @@ void Renderer::set_size(uint32_t width, uint32_t height) {
   width_ = width;
   height_ = height;
   has_frame_ = false;
+  force_sort_ = true;
 }
 
 void Renderer::set_tile(uint32_t tile) {
@@ -63,6 +65,7 @@ void Renderer::load_scene(const HostScene &s) {
   scene_.reset();
   scene_ = upload_scene(s, stream_);
   has_frame_ = false;
+  force_sort_ = true;
 }
 
 void Renderer::ensure_image() {
@@ -81,16 +84,43 @@ std::vector<ViewSpec> Renderer::one_view(const GsplatCamera &cam) {
   return {ViewSpec{scene_.get(), cam, width_, height_}};
 }
 
+void Renderer::set_sort_interval(uint32_t interval) { sort_interval_ = interval; }
+
+// Interval 0 sorts every frame, as the reference's Renderer::render_frame
+// does. Otherwise the reference's SurfaceFrameState::plan
+// (surface_session.rs:536-596): sort when forced, when there is no order
+// yet, or when the camera has changed `interval` times since the last sort.
+void Renderer::plan_order(const GsplatCamera &cam) {
+  const bool changed = !has_last_camera_ || std::memcmp(&cam, &last_camera_, sizeof cam) != 0;
+  if (changed) ++changes_since_sort_;
+  const bool refresh = sort_interval_ == 0 || force_sort_ ||
+                       (changed && changes_since_sort_ >= sort_interval_);
+  pipe_->set_reuse_order(!refresh);
+  last_camera_ = cam;
+  has_last_camera_ = true;
+}
+
+void Renderer::finish_order() {
+  if (!pipe_->last_reused_order()) {
+    changes_since_sort_ = 0;
+    force_sort_ = false;
+  }
+}
+
 FrameResult Renderer::render(const GsplatCamera &cam) {
   auto views = one_view(cam);
+  plan_order(cam);
   last_ = pipe_->run(views, image_.as<uint32_t>(), image_base_);
+  finish_order();
   has_frame_ = true;
   return last_;
 }
 
 void Renderer::render_async(const GsplatCamera &cam) {
   auto views = one_view(cam);
+  plan_order(cam);
   pipe_->enqueue(views, image_.as<uint32_t>(), image_base_);
+  finish_order();
   has_frame_ = true;
 }
 

@@ -34,6 +34,13 @@ class Renderer {
   void set_debug(bool on) { pipe_->set_debug(on); }
   void set_use_graph(bool on) { pipe_->set_use_graph(on); }
   void set_raster_config(const RasterConfig &c) { pipe_->set_raster_config(c); }
+  // Depth-order refresh cadence. 0 (the default): every frame sorts, as the
+  // reference's context does. k >= 1: the reference's surface sort interval —
+  // the order is re-sorted when the camera has changed k times since the
+  // last sort; other frames reuse the last sorted visible order with the new
+  // camera's projection.
+  void set_sort_interval(uint32_t interval);
+  uint32_t sort_interval() const { return sort_interval_; }
 
   void load_scene(const HostScene &s);
   bool has_scene() const { return scene_ != nullptr; }
@@ -65,11 +72,16 @@ class Renderer {
  private:
   std::vector<ViewSpec> one_view(const GsplatCamera &cam);
   void ensure_image();
+  void plan_order(const GsplatCamera &cam);  // sets the pipeline's order reuse
+  void finish_order();
 
   int device_ = 0;
   cudaStream_t stream_ = nullptr;
   uint32_t width_, height_;
   bool has_frame_ = false;
+  uint32_t sort_interval_ = 0, changes_since_sort_ = 0;
+  bool force_sort_ = true, has_last_camera_ = false;
+  GsplatCamera last_camera_{};
   std::unique_ptr<Pipeline> pipe_;
   std::unique_ptr<DeviceScene> scene_;
   FrameResult last_;

@@ -88,7 +88,7 @@ class GsplatFrameCounts(ctypes.Structure):
                 ("tile_size", ctypes.c_uint32), ("blend_mode", ctypes.c_uint32),
                 ("preprocess_ms", ctypes.c_float), ("sort_ms", ctypes.c_float),
                 ("raster_ms", ctypes.c_float), ("frame_ms", ctypes.c_float),
-                ("frame_reruns", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("frame_reruns", ctypes.c_uint32), ("sort_refreshed", ctypes.c_uint32)]
 
 
 class GsplatBatchView(ctypes.Structure):
@@ -203,6 +203,7 @@ _SIGS = [
     ("gsplat_context_set_cuda_graph", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
     ("gsplat_context_set_raster_config", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]),
+    ("gsplat_context_set_sort_interval", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
     ("gsplat_context_load_scene_buffers", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.POINTER(GsplatSceneDesc)]),
     ("gsplat_context_readback_rgba8", ctypes.c_int32, [ctypes.c_void_p, _u8p, ctypes.c_uint64]),
@@ -392,6 +393,9 @@ class Context:
 
     def set_raster_config(self, chunk, blocks_per_sm=0):
         check(lib().gsplat_context_set_raster_config(self.ptr, chunk, blocks_per_sm))
+
+    def set_sort_interval(self, interval):
+        check(lib().gsplat_context_set_sort_interval(self.ptr, interval))
 
     def load_scene_path(self, path):
         check(lib().gsplat_context_load_scene_path(self.ptr, os.fsencode(path)))

@@ -74,7 +74,7 @@ typedef struct GsplatFrameCounts {
   uint32_t tiles_x, tiles_y, tile_size, blend_mode;
   float preprocess_ms, sort_ms, raster_ms, frame_ms;
   uint32_t frame_reruns; /* frames re-run after growing the pair buffers */
-  uint32_t reserved;
+  uint32_t sort_refreshed; /* 1: the frame sorted its depth order; 0: it reused the last one */
 } GsplatFrameCounts;
 
 /* ---- context extensions ---- */
@@ -100,6 +100,16 @@ int32_t gsplat_context_set_cuda_graph(GsplatContext *ctx, uint32_t enabled);
  * at most 32). Changing the tile size resets an invalid chunk to the full
  * tile. Images do not depend on either setting. */
 int32_t gsplat_context_set_raster_config(GsplatContext *ctx, uint32_t chunk, uint32_t blocks_per_sm);
+/* Depth-order refresh cadence. 0 (the default) sorts every frame, as the
+ * reference's gsplat_context_render_frame does. interval >= 1 applies the
+ * reference's surface sort interval (crates/gsplat-render-wgpu/src/
+ * surface_session.rs:17, 536-596; gsplat_surface_renderer_set_sort_interval
+ * there): the visible splats are re-sorted when the camera has changed
+ * `interval` times since the last sort, and always after a scene load or
+ * resize. Frames in between (an unchanged camera included) project every
+ * splat with their own camera but draw only the splats of the last sorted
+ * order, in that order (stale-order frames, as in the reference). */
+int32_t gsplat_context_set_sort_interval(GsplatContext *ctx, uint32_t interval);
 
 /* Load a scene from host memory (validated like SceneBuffers::validate,
  * crates/gsplat-core/src/lib.rs:224-276). Replaces any loaded scene. */

@@ -230,12 +230,18 @@ def radix_count(values, shift, simd):
 class Frame:
     """Oracle evaluation of one SortedAlpha frame, stage by stage."""
 
-    def __init__(self, sv, cam, width, height, tile=16):
+    def __init__(self, sv, cam, width, height, tile=16, order=None):
+        """`order`: a back-to-front id list to draw instead of this camera's
+        own (a stale order, as the reference's surface session draws between
+        sort refreshes); every splat is still projected with `cam`."""
         L = lib()
         self.width, self.height, self.tile = width, height, tile
         self.params = frame_params(cam, width, height, tile, sv.degree)
         self.keys, self.visible_ids = preprocess_visible(sv.pos.reshape(-1, 3), cam)
-        self.order = sort_values_by_keys(self.keys, self.visible_ids.copy())
+        if order is None:
+            self.order = sort_values_by_keys(self.keys, self.visible_ids.copy())
+        else:
+            self.order = np.ascontiguousarray(order, np.uint32)
         n1 = max(sv.n, 1)
         self.proj = np.zeros(n1, PROJECTED_DTYPE)
         self.rec = np.zeros(n1, RECORD_DTYPE)

@@ -6,6 +6,7 @@ sequence; the FP32 image is additionally held to the reference's own image
 parity gate against the UNORM8 reference model and to <= 2/255 against the
 FP64 evaluation."""
 
+import math
 import os
 import subprocess
 
@@ -373,6 +374,53 @@ def test_raster_launch_shapes_do_not_change_pixels(oracle):
         ctx.set_raster_config(96, 0)
     with pytest.raises(ffi.GsplatError):
         ctx.set_raster_config(256, 33)
+
+
+def test_sort_interval_reuses_the_last_order(oracle):
+    """The reference's surface sort cadence: with interval 3 the depth order
+    is re-sorted on the 3rd camera change; frames in between draw the last
+    sorted order with their own projection, bit-exact against the oracle
+    given that stale order."""
+    scene, _, w, h = gsplat_scenes.config1(seed=21)
+    sv = oracle.SceneView(scene)
+    cams = [gsplat_scenes.camera((5.0 * math.sin(0.05 * k), 0.3, -5.0 * math.cos(0.05 * k)),
+                                 (0, 0, 0), 50.0) for k in range(6)]
+    ctx = _ctx(w, h)
+    ctx.set_debug_taps(True)
+    ctx.load_scene(scene)
+    ctx.set_sort_interval(3)
+    expect_sorted = [True, False, False, True, False, False]
+    stale = None
+    for k, cam in enumerate(cams):
+        ctx.set_camera(cam)
+        ctx.render_frame()
+        counts = ctx.frame_counts()
+        assert bool(counts.sort_refreshed) == expect_sorted[k], k
+        own = oracle.Frame(sv, cam, w, h)
+        if expect_sorted[k]:
+            stale = own.order
+        fr = oracle.Frame(sv, cam, w, h, order=stale)
+        assert np.array_equal(ctx.debug_order(), stale), k
+        assert counts.visible == own.visible  # depth-visible with this camera
+        tiles, ids = ctx.debug_tile_pairs()
+        assert np.array_equal(tiles, fr.pair_tiles) and np.array_equal(ids, fr.pair_ids), k
+        assert np.array_equal(ctx.readback_rgba8(), fr.raster_tiles_fp32()), k
+    # interval 1: an unchanged camera reuses the order and gives the same image
+    ctx.set_sort_interval(1)
+    ctx.set_camera(cams[2])
+    ctx.render_frame()
+    assert ctx.frame_counts().sort_refreshed == 1
+    img = ctx.readback_rgba8().copy()
+    ctx.render_frame()
+    assert ctx.frame_counts().sort_refreshed == 0
+    assert np.array_equal(ctx.readback_rgba8(), img)
+    # interval 0 (the context default): every frame sorts
+    ctx.set_sort_interval(0)
+    ctx.render_frame()
+    assert ctx.frame_counts().sort_refreshed == 1
+    ctx.render_frame()
+    assert ctx.frame_counts().sort_refreshed == 1
+    assert np.array_equal(ctx.readback_rgba8(), img)
 
 
 def test_benchmark_artifact_from_rendered_frames(tmp_path):
