@@ -93,7 +93,7 @@ constexpr uint32_t kMaxSetViews = 16;
 struct ViewCounters {
   uint32_t visible;  // depth-visible splats
   uint32_t drawn;    // splats with a raster record
-  uint32_t pairs;    // tile pairs the view emits (sum of its splats' tile-rect areas)
+  uint32_t pairs;    // tile pairs the view emits (its splats' exact row-span counts)
   uint32_t pad;
 };
 

@@ -379,7 +379,6 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
       z.flags = vis ? 1u : 0u;
       *dbg = z;
     }
-    uint32_t area = 0;  // tile pairs this splat will emit for the view
     bool drawn = false;
     if (vis) {
       Record rec;
@@ -387,7 +386,6 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
       drawn = project<kPlanes>(p, pa, ca, cb, col, rel, depth, rec, rect, dbg);
       b.rects[gid] = rect;
       if (drawn) b.records[gid] = rec;
-      area = ((rect.y & 0xffffu) - (rect.x & 0xffffu)) * ((rect.y >> 16) - (rect.x >> 16));
       // Digit histograms of the depth keys for every radix pass.
       if (!b.reuse_order) {
         const uint32_t key = ~__float_as_uint(fmaxf(depth, 0.0f));
@@ -399,13 +397,9 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
       b.rects[gid] = make_uint2(0u, 0u);
     }
     const uint32_t dmask = __ballot_sync(0xffffffffu, drawn);
-    area = warp_sum(area);
-    if (lane == 0) {
-      if (dmask) {
-        atomicAdd(&b.counters->drawn, __popc(dmask));
-        atomicAdd(&b.view_counters[view].drawn, __popc(dmask));
-      }
-      if (area) atomicAdd(&b.view_counters[view].pairs, area);
+    if (lane == 0 && dmask) {
+      atomicAdd(&b.counters->drawn, __popc(dmask));
+      atomicAdd(&b.view_counters[view].drawn, __popc(dmask));
     }
   }
 

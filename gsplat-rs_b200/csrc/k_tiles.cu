@@ -2,39 +2,104 @@
 // global over the views of a batch: views[v].tile_base + local tile.
 //
 // Emission walks the depth-sorted visible ids. Each block takes the next
-// 1024 sorted positions from an atomic ticket, sums their tile counts (area
-// of each splat's tile rect), and gets its global pair offset from a
-// decoupled look-back, so pairs land in exactly the order a sequential walk
-// would write them: depth order, then rect rows, then rect columns. The
-// block then writes its pairs cooperatively: each warp walks the pairs of
-// its 128 items 32 at a time, every lane finding its splat with a shuffle
-// search over the items' inclusive pair counts, so a splat covering thousands
-// of tiles is spread over the lanes. The digit histograms the tile sort needs
-// are accumulated while the pairs are written.
+// kEmitThreads * kEmitIpt sorted positions from an atomic ticket. A splat
+// covers, per row of its tile rect, only the span of columns its ellipse
+// reaches (tile_span.cuh), so the block first computes every row's span: each
+// warp walks the rows of its own items 32 at a time (a lane finds its item by
+// a 5-step shuffle search over the items' inclusive row counts), keeps the
+// spans in shared memory and adds their widths to the items' pair counts.
+// The block's total then gets its global pair offset from a decoupled
+// look-back, so pairs land in exactly the order a sequential walk would write
+// them: depth order, then rect rows, then the row's columns. Each warp then
+// walks the same row windows again and writes the window's pairs 32 at a
+// time (a lane finds its row by a second search over the rows' inclusive
+// widths), so a splat covering thousands of tiles is spread over the lanes.
+// The digit histograms the tile sort needs are accumulated while the pairs
+// are written, and the per-view pair counts per block.
 
 #include "device_common.cuh"
 #include "kernels.h"
+#include "tile_span.cuh"
 
 namespace gsr {
 namespace {
 
+// Sorted ids per thread (tuning knob).
+#ifndef GSR_EMIT_IPT
+#define GSR_EMIT_IPT 2
+#endif
+// Row spans each warp keeps between its two walks (tuning knob); rows past
+// them are computed again in the second walk.
+#ifndef GSR_EMIT_ROW_SLOTS
+#define GSR_EMIT_ROW_SLOTS 256
+#endif
 constexpr int kEmitThreads = 256;
-constexpr int kEmitIpt = 4;
+constexpr int kEmitIpt = GSR_EMIT_IPT;
 constexpr int kEmitItems = kEmitThreads * kEmitIpt;
 constexpr int kEmitWarps = kEmitThreads / 32;
+constexpr int kWarpItems = kEmitItems / kEmitWarps;
+constexpr uint32_t kRowSlots = GSR_EMIT_ROW_SLOTS;
+
+// Index of the first lane whose inclusive end exceeds x (31 when none does),
+// by a 5-step shuffle search over the warp's ascending inclusive ends.
+__device__ __forceinline__ uint32_t lane_search(uint32_t incl, uint32_t x) {
+  uint32_t c = 0;
+#pragma unroll
+  for (uint32_t step = 16; step >= 1; step >>= 1) {
+    const uint32_t v = __shfl_sync(0xffffffffu, incl, c + step - 1);
+    if (v <= x) c += step;
+  }
+  return c;
+}
+
+// One window of a warp's row walk: rows r .. round_end-1 of the items from
+// `it` on, one per lane. Both walks take the same windows.
+struct RowWindow {
+  uint32_t inc_w;      // inclusive row end of item it + lane (clamped to the warp's last)
+  uint32_t round_end;  // one past the window's last row
+  uint32_t item;       // the lane's item (valid when r + lane < round_end)
+  uint32_t row;        // the lane's row within its item
+};
+
+__device__ __forceinline__ RowWindow row_window(const uint32_t *s_rinc, uint32_t ib, uint32_t il,
+                                                uint32_t it, uint32_t r, uint32_t lane) {
+  RowWindow w;
+  w.inc_w = s_rinc[min(it + lane, il)];
+  const uint32_t win_start = it > ib ? s_rinc[it - 1] : 0u;
+  const uint32_t win_end = __shfl_sync(0xffffffffu, w.inc_w, 31);
+  w.round_end = min(r + 32u, win_end);
+  const uint32_t my = r + lane;
+  const uint32_t c = lane_search(w.inc_w, my);
+  const uint32_t prev = __shfl_sync(0xffffffffu, w.inc_w, c ? c - 1 : 0);
+  w.item = it + c;
+  w.row = my - (c ? prev : win_start);
+  return w;
+}
+
+// Span [c0, c1) of row `ty` of splat `id` with tile rect rc.
+__device__ __forceinline__ uint2 compute_row(const EmitBuffers &b, uint32_t id, uint2 rc,
+                                             uint32_t ty, float inv_tile) {
+  const Record *rec = &b.records[id];
+  const float4 ra = rec->a, rb = rec->b;
+  const SpanPre pre = span_pre(ra, rb);
+  return row_span(ra.x, ra.y, pre, ty, b.tile, inv_tile, rc.x & 0xffffu, rc.y & 0xffffu);
+}
 
 __global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b) {
-  __shared__ uint32_t s_incl[kEmitItems];
+  __shared__ uint32_t s_rinc[kEmitItems];  // inclusive row counts within the warp's items
+  __shared__ uint32_t s_cnt[kEmitItems];   // pair counts
   __shared__ uint32_t s_id[kEmitItems];
   __shared__ uint2 s_rect[kEmitItems];
   __shared__ uint16_t s_vi[kEmitItems];
-  __shared__ uint32_t s_wsum[kEmitThreads / 32];
+  __shared__ uint32_t s_span[kEmitWarps][kRowSlots];  // c0 | c1 << 16 per warp row
+  __shared__ uint32_t s_wsum[kEmitWarps];
   __shared__ uint32_t s_hist[3][256];
   __shared__ uint32_t s_block;
   __shared__ unsigned long long s_prefix;
-  // View table columns: splat base, tile base, tiles per row.
+  // View table columns: splat base, tile base, tiles per row; pairs per view.
   extern __shared__ uint32_t s_views[];
   uint32_t *s_vsb = s_views, *s_vtb = s_views + b.num_views, *s_vtx = s_views + 2 * b.num_views;
+  uint32_t *s_vpairs = s_views + 3 * b.num_views;
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_block = atomicAdd(&b.counters->emit_ticket, 1u);
   for (uint32_t k = tid; k < 3 * 256; k += kEmitThreads) (&s_hist[0][0])[k] = 0;
@@ -42,6 +107,7 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b) {
     s_vsb[v] = b.views[v].splat_base;
     s_vtb[v] = b.views[v].tile_base;
     s_vtx[v] = b.views[v].p.tiles_x;
+    s_vpairs[v] = 0;
   }
   __syncthreads();
   // The sorted visible ids: this frame's, or the order reused from the last
@@ -52,128 +118,167 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b) {
   if (start >= V) return;
   const uint32_t *ids = b.depth_plan->final_buffer == 0 ? b.ids0 : b.ids1;
 
-  uint32_t cnt[kEmitIpt];
-  uint32_t local = 0;
+  uint32_t rows[kEmitIpt];
+  uint32_t local_rows = 0;
 #pragma unroll
   for (int k = 0; k < kEmitIpt; ++k) {
-    uint32_t slot = tid * kEmitIpt + k;
-    uint32_t j = start + slot;
-    uint32_t id = 0, c = 0, vi = 0;
+    const uint32_t slot = tid * kEmitIpt + k;
+    const uint32_t j = start + slot;
+    uint32_t id = 0, h = 0, vi = 0;
     uint2 r = make_uint2(0u, 0u);
     if (j < V) {
       id = ids[j];
       r = b.rects[id];
-      uint32_t w = (r.y & 0xffffu) - (r.x & 0xffffu);
-      uint32_t h = (r.y >> 16) - (r.x >> 16);
-      c = w * h;
-      uint32_t lo = 0, hi = b.num_views - 1;
-      while (lo < hi) {
-        uint32_t mid = (lo + hi + 1) >> 1;
-        if (s_vsb[mid] <= id) lo = mid;
-        else hi = mid - 1;
+      if ((r.y & 0xffffu) > (r.x & 0xffffu) && (r.y >> 16) > (r.x >> 16)) {
+        h = (r.y >> 16) - (r.x >> 16);
+        vi = find_view(b.num_views, id, [&](uint32_t v) { return s_vsb[v]; });
       }
-      vi = lo;
     }
     s_id[slot] = id;
     s_rect[slot] = r;
     s_vi[slot] = (uint16_t)vi;
-    cnt[k] = c;
-    local += c;
+    s_cnt[slot] = 0;
+    rows[k] = h;
+    local_rows += h;
   }
-  // Block exclusive scan of the per-thread sums.
+  uint32_t rinc = local_rows;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, rinc, o);
+    if (lane >= (uint32_t)o) rinc += t;
+  }
+  uint32_t rrun = rinc - local_rows;
+#pragma unroll
+  for (int k = 0; k < kEmitIpt; ++k) {
+    rrun += rows[k];
+    s_rinc[tid * kEmitIpt + k] = rrun;
+  }
+  __syncwarp();
+
+  const uint32_t tile = b.tile;
+  const float inv_tile = __fdiv_rn(1.0f, (float)tile);
+  const uint32_t ib = warp * kWarpItems, il = ib + kWarpItems - 1;
+  const uint32_t rows_total = s_rinc[il];
+  // First walk: every row's span, kept for the second walk, summed per item.
+  for (uint32_t r = 0, it = ib; r < rows_total;) {
+    const RowWindow w = row_window(s_rinc, ib, il, it, r, lane);
+    const uint32_t my = r + lane;
+    if (my < w.round_end) {
+      const uint2 rc = s_rect[w.item];
+      const uint2 sp = compute_row(b, s_id[w.item], rc, (rc.x >> 16) + w.row, inv_tile);
+      if (my < kRowSlots) s_span[warp][my] = sp.x | (sp.y << 16);
+      if (sp.y > sp.x) atomicAdd(&s_cnt[w.item], sp.y - sp.x);
+    }
+    it += __popc(__ballot_sync(0xffffffffu, w.inc_w <= w.round_end));
+    r = w.round_end;
+  }
+  __syncwarp();
+
+  // Block exclusive scan of the per-thread pair sums.
+  uint32_t local = 0;
+#pragma unroll
+  for (int k = 0; k < kEmitIpt; ++k) {
+    const uint32_t slot = tid * kEmitIpt + k;
+    const uint32_t c = s_cnt[slot];
+    local += c;
+    if (c) atomicAdd(&s_vpairs[s_vi[slot]], c);
+  }
   uint32_t inc = local;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
     if (lane >= (uint32_t)o) inc += t;
   }
   if (lane == 31) s_wsum[warp] = inc;
   __syncthreads();
   uint32_t before = 0, total = 0;
 #pragma unroll
-  for (int w = 0; w < kEmitThreads / 32; ++w) {
-    uint32_t c = s_wsum[w];
+  for (int w = 0; w < kEmitWarps; ++w) {
+    const uint32_t c = s_wsum[w];
     before += (w < (int)warp) ? c : 0u;
     total += c;
   }
-  uint32_t run = before + inc - local;
-#pragma unroll
-  for (int k = 0; k < kEmitIpt; ++k) {
-    run += cnt[k];
-    s_incl[tid * kEmitIpt + k] = run;
-  }
   if (warp == 0) {
-    unsigned long long ex = lookback_warp(b.status, block, total, &b.counters->error);
+    const unsigned long long ex = lookback_warp(b.status, block, total, &b.counters->error);
     if (lane == 0) s_prefix = ex;
   }
   __syncthreads();
   const unsigned long long prefix = s_prefix;
   if (tid == 0 && block == (V - 1) / kEmitItems) {
-    unsigned long long all = prefix + total;
+    const unsigned long long all = prefix + total;
     b.counters->keys = all;
     b.counters->pairs = (uint32_t)(all < b.capacity ? all : b.capacity);
     if (all > b.capacity) b.counters->overflow = 1u;
   }
 
-  // Each warp writes the pairs of its own 128 items, 32 pairs per round. For
-  // pair `my` a lane finds its item by a 5-step shuffle search over the
-  // inclusive ends of a 32-item window starting at the round's first item.
-  const uint32_t ib = warp * (kEmitItems / kEmitWarps);
-  const uint32_t il = ib + kEmitItems / kEmitWarps - 1;
-  uint32_t k = ib ? s_incl[ib - 1] : 0u;
-  const uint32_t kend = s_incl[il];
-  uint32_t it = ib;
-  while (k < kend) {
-    const uint32_t inc_w = s_incl[min(it + lane, il)];
-    const uint32_t win_start = it ? s_incl[it - 1] : 0u;
-    const uint32_t win_end = __shfl_sync(0xffffffffu, inc_w, 31);
-    const uint32_t round_end = min(k + 32u, win_end);
-    const uint32_t my = k + lane;
-    uint32_t c = 0;
+  // Second walk: the pairs of each row window, 32 per round.
+  unsigned long long kpos = prefix + before;  // position of the warp's next pair
+  for (uint32_t r = 0, it = ib; r < rows_total;) {
+    const RowWindow w = row_window(s_rinc, ib, il, it, r, lane);
+    const uint32_t my = r + lane;
+    uint32_t c0 = 0, c1 = 0, row_tile = 0, id = 0;
+    if (my < w.round_end) {
+      const uint2 rc = s_rect[w.item];
+      const uint32_t ty = (rc.x >> 16) + w.row;
+      id = s_id[w.item];
+      if (my < kRowSlots) {
+        const uint32_t sp = s_span[warp][my];
+        c0 = sp & 0xffffu;
+        c1 = sp >> 16;
+      } else {
+        const uint2 sp = compute_row(b, id, rc, ty, inv_tile);
+        c0 = sp.x;
+        c1 = sp.y;
+      }
+      const uint32_t vi = s_vi[w.item];
+      row_tile = s_vtb[vi] + ty * s_vtx[vi] + c0;  // global id of the span's first tile
+    }
+    uint32_t winc = c1 - c0;
 #pragma unroll
-    for (uint32_t step = 16; step >= 1; step >>= 1) {
-      uint32_t v = __shfl_sync(0xffffffffu, inc_w, c + step - 1);
-      if (v <= my) c += step;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, winc, o);
+      if (lane >= (uint32_t)o) winc += t;
     }
-    const uint32_t prev = __shfl_sync(0xffffffffu, inc_w, c ? c - 1 : 0);
-    const unsigned long long g = prefix + my;
-    if (my < round_end && g < b.capacity) {
-      const uint32_t item = it + c;
-      const uint32_t off = my - (c ? prev : win_start);
-      const uint2 r = s_rect[item];
-      const uint32_t x0 = r.x & 0xffffu, y0 = r.x >> 16;
-      const uint32_t w = (r.y & 0xffffu) - x0;
-      uint32_t row = (uint32_t)((float)off * (1.0f / (float)w));
-      if (row * w > off) --row;
-      else if ((row + 1) * w <= off) ++row;
-      const uint32_t vi = s_vi[item];
-      const uint32_t tile = s_vtb[vi] + (y0 + row) * s_vtx[vi] + x0 + (off - row * w);
-      b.tile_keys[g] = tile;
-      b.tile_vals[g] = s_id[item];
-      atomicAdd(&s_hist[0][tile & 255u], 1u);
-      // The higher digits of a round's tiles are mostly equal: one add per
-      // distinct digit instead of up to 32 colliding ones.
-      const uint32_t act = __activemask();
-      const uint32_t lt = lanemask_lt();
-      if (b.tile_passes > 1) {
-        const uint32_t d1 = (tile >> 8) & 255u;
-        const uint32_t peers = __match_any_sync(act, d1);
-        if ((peers & lt) == 0) atomicAdd(&s_hist[1][d1], __popc(peers));
-      }
-      if (b.tile_passes > 2) {
-        const uint32_t d2 = (tile >> 16) & 255u;
-        const uint32_t peers = __match_any_sync(act, d2);
-        if ((peers & lt) == 0) atomicAdd(&s_hist[2][d2], __popc(peers));
+    const uint32_t W = __shfl_sync(0xffffffffu, winc, 31);
+    for (uint32_t q = 0; q < W; q += 32) {
+      const uint32_t myp = q + lane;
+      const uint32_t j = lane_search(winc, myp);
+      const uint32_t pj = __shfl_sync(0xffffffffu, winc, j ? j - 1 : 0);
+      const uint32_t tj = __shfl_sync(0xffffffffu, row_tile, j);
+      const uint32_t idj = __shfl_sync(0xffffffffu, id, j);
+      const unsigned long long g = kpos + myp;
+      if (myp < W && g < b.capacity) {
+        const uint32_t t = tj + myp - (j ? pj : 0u);
+        b.tile_keys[g] = t;
+        b.tile_vals[g] = idj;
+        atomicAdd(&s_hist[0][t & 255u], 1u);
+        // The higher digits of a round's tiles are mostly equal: one add per
+        // distinct digit instead of up to 32 colliding ones.
+        const uint32_t act = __activemask();
+        const uint32_t lt = lanemask_lt();
+        if (b.tile_passes > 1) {
+          const uint32_t d1 = (t >> 8) & 255u;
+          const uint32_t peers = __match_any_sync(act, d1);
+          if ((peers & lt) == 0) atomicAdd(&s_hist[1][d1], __popc(peers));
+        }
+        if (b.tile_passes > 2) {
+          const uint32_t d2 = (t >> 16) & 255u;
+          const uint32_t peers = __match_any_sync(act, d2);
+          if ((peers & lt) == 0) atomicAdd(&s_hist[2][d2], __popc(peers));
+        }
       }
     }
-    it += __popc(__ballot_sync(0xffffffffu, inc_w <= round_end));
-    k = round_end;
+    kpos += W;
+    it += __popc(__ballot_sync(0xffffffffu, w.inc_w <= w.round_end));
+    r = w.round_end;
   }
   __syncthreads();
   for (uint32_t q = tid; q < b.tile_passes * 256; q += kEmitThreads) {
-    uint32_t c = (&s_hist[0][0])[q];
-    if (c) atomicAdd(&b.tile_hist[q], c);
+    const uint32_t n = (&s_hist[0][0])[q];
+    if (n) atomicAdd(&b.tile_hist[q], n);
   }
+  for (uint32_t v = tid; v < b.num_views; v += kEmitThreads)
+    if (s_vpairs[v]) atomicAdd(&b.view_counters[v].pairs, s_vpairs[v]);
 }
 
 // Tile boundaries of the sorted keys: four keys per thread (one 16-byte
@@ -219,10 +324,18 @@ __global__ void fill_kernel(uint32_t *dst, uint32_t value, uint64_t count) {
 
 }  // namespace
 
+uint64_t emit_blocks(uint64_t splats) { return (splats + kEmitItems - 1) / kEmitItems; }
+
 void launch_emit(const EmitBuffers &b, cudaStream_t stream) {
-  uint32_t blocks = (b.n + kEmitItems - 1) / kEmitItems;
+  const uint32_t blocks = (uint32_t)emit_blocks(b.n);
   if (blocks == 0 || b.num_views == 0) return;
-  emit_kernel<<<blocks, kEmitThreads, 3 * 4 * b.num_views, stream>>>(b);
+  static const bool configured = [] {
+    cudaFuncSetAttribute(emit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(4 * 4 * kMaxViewsPerLaunch));
+    return true;
+  }();
+  (void)configured;
+  emit_kernel<<<blocks, kEmitThreads, 4 * 4 * b.num_views, stream>>>(b);
 }
 
 void launch_ranges(const SortPlan *tile_plan, const uint32_t *keys0, const uint32_t *keys1,

@@ -22,7 +22,7 @@ struct SortPlan;
 struct K1Buffers {
   uint32_t *vis_keys;          // [total splats] ~depth bits of visible splats, compacted
   uint32_t *vis_ids;           // [total splats] their gids, view-major then ascending id
-  uint2 *rects;                // [gid] tile rect per visible splat
+  uint2 *rects;                // [gid] tile rect per visible splat ((0, 0): none)
   Record *records;             // [gid] raster record per drawn splat
   unsigned long long *status;  // [total blocks] look-back words, zeroed
   FrameCounters *counters;
@@ -67,18 +67,22 @@ void launch_sort(const SortBuffers &b, cudaStream_t stream);
 struct EmitBuffers {
   const SortPlan *depth_plan;      // selects the buffer holding the sorted ids; n = their count
   const uint32_t *ids0, *ids1;     // depth-sorted gids, [visible]
-  const uint2 *rects;              // [gid]
+  const uint2 *rects;              // [gid] tile rects
+  const Record *records;           // [gid] raster records (row spans)
   uint32_t *tile_keys, *tile_vals; // [capacity] output pairs (global tile id, gid)
   uint64_t capacity;
-  unsigned long long *status;      // [ceil(total splats/1024)] look-back words, zeroed
+  unsigned long long *status;      // [emit_blocks(total splats)] look-back words, zeroed
   FrameCounters *counters;
+  ViewCounters *view_counters;     // [views] pairs per view are added here
   uint32_t *tile_hist;             // [passes][256] digit histograms of the tile ids, zeroed
   uint32_t tile_passes;
   uint32_t n;                      // total splats over the views (upper bound of visible)
   const ViewDev *views;
   uint32_t num_views;              // at most kMaxViewsPerLaunch
+  uint32_t tile;                   // tile size in pixels (8 or 16)
 };
 constexpr uint32_t kMaxViewsPerLaunch = 1024;
+uint64_t emit_blocks(uint64_t splats);  // emission blocks (look-back words) for `splats` ids
 void launch_emit(const EmitBuffers &b, cudaStream_t stream);
 
 // ---- tile ranges from the tile-sorted keys -------------------------------

@@ -121,9 +121,12 @@ uint64_t orc_build_instances(const OrcScene *scene, const float *alpha, const fl
                              uint32_t *out_index);
 
 /* ---- tile keys (the CUDA design's key contract) ---- */
-uint64_t orc_emit_tile_pairs(const OrcProjected *proj, const uint32_t *order, uint64_t v,
-                             uint32_t tiles_x, uint32_t *tile_out, uint32_t *id_out,
-                             uint64_t capacity);
+/* (tile, id) pairs in depth order; with `exact` each drawn splat covers, per
+ * row of its tile rect, only the columns its ellipse reaches (exact row
+ * spans, the CUDA design), else its whole tile rect. */
+uint64_t orc_emit_tile_pairs(const OrcProjected *proj, const OrcRecord *rec, const uint32_t *order,
+                             uint64_t v, uint32_t tiles_x, uint32_t tile, uint32_t exact,
+                             uint32_t *tile_out, uint32_t *id_out, uint64_t capacity);
 void orc_tile_lists(const uint32_t *tiles, const uint32_t *ids, uint64_t k, uint32_t num_tiles,
                     uint32_t *ranges, uint32_t *sorted_ids);
 void orc_sort_u64_pairs_stable(uint64_t *keys, uint32_t *values, uint64_t n);

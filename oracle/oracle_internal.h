@@ -93,6 +93,67 @@ inline bool pixel_weight(const OrcRecord &r, int px, int py, float &g, float &w)
   return w > (1.0f / 256.0f);
 }
 
+// Exact tile-row culling (the CUDA design's pair emission): for row ty of a
+// drawn splat's tile rect [x0, x1) x [y0, y1), the tile columns [c0, c1)
+// whose pixel centres the ellipse |local| <= s can reach. q(dx, dy) =
+// qa dx^2 + 2 qb dx dy + qc dy^2 is |local|^2 in pixel units; s^2 is widened
+// by a relative 1e-5 and an absolute 1e-6, far above the rounding of the
+// weight threshold (alpha * exp(-4.5 r2) > 1/256 holds only for r2 < s^2 up
+// to that rounding). The row's band is its pixel-centre rows +-0.5 px; within
+// it the ellipse's x-extent (at the band ends, or the leftmost/rightmost
+// point when it lies inside the band) +-0.5 px selects the columns. A
+// degenerate conic keeps the whole row. Every operation is a single IEEE f32
+// operation (no contraction), as on the device.
+struct SpanPre {
+  float qa, qb, qc, det, hx, hy, dy_left, s2a, inv_qa;
+  bool degenerate;
+};
+
+inline SpanPre span_pre(const OrcRecord &r) {
+  SpanPre p;
+  p.qa = std::fma(r.ax, r.ax, r.bx * r.bx);
+  p.qb = std::fma(r.ax, r.ay, r.bx * r.by);
+  p.qc = std::fma(r.ay, r.ay, r.by * r.by);
+  const float s2 = std::fma(r.s * r.s, 1.00001f, 1e-6f);
+  p.det = std::fma(p.qa, p.qc, -(p.qb * p.qb));
+  p.hx = std::sqrt(s2 * p.qc / p.det);
+  p.hy = std::sqrt(s2 * p.qa / p.det);
+  p.dy_left = p.qb * p.hx / p.qc;
+  p.s2a = s2 * p.qa;
+  p.inv_qa = 1.0f / p.qa;
+  p.degenerate = !(p.det > 0.0f) || !(p.hx < 3.0e38f) || !(p.hy < 3.0e38f);
+  return p;
+}
+
+// inv_tile = 1 / tile, exact (tile is 8 or 16).
+inline void row_span(const OrcRecord &r, const SpanPre &p, uint32_t ty, uint32_t tile,
+                     float inv_tile, uint32_t x0, uint32_t x1, uint32_t &c0, uint32_t &c1) {
+  c0 = x0;
+  c1 = x1;
+  if (p.degenerate) return;
+  const float lo = std::fmax((float)(ty * tile) - 0.5f - r.cy, -p.hy);
+  const float hi = std::fmin((float)(ty * tile + tile) - 0.5f - r.cy, p.hy);
+  if (!(lo <= hi)) {
+    c1 = x0;
+    return;
+  }
+  const float r_lo = std::sqrt(std::fmax(p.s2a - p.det * lo * lo, 0.0f));
+  const float r_hi = std::sqrt(std::fmax(p.s2a - p.det * hi * hi, 0.0f));
+  const float blo = -p.qb * lo, bhi = -p.qb * hi;
+  float xmin = std::fmin((blo - r_lo) * p.inv_qa, (bhi - r_hi) * p.inv_qa);
+  float xmax = std::fmax((blo + r_lo) * p.inv_qa, (bhi + r_hi) * p.inv_qa);
+  if (p.dy_left >= lo && p.dy_left <= hi) xmin = -p.hx;
+  if (-p.dy_left >= lo && -p.dy_left <= hi) xmax = p.hx;
+  const float f0 = std::fmax(std::floor((r.cx + xmin - 0.5f) * inv_tile), (float)x0);
+  const float f1 = std::fmin(std::floor((r.cx + xmax + 0.5f) * inv_tile) + 1.0f, (float)x1);
+  if (!(f0 < f1)) {
+    c1 = x0;
+    return;
+  }
+  c0 = (uint32_t)f0;
+  c1 = (uint32_t)f1;
+}
+
 }  // namespace orc
 
 #endif

@@ -99,8 +99,9 @@ def lib():
                                           ctypes.POINTER(OrcCamera), ctypes.c_uint32,
                                           ctypes.c_uint32, _u32p, ctypes.c_uint64, _f32p, _u32p]
         L.orc_build_instances.restype = ctypes.c_uint64
-        L.orc_emit_tile_pairs.argtypes = [ctypes.c_void_p, _u32p, ctypes.c_uint64, ctypes.c_uint32,
-                                          _u32p, _u32p, ctypes.c_uint64]
+        L.orc_emit_tile_pairs.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _u32p, ctypes.c_uint64,
+                                          ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u32p,
+                                          _u32p, ctypes.c_uint64]
         L.orc_emit_tile_pairs.restype = ctypes.c_uint64
         L.orc_tile_lists.argtypes = [_u32p, _u32p, ctypes.c_uint64, ctypes.c_uint32, _u32p, _u32p]
         L.orc_sort_u64_pairs_stable.argtypes = [_u64p, _u32p, ctypes.c_uint64]
@@ -230,10 +231,12 @@ def radix_count(values, shift, simd):
 class Frame:
     """Oracle evaluation of one SortedAlpha frame, stage by stage."""
 
-    def __init__(self, sv, cam, width, height, tile=16, order=None):
+    def __init__(self, sv, cam, width, height, tile=16, order=None, exact=True):
         """`order`: a back-to-front id list to draw instead of this camera's
         own (a stale order, as the reference's surface session draws between
-        sort refreshes); every splat is still projected with `cam`."""
+        sort refreshes); every splat is still projected with `cam`.
+        `exact`: tile pairs from exact row spans (the CUDA design) or, when
+        false, from whole tile rects."""
         L = lib()
         self.width, self.height, self.tile = width, height, tile
         self.params = frame_params(cam, width, height, tile, sv.degree)
@@ -253,12 +256,13 @@ class Frame:
         self.num_tiles = self.tiles_x * self.tiles_y
         v = len(self.order)
         order = np.ascontiguousarray(self.order, np.uint32) if v else np.zeros(1, np.uint32)
-        k = L.orc_emit_tile_pairs(self.proj.ctypes.data, _p(order, _u32p), v, self.tiles_x,
-                                  None, None, 0)
+        k = L.orc_emit_tile_pairs(self.proj.ctypes.data, self.rec.ctypes.data, _p(order, _u32p), v,
+                                  self.tiles_x, tile, int(exact), None, None, 0)
         self.pair_tiles = np.zeros(max(k, 1), np.uint32)
         self.pair_ids = np.zeros(max(k, 1), np.uint32)
-        L.orc_emit_tile_pairs(self.proj.ctypes.data, _p(order, _u32p), v, self.tiles_x,
-                              _p(self.pair_tiles, _u32p), _p(self.pair_ids, _u32p), k)
+        L.orc_emit_tile_pairs(self.proj.ctypes.data, self.rec.ctypes.data, _p(order, _u32p), v,
+                              self.tiles_x, tile, int(exact), _p(self.pair_tiles, _u32p),
+                              _p(self.pair_ids, _u32p), k)
         self.pair_tiles = self.pair_tiles[:k]
         self.pair_ids = self.pair_ids[:k]
         self.ranges = np.zeros(2 * self.num_tiles, np.uint32)

@@ -505,25 +505,31 @@ uint64_t orc_build_instances(const OrcScene *sc, const float *alpha, const float
 }
 
 // Tile-key contract of the CUDA design: walking the depth-sorted visible ids
-// in order, each drawn splat emits one (tile, id) pair per tile of its rect,
-// rows outer, columns inner. Returns the pair count (may exceed capacity;
-// only the first `capacity` pairs are written).
-uint64_t orc_emit_tile_pairs(const OrcProjected *proj, const uint32_t *order, uint64_t v,
-                             uint32_t tiles_x, uint32_t *tile_out, uint32_t *id_out,
-                             uint64_t capacity) {
+// in order, each drawn splat emits one (tile, id) pair per tile it covers,
+// rows outer, columns inner: per row of its tile rect the exact span
+// (orc::row_span), or with exact = 0 the whole rect. Returns the pair count
+// (may exceed capacity; only the first `capacity` pairs are written).
+uint64_t orc_emit_tile_pairs(const OrcProjected *proj, const OrcRecord *rec, const uint32_t *order,
+                             uint64_t v, uint32_t tiles_x, uint32_t tile, uint32_t exact,
+                             uint32_t *tile_out, uint32_t *id_out, uint64_t capacity) {
   uint64_t k = 0;
   for (uint64_t j = 0; j < v; ++j) {
     uint32_t s = order[j];
     const OrcProjected &p = proj[s];
-    if (!(p.flags & 2u)) continue;
-    for (uint32_t ty = p.tile_y0; ty < p.tile_y1; ++ty)
-      for (uint32_t tx = p.tile_x0; tx < p.tile_x1; ++tx) {
+    if (!(p.flags & 2u) || p.tile_x1 <= p.tile_x0 || p.tile_y1 <= p.tile_y0) continue;
+    const orc::SpanPre pre = orc::span_pre(rec[s]);
+    const float inv_tile = 1.0f / (float)tile;
+    for (uint32_t ty = p.tile_y0; ty < p.tile_y1; ++ty) {
+      uint32_t c0 = p.tile_x0, c1 = p.tile_x1;
+      if (exact) orc::row_span(rec[s], pre, ty, tile, inv_tile, p.tile_x0, p.tile_x1, c0, c1);
+      for (uint32_t tx = c0; tx < c1; ++tx) {
         if (k < capacity) {
           tile_out[k] = ty * tiles_x + tx;
           id_out[k] = s;
         }
         ++k;
       }
+    }
   }
   return k;
 }

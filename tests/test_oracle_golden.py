@@ -175,24 +175,19 @@ def test_wgsl_restatement_matches_cpu_builder(oracle):
 
 
 def test_two_stage_tile_order_equals_u64_key_sort(oracle):
+    """Emission in depth order then a stable sort by tile equals one stable
+    sort of 64-bit (tile, ~depth bits) keys emitted in id order."""
     scene, cam, w, h = gsplat_scenes.config1(seed=5)
     sv = oracle.SceneView(scene)
     fr = oracle.Frame(sv, cam, w, h)
-    # 64-bit keys emitted in id order, sorted stably ascending
-    keys, vals = [], []
-    for s in range(sv.n):
-        p = fr.proj[s]
-        if not (p["flags"] & 2):
-            continue
-        dbits = int(np.float32(max(p["depth"], 0.0)).view(np.uint32))
-        for ty in range(p["tile_y0"], p["tile_y1"]):
-            for tx in range(p["tile_x0"], p["tile_x1"]):
-                keys.append(((ty * fr.tiles_x + tx) << 32) | (~dbits & 0xFFFFFFFF))
-                vals.append(s)
-    keys = np.array(keys, np.uint64)
-    vals = np.array(vals, np.uint32)
+    # the emitted pairs, regrouped in id order (emission order within an id)
+    by_id = np.argsort(fr.pair_ids, kind="stable")
+    tiles = fr.pair_tiles[by_id].astype(np.uint64)
+    ids = fr.pair_ids[by_id]
+    dbits = np.maximum(fr.proj["depth"][ids], np.float32(0.0)).view(np.uint32)
+    keys = (tiles << np.uint64(32)) | (~dbits).astype(np.uint64)
     order = np.argsort(keys, kind="stable")
-    assert np.array_equal(vals[order], fr.tile_ids)
+    assert np.array_equal(ids[order], fr.tile_ids)
     assert np.array_equal((keys[order] >> np.uint64(32)).astype(np.uint32),
                           np.sort(fr.pair_tiles, kind="stable"))
 
