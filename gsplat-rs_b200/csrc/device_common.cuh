@@ -164,24 +164,16 @@ __device__ __forceinline__ float exp_neg(float x) {
   return __int_as_float(__float_as_int(p) + e * (1 << 23));
 }
 
-// e^(-4.5 r2) for r2 in [0, 1], the form the FP32 raster uses: the scale is
-// folded into one constant (-4.5 log2 e), the nearest integer n of
-// t = -4.5 log2(e) r2 is taken with the 1.5 * 2^23 shifter (no conversion
-// instructions), f = t - n in [-0.5, 0.5] feeds the same degree-6 Taylor
-// polynomial of 2^f, and 2^n is added to the exponent bits.
+// e^(-4.5 r2) for r2 in [0, 1], the FP32 raster's weight: one multiply by
+// -4.5 log2(e) and the hardware base-2 exponential (ex2.approx, a few ulp;
+// the argument lies in [-6.5, 0], so no subnormal is involved). The CPU
+// model of this raster evaluates 2^t with a degree-6 polynomial instead;
+// the two images agree to the last UNORM8 step except where a weight sits
+// on the 1/256 threshold or a channel on a rounding boundary.
 __device__ __forceinline__ float gauss_weight(float r2) {
-  const float kShift = 12582912.0f;
-  float t = r2 * -6.49212768f;
-  float tr = t + kShift;
-  float n = tr - kShift;
-  float f = t - n;
-  float p = fmaf(1.54035304e-4f, f, 1.33335581e-3f);
-  p = fmaf(p, f, 9.61812911e-3f);
-  p = fmaf(p, f, 5.55041087e-2f);
-  p = fmaf(p, f, 2.40226507e-1f);
-  p = fmaf(p, f, 6.93147181e-1f);
-  p = fmaf(p, f, 1.0f);
-  return __int_as_float(__float_as_int(p) + (__float_as_int(tr) << 23));
+  float g;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(g) : "f"(r2 * -6.49212768f));
+  return g;
 }
 
 __device__ __forceinline__ uint32_t to_unorm8(float x) {

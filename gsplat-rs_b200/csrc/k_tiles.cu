@@ -15,7 +15,9 @@
 // time (a lane finds its row by a second search over the rows' inclusive
 // widths), so a splat covering thousands of tiles is spread over the lanes.
 // The digit histograms the tile sort needs are accumulated while the pairs
-// are written, and the per-view pair counts per block.
+// are written.
+
+#include <algorithm>
 
 #include "device_common.cuh"
 #include "kernels.h"
@@ -24,9 +26,11 @@
 namespace gsr {
 namespace {
 
-// Sorted ids per thread (tuning knob).
-#ifndef GSR_EMIT_IPT
-#define GSR_EMIT_IPT 2
+// Sorted ids per thread: 2 up to GSR_EMIT_SMALL_IDS ids (more blocks in
+// flight for a single frame), 4 above (fewer blocks, each reading the view
+// table once) (tuning knob).
+#ifndef GSR_EMIT_SMALL_IDS
+#define GSR_EMIT_SMALL_IDS (1u << 21)
 #endif
 // Row spans each warp keeps between its two walks (tuning knob); rows past
 // them are computed again in the second walk.
@@ -34,11 +38,11 @@ namespace {
 #define GSR_EMIT_ROW_SLOTS 256
 #endif
 constexpr int kEmitThreads = 256;
-constexpr int kEmitIpt = GSR_EMIT_IPT;
-constexpr int kEmitItems = kEmitThreads * kEmitIpt;
 constexpr int kEmitWarps = kEmitThreads / 32;
-constexpr int kWarpItems = kEmitItems / kEmitWarps;
 constexpr uint32_t kRowSlots = GSR_EMIT_ROW_SLOTS;
+constexpr uint64_t kEmitSmallIds = GSR_EMIT_SMALL_IDS;
+
+inline uint32_t emit_ipt(uint64_t ids) { return ids <= kEmitSmallIds ? 2u : 4u; }
 
 // Index of the first lane whose inclusive end exceeds x (31 when none does),
 // by a 5-step shuffle search over the warp's ascending inclusive ends.
@@ -85,7 +89,10 @@ __device__ __forceinline__ uint2 compute_row(const EmitBuffers &b, uint32_t id, 
   return row_span(ra.x, ra.y, pre, ty, b.tile, inv_tile, rc.x & 0xffffu, rc.y & 0xffffu);
 }
 
+template <int kEmitIpt>
 __global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b) {
+  constexpr int kEmitItems = kEmitThreads * kEmitIpt;
+  constexpr int kWarpItems = kEmitItems / kEmitWarps;
   __shared__ uint32_t s_rinc[kEmitItems];  // inclusive row counts within the warp's items
   __shared__ uint32_t s_cnt[kEmitItems];   // pair counts
   __shared__ uint32_t s_id[kEmitItems];
@@ -96,10 +103,9 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b) {
   __shared__ uint32_t s_hist[3][256];
   __shared__ uint32_t s_block;
   __shared__ unsigned long long s_prefix;
-  // View table columns: splat base, tile base, tiles per row; pairs per view.
+  // View table columns: splat base, tile base, tiles per row.
   extern __shared__ uint32_t s_views[];
   uint32_t *s_vsb = s_views, *s_vtb = s_views + b.num_views, *s_vtx = s_views + 2 * b.num_views;
-  uint32_t *s_vpairs = s_views + 3 * b.num_views;
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_block = atomicAdd(&b.counters->emit_ticket, 1u);
   for (uint32_t k = tid; k < 3 * 256; k += kEmitThreads) (&s_hist[0][0])[k] = 0;
@@ -107,7 +113,6 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b) {
     s_vsb[v] = b.views[v].splat_base;
     s_vtb[v] = b.views[v].tile_base;
     s_vtx[v] = b.views[v].p.tiles_x;
-    s_vpairs[v] = 0;
   }
   __syncthreads();
   // The sorted visible ids: this frame's, or the order reused from the last
@@ -179,9 +184,7 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b) {
 #pragma unroll
   for (int k = 0; k < kEmitIpt; ++k) {
     const uint32_t slot = tid * kEmitIpt + k;
-    const uint32_t c = s_cnt[slot];
-    local += c;
-    if (c) atomicAdd(&s_vpairs[s_vi[slot]], c);
+    local += s_cnt[slot];
   }
   uint32_t inc = local;
 #pragma unroll
@@ -277,17 +280,36 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitBuffers b) {
     const uint32_t n = (&s_hist[0][0])[q];
     if (n) atomicAdd(&b.tile_hist[q], n);
   }
-  for (uint32_t v = tid; v < b.num_views; v += kEmitThreads)
-    if (s_vpairs[v]) atomicAdd(&b.view_counters[v].pairs, s_vpairs[v]);
+}
+
+// First position of a key >= t in the ascending keys[0, K).
+__device__ __forceinline__ uint32_t lower_bound(const uint32_t *keys, uint32_t K, uint32_t t) {
+  uint32_t lo = 0, hi = K;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (keys[mid] < t) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
 }
 
 // Tile boundaries of the sorted keys: four keys per thread (one 16-byte
-// load) plus the neighbour on each side.
+// load) plus the neighbour on each side. The first num_views threads also
+// count each view's pairs: its tiles are one contiguous id range, so its
+// pairs are one run of the sorted keys.
 __global__ void ranges_kernel(const SortPlan *__restrict__ plan, const uint32_t *k0,
                               const uint32_t *k1, const FrameCounters *__restrict__ counters,
-                              uint2 *__restrict__ ranges) {
+                              uint2 *__restrict__ ranges, const ViewDev *__restrict__ views,
+                              uint32_t num_views, ViewCounters *__restrict__ view_counters) {
   const uint32_t K = counters->pairs;
   const uint32_t *keys = plan->final_buffer == 0 ? k0 : k1;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid < num_views) {  // the first view starts at 0, the last ends at K
+    const uint32_t first = tid ? lower_bound(keys, K, views[tid].tile_base) : 0u;
+    const uint32_t end =
+        tid + 1 < num_views ? lower_bound(keys, K, views[tid + 1].tile_base) : K;
+    view_counters[tid].pairs = end - first;
+  }
   const uint32_t groups = (K + 3) / 4;
   for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < groups;
        q += gridDim.x * blockDim.x) {
@@ -324,26 +346,34 @@ __global__ void fill_kernel(uint32_t *dst, uint32_t value, uint64_t count) {
 
 }  // namespace
 
-uint64_t emit_blocks(uint64_t splats) { return (splats + kEmitItems - 1) / kEmitItems; }
+uint64_t emit_blocks(uint64_t ids) {
+  const uint64_t items = kEmitThreads * emit_ipt(ids);
+  return (ids + items - 1) / items;
+}
+
+uint64_t emit_status_words(uint64_t capacity) {
+  return std::max(emit_blocks(std::min(capacity, kEmitSmallIds)), emit_blocks(capacity));
+}
 
 void launch_emit(const EmitBuffers &b, cudaStream_t stream) {
   const uint32_t blocks = (uint32_t)emit_blocks(b.n);
   if (blocks == 0 || b.num_views == 0) return;
-  static const bool configured = [] {
-    cudaFuncSetAttribute(emit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(4 * 4 * kMaxViewsPerLaunch));
-    return true;
-  }();
-  (void)configured;
-  emit_kernel<<<blocks, kEmitThreads, 4 * 4 * b.num_views, stream>>>(b);
+  const size_t smem = 3 * 4 * b.num_views;
+  if (emit_ipt(b.n) == 2)
+    emit_kernel<2><<<blocks, kEmitThreads, smem, stream>>>(b);
+  else
+    emit_kernel<4><<<blocks, kEmitThreads, smem, stream>>>(b);
 }
 
 void launch_ranges(const SortPlan *tile_plan, const uint32_t *keys0, const uint32_t *keys1,
                    const FrameCounters *counters, uint32_t capacity, uint2 *ranges,
+                   const ViewDev *views, uint32_t num_views, ViewCounters *view_counters,
                    cudaStream_t stream) {
   uint32_t blocks = (capacity + 255) / 256;
   blocks = blocks < 148 * 8 ? (blocks ? blocks : 1) : 148 * 8;
-  ranges_kernel<<<blocks, 256, 0, stream>>>(tile_plan, keys0, keys1, counters, ranges);
+  blocks = std::max(blocks, (num_views + 255) / 256);
+  ranges_kernel<<<blocks, 256, 0, stream>>>(tile_plan, keys0, keys1, counters, ranges, views,
+                                            num_views, view_counters);
 }
 
 void launch_fill_u32(uint32_t *dst, uint32_t value, uint64_t count, cudaStream_t stream) {

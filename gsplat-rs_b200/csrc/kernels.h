@@ -71,9 +71,8 @@ struct EmitBuffers {
   const Record *records;           // [gid] raster records (row spans)
   uint32_t *tile_keys, *tile_vals; // [capacity] output pairs (global tile id, gid)
   uint64_t capacity;
-  unsigned long long *status;      // [emit_blocks(total splats)] look-back words, zeroed
+  unsigned long long *status;      // [emit_blocks(n)] look-back words, zeroed
   FrameCounters *counters;
-  ViewCounters *view_counters;     // [views] pairs per view are added here
   uint32_t *tile_hist;             // [passes][256] digit histograms of the tile ids, zeroed
   uint32_t tile_passes;
   uint32_t n;                      // total splats over the views (upper bound of visible)
@@ -82,12 +81,15 @@ struct EmitBuffers {
   uint32_t tile;                   // tile size in pixels (8 or 16)
 };
 constexpr uint32_t kMaxViewsPerLaunch = 1024;
-uint64_t emit_blocks(uint64_t splats);  // emission blocks (look-back words) for `splats` ids
+uint64_t emit_blocks(uint64_t ids);              // emission blocks (look-back words) for n ids
+uint64_t emit_status_words(uint64_t capacity);   // look-back words any n <= capacity needs
 void launch_emit(const EmitBuffers &b, cudaStream_t stream);
 
 // ---- tile ranges from the tile-sorted keys -------------------------------
+// Also writes each view's pair count (view_counters[v].pairs).
 void launch_ranges(const SortPlan *tile_plan, const uint32_t *keys0, const uint32_t *keys1,
                    const FrameCounters *counters, uint32_t capacity, uint2 *ranges,
+                   const ViewDev *views, uint32_t num_views, ViewCounters *view_counters,
                    cudaStream_t stream);
 
 // ---- K4: tile raster ------------------------------------------------------

@@ -217,7 +217,7 @@ void Pipeline::ensure_workspace(const Layout &l) {
     // view workspace: [view counters | K1 status | emit status] zeroed, then the table.
     const uint64_t k1_words = (ncap + 255) / 256 + 1;  // + views: blocks round up per set
     const uint64_t k1_total = k1_words + vcap;
-    const uint64_t emit_words = emit_blocks(ncap);
+    const uint64_t emit_words = emit_status_words(ncap);
     uint64_t off = 0;
     const uint64_t o_vc = off; off += align256(sizeof(ViewCounters) * vcap);
     const uint64_t o_k1 = off; off += align256(8 * k1_total);
@@ -347,10 +347,10 @@ void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &si
   }
   record(2);
 
-  EmitBuffers eb{depth_plan_, vis_vals0_,   vis_vals1_,    rects_,         records_,
-                 tile_keys0_, tile_vals0_,  key_cap_,      emit_status_,   counters_,
-                 view_counters_, tile_hist_, l.tile_passes, l.total_splats, views_dev_,
-                 l.views,     tile_};
+  EmitBuffers eb{depth_plan_, vis_vals0_,  vis_vals1_, rects_,        records_,
+                 tile_keys0_, tile_vals0_, key_cap_,   emit_status_,  counters_,
+                 tile_hist_,  l.tile_passes, l.total_splats, views_dev_, l.views,
+                 tile_};
   launch_emit(eb, stream_);
   if (debug_) {
     GSR_CUDA(cudaMemcpyAsync(debug_pairs_.as<uint32_t>(), tile_keys0_, 4 * key_cap_,
@@ -365,7 +365,7 @@ void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &si
   launch_sort(ts, stream_);
   record(4);
   launch_ranges(tile_plan_, tile_keys0_, tile_keys1_, counters_, (uint32_t)key_cap_, ranges_,
-                stream_);
+                views_dev_, l.views, view_counters_, stream_);
   record(5);
   RasterArgs ra{views_dev_, l.views,  l.total_tiles, ranges_,   tile_plan_,
                 tile_vals0_, tile_vals1_, records_,  images, counters_, sticky_};

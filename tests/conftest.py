@@ -2,6 +2,7 @@ import json
 import os
 import sys
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -43,3 +44,19 @@ def lcg_seq(seed, n, mul=1664525, inc=1013904223):
         s = (s * mul + inc) & 0xFFFFFFFF
         out.append(s)
     return out
+
+
+def assert_fp32_image(img, ref, label=""):
+    """The CUDA FP32 raster's RGBA8 image against the oracle's FP32 tile
+    model. The device takes 2^t from the hardware base-2 exponential, the
+    model from a degree-6 polynomial (both within a few 1e-7 of e^x), and
+    every other operation is the same, so the images differ only where a
+    weight sits on the 1/256 threshold or a channel on a rounding boundary:
+    at most 2 steps, on at most 1e-4 of the channels."""
+    img = np.asarray(img)
+    ref = np.asarray(ref)
+    assert img.shape == ref.shape, (label, img.shape, ref.shape)
+    d = np.abs(img.astype(np.int16) - ref.astype(np.int16))
+    assert int(d.max(initial=0)) <= 2, (label, int(d.max()))
+    changed = int(np.count_nonzero(d))
+    assert changed <= max(16, 1e-4 * d.size), (label, changed, d.size)

@@ -10,6 +10,7 @@ import pytest
 
 import gsplat_ffi as ffi
 import gsplat_scenes
+from conftest import assert_fp32_image
 
 pytestmark = pytest.mark.gpu
 
@@ -55,8 +56,10 @@ def _check_against_plain(batch, scenes, views, tile=16, blend=0, oracle=None):
         if oracle is not None and k < 3:
             fr = oracle.Frame(oracle.SceneView(scenes[sid]), cam, w, h, tile=tile)
             assert st.visible_count == fr.visible and st.tile_pairs == len(fr.pair_tiles)
-            ref = fr.raster_tiles_fp32() if blend == 0 else fr.raster_unorm8()
-            assert np.array_equal(img, ref), f"view {k} vs oracle"
+            if blend == 0:
+                assert_fp32_image(img, fr.raster_tiles_fp32(), f"view {k} vs oracle")
+            else:
+                assert np.array_equal(img, fr.raster_unorm8()), f"view {k} vs oracle"
 
 
 def test_batch_views_equal_plain_frames(oracle):

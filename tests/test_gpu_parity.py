@@ -1,10 +1,12 @@
 """GPU parity of the CUDA SortedAlpha path against the CPU oracle, through the
 C ABI. Integer and index work (visible order, tile pairs, tile ranges) must be
-bit-exact; the projected records and both compositing modes are also expected
-bit-exact because the kernels and the oracle run the same f32 operation
-sequence; the FP32 image is additionally held to the reference's own image
-parity gate against the UNORM8 reference model and to <= 2/255 against the
-FP64 evaluation."""
+bit-exact; the projected records and the UNORM8 compositing mode are also
+expected bit-exact because the kernels and the oracle run the same f32
+operation sequence. The FP32 image equals the oracle's FP32 tile model up to
+rare single steps (the raster's weight uses the hardware base-2 exponential,
+the model a polynomial), and is held to the reference's own image parity
+gate against the UNORM8 reference model and to <= 2/255 against the FP64
+evaluation."""
 
 import math
 import os
@@ -15,7 +17,7 @@ import pytest
 
 import gsplat_ffi as ffi
 import gsplat_scenes
-from conftest import GOLDEN, ROOT, lcg_seq
+from conftest import GOLDEN, ROOT, assert_fp32_image, lcg_seq
 
 pytestmark = pytest.mark.gpu
 
@@ -89,7 +91,7 @@ def test_frame_parity_stages_and_images(oracle, cfg):
     ctx = _render(scene, cam, w, h, blend=0)
     _compare_stages(ctx, fr, sv)
     img32 = ctx.readback_rgba8()
-    assert np.array_equal(img32, fr.raster_tiles_fp32()), "fp32 image vs restatement"
+    assert_fp32_image(img32, fr.raster_tiles_fp32(), "fp32 image vs restatement")
     ref8 = fr.raster_unorm8()
     ref64, _ = fr.raster_f64()
     m = _image_metrics(img32, ref8, ref64)
@@ -105,14 +107,15 @@ def test_frame_parity_stages_and_images(oracle, cfg):
 
 
 def test_full_config2_parity(oracle):
-    """279,199 splats, SH3, 1920x1080: every stage bit-exact at full size."""
+    """279,199 splats, SH3, 1920x1080: every stage bit-exact at full size (the
+    FP32 image within its tolerance)."""
     scene, cam, w, h = gsplat_scenes.config2()
     sv = oracle.SceneView(scene)
     fr = oracle.Frame(sv, cam, w, h)
     ctx = _render(scene, cam, w, h)
     _compare_stages(ctx, fr, sv)
     img = ctx.readback_rgba8()
-    assert np.array_equal(img, fr.raster_tiles_fp32())
+    assert_fp32_image(img, fr.raster_tiles_fp32())
     ref8 = fr.raster_unorm8()
     ref64, _ = fr.raster_f64()
     m = _image_metrics(img, ref8, ref64)
@@ -223,7 +226,7 @@ def test_sh_degrees(oracle, degree):
     fr = oracle.Frame(sv, cam, 400, 300)
     ctx = _render(scene, cam, 400, 300)
     _compare_stages(ctx, fr, sv)
-    assert np.array_equal(ctx.readback_rgba8(), fr.raster_tiles_fp32())
+    assert_fp32_image(ctx.readback_rgba8(), fr.raster_tiles_fp32())
 
 
 def test_edge_cases(oracle):
@@ -240,12 +243,12 @@ def test_edge_cases(oracle):
     ctx = _render(scene, back, w, h)
     fr = oracle.Frame(oracle.SceneView(scene), back, w, h)
     assert ctx.stats().visible_count == fr.visible
-    assert np.array_equal(ctx.readback_rgba8(), fr.raster_tiles_fp32())
+    assert_fp32_image(ctx.readback_rgba8(), fr.raster_tiles_fp32())
     # odd image sizes (partial edge tiles)
     for (w2, h2) in ((1, 1), (17, 33), (255, 1)):
         ctx = _render(scene, cam, w2, h2)
         fr = oracle.Frame(oracle.SceneView(scene), cam, w2, h2)
-        assert np.array_equal(ctx.readback_rgba8(), fr.raster_tiles_fp32()), (w2, h2)
+        assert_fp32_image(ctx.readback_rgba8(), fr.raster_tiles_fp32(), (w2, h2))
 
 
 def test_large_splats_grow_pair_buffers(oracle):
@@ -263,7 +266,7 @@ def test_large_splats_grow_pair_buffers(oracle):
     assert counts.tile_keys == len(fr.pair_tiles) > 16 * n
     assert counts.frame_reruns >= 1
     _compare_stages(ctx, fr, sv)
-    assert np.array_equal(ctx.readback_rgba8(), fr.raster_tiles_fp32())
+    assert_fp32_image(ctx.readback_rgba8(), fr.raster_tiles_fp32())
 
 
 def test_repeat_frames_are_identical_and_camera_errors():
@@ -295,7 +298,7 @@ def test_repeat_frames_are_identical_and_camera_errors():
 def test_cuda_graph_replay_matches_direct_launches(oracle):
     """Frames replayed from the captured CUDA graph (same layout, new camera
     each frame, synchronous and enqueued) equal frames issued launch by
-    launch and the oracle, bit for bit; phase timings stay available."""
+    launch bit for bit, and the oracle's; phase timings stay available."""
     scene, cam, w, h = gsplat_scenes.config1(seed=5)
     sv = oracle.SceneView(scene)
     rng = np.random.default_rng(11)
@@ -312,7 +315,7 @@ def test_cuda_graph_replay_matches_direct_launches(oracle):
         graph.render_frame()
         img = graph.readback_rgba8()
         assert np.array_equal(img, direct.readback_rgba8())
-        assert np.array_equal(img, oracle.Frame(sv, c, w, h).raster_tiles_fp32())
+        assert_fp32_image(img, oracle.Frame(sv, c, w, h).raster_tiles_fp32())
         t = graph.phase_times()
         assert all(v >= 0.0 for v in t.values()) and sum(t.values()) > 0.0
     for c in cams:
@@ -340,13 +343,13 @@ def test_smaller_scene_after_larger_reuses_workspace(oracle):
     ctx.render_frame()
     ctx.load_scene(small)
     ctx.render_frame()
-    assert np.array_equal(ctx.readback_rgba8(), ref)
+    assert_fp32_image(ctx.readback_rgba8(), ref)
     with ffi.Batch() as b:
         b.add_scene(big)
         b.add_scene(small)
         b.render([(0, cam, w, h)])
         b.render([(1, cam, w, h)])
-        assert np.array_equal(b.readback_rgba8(0), ref)
+        assert_fp32_image(b.readback_rgba8(0), ref)
 
 
 RASTER_SHAPES = [(16, c, b) for c in (256, 128, 64) for b in (0, 2, 4)] + \
@@ -355,17 +358,23 @@ RASTER_SHAPES = [(16, c, b) for c in (256, 128, 64) for b in (0, 2, 4)] + \
 
 def test_raster_launch_shapes_do_not_change_pixels(oracle):
     """Every tile size, chunk size and persistent-queue setting the autotuner
-    may pick gives the oracle's image bit for bit."""
+    may pick gives the same image bit for bit, within the FP32 tolerance of
+    the oracle's."""
     scene, cam, w, h = gsplat_scenes.config1(seed=12)
     ref = oracle.Frame(oracle.SceneView(scene), cam, w + 37, h + 5).raster_tiles_fp32()
     ctx = _ctx(w + 37, h + 5)
     ctx.load_scene(scene)
     ctx.set_camera(cam)
+    first = None
     for tile, chunk, bps in RASTER_SHAPES:
         ctx.set_tile_size(tile)
         ctx.set_raster_config(chunk, bps)
         ctx.render_frame()
-        assert np.array_equal(ctx.readback_rgba8(), ref), (tile, chunk, bps)
+        img = ctx.readback_rgba8()
+        if first is None:
+            first = img
+            assert_fp32_image(img, ref)
+        assert np.array_equal(img, first), (tile, chunk, bps)
     with pytest.raises(ffi.GsplatError) as e:
         ctx.set_raster_config(256, 0)  # tile size is 8 now
     assert e.value.code == ffi.INVALID_ARGUMENT
@@ -379,8 +388,8 @@ def test_raster_launch_shapes_do_not_change_pixels(oracle):
 def test_sort_interval_reuses_the_last_order(oracle):
     """The reference's surface sort cadence: with interval 3 the depth order
     is re-sorted on the 3rd camera change; frames in between draw the last
-    sorted order with their own projection, bit-exact against the oracle
-    given that stale order."""
+    sorted order with their own projection, equal to the oracle given that
+    stale order."""
     scene, _, w, h = gsplat_scenes.config1(seed=21)
     sv = oracle.SceneView(scene)
     cams = [gsplat_scenes.camera((5.0 * math.sin(0.05 * k), 0.3, -5.0 * math.cos(0.05 * k)),
@@ -404,7 +413,7 @@ def test_sort_interval_reuses_the_last_order(oracle):
         assert counts.visible == own.visible  # depth-visible with this camera
         tiles, ids = ctx.debug_tile_pairs()
         assert np.array_equal(tiles, fr.pair_tiles) and np.array_equal(ids, fr.pair_ids), k
-        assert np.array_equal(ctx.readback_rgba8(), fr.raster_tiles_fp32()), k
+        assert_fp32_image(ctx.readback_rgba8(), fr.raster_tiles_fp32(), k)
     # interval 1: an unchanged camera reuses the order and gives the same image
     ctx.set_sort_interval(1)
     ctx.set_camera(cams[2])
