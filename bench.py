@@ -487,6 +487,38 @@ def write_plain_artifact(args, ffi, ctx, scene, cams, out, w, h):
     bench_artifact.validate(args.artifact)
 
 
+def measure_ingest(ffi, splats=279_199, repeats=3):
+    """PLY ingestion: a synthetic SH3 scene written as a binary PLY and loaded
+    through gsplat_context_load_scene_path (body decoded on the device) and
+    through the host path (gsplat_ply_load, host precompute, upload). The
+    file is read once before timing (page cache warm); best of `repeats`."""
+    rng = np.random.default_rng(11)
+    scene = gsplat_scenes.make_scene(rng, gsplat_scenes.gmm_means(rng, splats), -4.5, 0.7, 0.5,
+                                     1.5, 3)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "scene.ply")
+        gsplat_scenes.write_ply(path, scene)
+        size = os.path.getsize(path)
+        with open(path, "rb") as f:
+            while f.read(64 << 20):
+                pass
+        dev, host = [], []
+        with ffi.Context(64, 64) as ctx:
+            for _ in range(repeats):
+                t0 = time.perf_counter()
+                ctx.load_scene_path(path)
+                dev.append(time.perf_counter() - t0)
+            for _ in range(repeats):
+                t0 = time.perf_counter()
+                ctx.load_scene(ffi.ply_load(path))
+                host.append(time.perf_counter() - t0)
+    return {"workload": f"binary PLY, {splats} splats, SH degree 3, page cache warm",
+            "file_bytes": size, "splats": splats,
+            "device_ms": min(dev) * 1e3, "host_ms": min(host) * 1e3,
+            "device_gbs": size / min(dev) / 1e9, "host_gbs": size / min(host) / 1e9,
+            "speedup": min(host) / min(dev)}
+
+
 def run_sections_only(args, ffi, torch):
     """The batched and/or served sections alone (no plain-frame line), for
     profiling those workloads by themselves."""
@@ -497,6 +529,8 @@ def run_sections_only(args, ffi, torch):
     if "served" in args.only:
         out["served"] = measure_served(ffi, [float(x) for x in args.serve_rates.split(",")],
                                        args.serve_seconds, 4000)
+    if "ingest" in args.only:
+        out["ingest"] = measure_ingest(ffi, args.ingest_splats)
     print(json.dumps(out), flush=True)
 
 
@@ -632,6 +666,8 @@ def run_cuda(args, world, rank, local):
     if not args.no_served and world == 1:
         line["served"] = measure_served(ffi, [float(x) for x in args.serve_rates.split(",")],
                                         args.serve_seconds, 4000)
+    if not args.no_ingest and world == 1:
+        line["ingest"] = measure_ingest(ffi, args.ingest_splats)
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:
@@ -655,8 +691,11 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=1.0)
     ap.add_argument("--artifact", default="",
                     help="also write the plain frames as a v1 benchmark artifact into this folder")
+    ap.add_argument("--no-ingest", action="store_true")
+    ap.add_argument("--ingest-splats", type=int, default=279_199,
+                    help="splats of the PLY ingestion workload")
     ap.add_argument("--only", default="",
-                    help="comma list of batched,served: run just those sections (profiling)")
+                    help="comma list of batched,served,ingest: run just those sections (profiling)")
     args = ap.parse_args()
     args.only = [x for x in args.only.split(",") if x]
     world, rank, local = dist_setup()

@@ -29,7 +29,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
               "-ffp-contract=off", "-I", CSRC, "-I", INCLUDE] + ARCH
-EXACT_FP = {"k_preprocess.cu", "k_raster.cu"}
+EXACT_FP = {"k_preprocess.cu", "k_raster.cu", "ply_device.cu"}
 CXX = os.environ.get("CXX", "g++")
 CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra",
              "-Wno-unused-parameter", "-I", CSRC, "-I", INCLUDE,

@@ -33,6 +33,10 @@ uint32_t SceneStore::add(const HostScene &s, cudaStream_t stream) {
   return insert(upload_scene(s, stream));
 }
 
+uint32_t SceneStore::add_path(const std::string &path, cudaStream_t stream) {
+  return insert(load_scene_file(path, stream, [this](uint64_t bytes) { check_budget(bytes); }));
+}
+
 uint32_t SceneStore::insert(std::unique_ptr<DeviceScene> sc) {
   check_budget(sc->bytes());
   bytes_ += sc->bytes();

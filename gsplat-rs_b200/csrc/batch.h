@@ -32,6 +32,9 @@ class SceneStore {
   uint32_t add(const HostScene &s, cudaStream_t stream);
   // Throws Unsupported if `bytes` more would exceed the budget.
   void check_budget(uint64_t bytes) const;
+  // Loads a PLY file (a binary body decoded on the device), budget checked
+  // before any allocation.
+  uint32_t add_path(const std::string &path, cudaStream_t stream);
   // Takes an uploaded scene (budget checked again).
   uint32_t insert(std::unique_ptr<DeviceScene> sc);
   const DeviceScene &get(uint32_t id) const;

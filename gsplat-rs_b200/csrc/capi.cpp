@@ -12,6 +12,7 @@
 #include "../../include/gsplat_cuda.h"
 #include "gsr_host.h"
 #include "autotune.h"
+#include "cuda_check.h"
 #include "batch.h"
 #include "renderer.h"
 #include "server.h"
@@ -190,8 +191,7 @@ int32_t gsplat_context_load_scene_path(GsplatContext *ctx, const char *path) {
     std::string p(path);
     if (!valid_utf8(p))
       return fail(Code::InvalidArgument, "gsplat_context_load_scene_path: path is not valid UTF-8");
-    gsr::HostScene s = gsr::load_ply(p);
-    ctx->renderer->load_scene(s);
+    ctx->renderer->load_scene_path(p);
     return ok();
   });
 }
@@ -476,6 +476,27 @@ int32_t gsplat_context_debug_order(GsplatContext *ctx, uint32_t *out, uint64_t c
   });
 }
 
+int32_t gsplat_context_debug_scene(GsplatContext *ctx, float *out, uint64_t capacity,
+                                   uint64_t *out_len) {
+  return guarded("gsplat_context_debug_scene", [&]() -> int32_t {
+    if (!ctx || !out_len) return fail(Code::InvalidArgument, "gsplat_context_debug_scene: null argument");
+    const gsr::DeviceScene *sc = ctx->renderer->scene();
+    if (!sc) return fail(Code::SceneNotLoaded, "gsplat_context_debug_scene: no scene loaded");
+    const uint64_t n = sc->n, planes = sc->dev.planes;
+    *out_len = 4 * n * (3 + planes);
+    if (!out || n == 0) return ok();
+    const float4 *src[4] = {sc->dev.pos_alpha, sc->dev.cov_a, sc->dev.cov_b, sc->dev.color};
+    const uint64_t count[4] = {n, n, n, n * planes};
+    uint64_t at = 0;
+    for (int k = 0; k < 4 && at < capacity; ++k) {
+      const uint64_t floats = std::min<uint64_t>(4 * count[k], capacity - at);
+      GSR_CUDA(cudaMemcpy(out + at, src[k], 4 * floats, cudaMemcpyDeviceToHost));
+      at += floats;
+    }
+    return ok();
+  });
+}
+
 int32_t gsplat_context_debug_projected(GsplatContext *ctx, GsplatProjectedSplat *out,
                                        uint64_t capacity, uint64_t *out_len) {
   return guarded("gsplat_context_debug_projected", [&]() -> int32_t {
@@ -651,8 +672,7 @@ int32_t gsplat_batch_add_scene_path(GsplatBatch *batch, const char *path, uint32
     std::string p(path);
     if (!valid_utf8(p))
       return fail(Code::InvalidArgument, "gsplat_batch_add_scene_path: path is not valid UTF-8");
-    gsr::HostScene s = gsr::load_ply(p);
-    *out_scene = batch->batch->scenes().add(s, batch->batch->stream());
+    *out_scene = batch->batch->scenes().add_path(p, batch->batch->stream());
     return ok();
   });
 }
@@ -838,7 +858,7 @@ int32_t gsplat_server_add_scene_path(GsplatServer *server, const char *path, uin
     std::string p(path);
     if (!valid_utf8(p))
       return fail(Code::InvalidArgument, "gsplat_server_add_scene_path: path is not valid UTF-8");
-    *out_scene = server->server->add_scene(gsr::load_ply(p));
+    *out_scene = server->server->add_scene_path(p);
     return ok();
   });
 }

@@ -243,22 +243,28 @@ static void mat3_mul(const float a[9], const float b[9], float out[9]) {
       out[3 * r + c] = a[3 * r + 0] * b[0 + c] + a[3 * r + 1] * b[3 + c] + a[3 * r + 2] * b[6 + c];
 }
 
+void splat_scalars(float opacity_logit, const float log_scale[3], float out[5]) {
+  // alpha: lib.rs:1251-1261
+  float a = 1.0f / (1.0f + std::exp(-opacity_logit));
+  a = std::fmin(std::fmax(a, 0.0f), 1.0f);
+  // alpha_extent_scale: splat_surface_direct.wgsl:74-77
+  float s2 = std::log(std::fmax(a, 1e-12f) * 256.0f) / 4.5f;
+  out[0] = a;
+  out[1] = std::sqrt(std::fmin(std::fmax(s2, 0.0f), 1.0f));
+  // axis scales of the world covariance: lib.rs:1654-1674
+  for (int k = 0; k < 3; ++k) out[2 + k] = std::fmax(std::exp(log_scale[k]), 1e-6f);
+}
+
 static void pack_range(const HostScene &s, ScenePacked &o, uint64_t begin, uint64_t end) {
   const uint64_t n = s.size();
   const uint32_t degree = s.sh_degree;
   const uint32_t per_channel = (degree + 1) * (degree + 1) - 1;
   const uint32_t planes = o.planes;
   for (uint64_t i = begin; i < end; ++i) {
-    // alpha: lib.rs:1251-1261
-    float a = 1.0f / (1.0f + std::exp(-s.opacity[i]));
-    a = std::fmin(std::fmax(a, 0.0f), 1.0f);
-    // alpha_extent_scale: splat_surface_direct.wgsl:74-77
-    float s2 = std::log(std::fmax(a, 1e-12f) * 256.0f) / 4.5f;
-    float ext = std::sqrt(std::fmin(std::fmax(s2, 0.0f), 1.0f));
+    float sc[5];
+    splat_scalars(s.opacity[i], &s.scale_xyz[3 * i], sc);
+    const float a = sc[0], ext = sc[1], sx = sc[2], sy = sc[3], sz = sc[4];
     // world covariance: lib.rs:1654-1674
-    float sx = std::fmax(std::exp(s.scale_xyz[3 * i + 0]), 1e-6f);
-    float sy = std::fmax(std::exp(s.scale_xyz[3 * i + 1]), 1e-6f);
-    float sz = std::fmax(std::exp(s.scale_xyz[3 * i + 2]), 1e-6f);
     float obj[9] = {sx * sx, 0.0f, 0.0f, 0.0f, sy * sy, 0.0f, 0.0f, 0.0f, sz * sz};
     float qn[4], rot[9], rt[9], tmp[9], w[9];
     quat_normalize(&s.rotation_xyzw[4 * i], qn);

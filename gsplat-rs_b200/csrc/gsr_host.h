@@ -51,6 +51,12 @@ inline uint32_t sh_rest_stride(uint32_t degree) { return 3u * ((degree + 1) * (d
 GsplatCamera camera_default();  // lib.rs:64-72
 GsplatConfig config_default();  // lib.rs:139-147
 
+// Load-time scalars of one splat with the reference's f32 expressions and
+// the C library's exp/log: alpha = clamp(sigmoid(opacity)), the extent scale
+// s (splat_surface_direct.wgsl:74-77) and max(exp(log_scale), 1e-6) per axis
+// (lib.rs:1251-1261, 1654-1674). out = {alpha, s, sx, sy, sz}.
+void splat_scalars(float opacity_logit, const float log_scale[3], float out[5]);
+
 // Quaternion helpers (crates/gsplat-render-wgpu/src/lib.rs:1374-1407).
 void quat_normalize(const float q[4], float out[4]);
 void quat_inverse(const float q[4], float out[4]);

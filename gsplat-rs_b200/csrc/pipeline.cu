@@ -45,41 +45,52 @@ uint32_t tile_sort_passes(uint32_t num_tiles) {
   return std::max(1u, (bits + 7) / 8);
 }
 
-uint64_t scene_device_bytes(const HostScene &s) {
-  const uint64_t n = std::max<uint64_t>(s.size(), 1);
-  return 3 * align256(16 * n) + align256(16 * n * color_planes(s.sh_degree));
+uint64_t scene_device_bytes(uint64_t splats, uint32_t sh_degree) {
+  const uint64_t n = std::max<uint64_t>(splats, 1);
+  return 3 * align256(16 * n) + align256(16 * n * color_planes(sh_degree));
 }
 
-std::unique_ptr<DeviceScene> upload_scene(const HostScene &s, cudaStream_t stream) {
-  const uint64_t n = s.size();
+uint64_t scene_device_bytes(const HostScene &s) { return scene_device_bytes(s.size(), s.sh_degree); }
+
+std::unique_ptr<DeviceScene> alloc_scene(uint64_t n, uint32_t sh_degree) {
   if (n > kMaxSortItems)
     throw Error(Code::Unsupported, "scene has more splats than the renderer supports (2^30 - 1)");
-  ScenePacked packed;
-  pack_scene(s, packed);
   auto sc = std::make_unique<DeviceScene>();
   sc->n = (uint32_t)n;
-  sc->sh_degree = s.sh_degree;
-  sc->positions = s.positions;
+  sc->sh_degree = sh_degree;
+  const uint32_t planes = color_planes(sh_degree);
   // Three geometry planes, then the colour planes as one tight region so
   // that plane p of splat i sits at color[p * n + i].
   const uint64_t plane = align256(16 * std::max<uint64_t>(n, 1));
-  const uint64_t color_bytes = align256(16 * std::max<uint64_t>(n, 1) * packed.planes);
-  sc->mem.reset(3 * plane + color_bytes);
+  sc->mem.reset(scene_device_bytes(n, sh_degree));
   char *base = sc->mem.as<char>();
-  if (n) {
-    GSR_CUDA(cudaMemcpyAsync(base, packed.pos_alpha.data(), 16 * n, cudaMemcpyHostToDevice, stream));
-    GSR_CUDA(cudaMemcpyAsync(base + plane, packed.cov_a.data(), 16 * n, cudaMemcpyHostToDevice, stream));
-    GSR_CUDA(cudaMemcpyAsync(base + 2 * plane, packed.cov_b.data(), 16 * n, cudaMemcpyHostToDevice, stream));
-    GSR_CUDA(cudaMemcpyAsync(base + 3 * plane, packed.color.data(), 16 * n * packed.planes,
-                             cudaMemcpyHostToDevice, stream));
-  }
-  GSR_CUDA(cudaStreamSynchronize(stream));
   sc->dev.pos_alpha = reinterpret_cast<const float4 *>(base);
   sc->dev.cov_a = reinterpret_cast<const float4 *>(base + plane);
   sc->dev.cov_b = reinterpret_cast<const float4 *>(base + 2 * plane);
   sc->dev.color = reinterpret_cast<const float4 *>(base + 3 * plane);
   sc->dev.n = (uint32_t)n;
-  sc->dev.planes = packed.planes;
+  sc->dev.planes = planes;
+  return sc;
+}
+
+std::unique_ptr<DeviceScene> upload_scene(const HostScene &s, cudaStream_t stream) {
+  const uint64_t n = s.size();
+  auto sc = alloc_scene(n, s.sh_degree);
+  ScenePacked packed;
+  pack_scene(s, packed);
+  sc->positions = s.positions;
+  if (n) {
+    const SceneDev &d = sc->dev;
+    GSR_CUDA(cudaMemcpyAsync((void *)d.pos_alpha, packed.pos_alpha.data(), 16 * n,
+                             cudaMemcpyHostToDevice, stream));
+    GSR_CUDA(cudaMemcpyAsync((void *)d.cov_a, packed.cov_a.data(), 16 * n, cudaMemcpyHostToDevice,
+                             stream));
+    GSR_CUDA(cudaMemcpyAsync((void *)d.cov_b, packed.cov_b.data(), 16 * n, cudaMemcpyHostToDevice,
+                             stream));
+    GSR_CUDA(cudaMemcpyAsync((void *)d.color, packed.color.data(), 16 * n * packed.planes,
+                             cudaMemcpyHostToDevice, stream));
+  }
+  GSR_CUDA(cudaStreamSynchronize(stream));
   return sc;
 }
 

@@ -4,7 +4,9 @@
 
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <functional>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "device_types.h"
@@ -42,9 +44,19 @@ struct DeviceScene {
   std::vector<float> positions;  // host copy for automatic camera framing
   uint64_t bytes() const { return mem.size(); }
 };
+// Allocates the planes of an n-splat scene (Unsupported above 2^30 - 1 splats).
+std::unique_ptr<DeviceScene> alloc_scene(uint64_t n, uint32_t sh_degree);
 std::unique_ptr<DeviceScene> upload_scene(const HostScene &s, cudaStream_t stream);
-// HBM bytes upload_scene allocates for `s`.
+// HBM bytes a scene's planes take.
+uint64_t scene_device_bytes(uint64_t splats, uint32_t sh_degree);
 uint64_t scene_device_bytes(const HostScene &s);
+// Loads a PLY file into HBM: a binary body is decoded on the device
+// (ply_device.cu), an ASCII one parsed on the host (load_ply) and uploaded.
+// `admit(bytes)` runs with the scene's HBM size before any allocation (a
+// budget check may throw). Same checks and error codes as load_ply; the
+// planes equal upload_scene(load_ply(path)) bit for bit.
+std::unique_ptr<DeviceScene> load_scene_file(const std::string &path, cudaStream_t stream,
+                                             const std::function<void(uint64_t)> &admit);
 
 // Device-timed phases of one run (CUDA events on the pipeline's stream).
 enum Phase : int { kPhasePreprocess, kPhaseDepthSort, kPhaseEmit, kPhaseTileSort, kPhaseRanges,

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "gsr_host.h"
+#include "ply.h"
 
 namespace gsr {
 namespace {
@@ -272,7 +273,124 @@ bool rot_layout_xyzw() {
   return e && (std::strcmp(e, "xyzw") == 0 || std::strcmp(e, "XYZW") == 0);
 }
 
+// What the body decode needs from a parsed header: the property index by
+// name (a later duplicate name overrides the earlier one, as a HashMap
+// insert does), the SH layout and the record layout of a binary body.
+struct Analysis {
+  std::map<std::string, size_t> idx;
+  std::vector<size_t> rest_props;
+  uint32_t degree = 0;
+  bool has_rest = false;
+  uint64_t rest_stride = 0;
+  std::vector<size_t> offsets;
+  size_t stride = 0;
+};
+
+Analysis analyze(const Header &h) {
+  Analysis a;
+  for (size_t k = 0; k < h.props.size(); ++k) a.idx.emplace(h.props[k].name, k);
+  static const char *kRequired[14] = {"x", "y", "z", "opacity", "scale_0", "scale_1", "scale_2",
+                                      "rot_0", "rot_1", "rot_2", "rot_3", "f_dc_0", "f_dc_1",
+                                      "f_dc_2"};
+  for (const char *r : kRequired)
+    if (!a.idx.count(r)) fail(Code::ParseFailed, std::string("missing required field `") + r + "`");
+  for (size_t k = 0; k < h.props.size(); ++k) a.idx[h.props[k].name] = k;
+  a.degree = infer_sh(h, a.rest_props);
+  a.has_rest = a.degree > 0 && !a.rest_props.empty();
+  a.rest_stride = a.has_rest ? sh_rest_stride(a.degree) : 0;
+  a.offsets.resize(h.props.size());
+  for (size_t k = 0; k < h.props.size(); ++k) {
+    a.offsets[k] = a.stride;
+    a.stride += ty_size(h.props[k].ty);
+  }
+  return a;
+}
+
+// lib.rs:376-404 (validate_body_before_allocation), binary bodies.
+void check_binary_body(uint64_t n, size_t stride, uint64_t body_len) {
+  if (stride != 0 && n > (uint64_t)-1 / stride)
+    fail(Code::Unsupported, "PLY resource size overflow while computing binary body bytes");
+  if (body_len < n * stride) fail(Code::ParseFailed, "vertex rows do not match declared vertex count");
+}
+
+// lib.rs:323-374 (allocate_scene): decoded bytes limit.
+void check_scene_bytes(uint64_t n, uint64_t rest_stride) {
+  uint64_t scene_bytes = n * (12 + 4 + 12 + 12 + 16) + n * rest_stride * 4;
+  limit("decoded scene bytes", scene_bytes, kMaxSceneBytes);
+}
+
+PlyType ply_type(Ty t) {
+  switch (t) {
+    case Ty::I8: return PlyType::I8;
+    case Ty::U8: return PlyType::U8;
+    case Ty::I16: return PlyType::I16;
+    case Ty::U16: return PlyType::U16;
+    case Ty::I32: return PlyType::I32;
+    case Ty::U32: return PlyType::U32;
+    case Ty::F32: return PlyType::F32;
+    case Ty::F64: return PlyType::F64;
+  }
+  return PlyType::F32;
+}
+
 }  // namespace
+
+bool ply_value_finite(float v) { return std::isfinite(v); }
+
+float ply_read_scalar(const unsigned char *p, PlyType t, bool big) {
+  static const Ty kTy[8] = {Ty::I8, Ty::U8, Ty::I16, Ty::U16, Ty::I32, Ty::U32, Ty::F32, Ty::F64};
+  return read_scalar(p, kTy[(int)t], big);
+}
+
+float ply_opacity_logit(float v) { return opacity_logit(v); }
+
+const float *ply_sh_flip() { return kShFlip; }
+
+// The checks of load_ply that precede the body decode, on the header alone
+// (the file's first bytes and its size).
+bool inspect_binary_ply(const std::string &path, PlyBinaryLayout &out) {
+  struct stat st;
+  if (::stat(path.c_str(), &st) != 0) fail(Code::NotFound, "I/O error while reading PLY");
+  limit("input bytes", (uint64_t)st.st_size, kMaxInputBytes);
+  std::ifstream f(path, std::ios::binary);
+  if (!f) fail(Code::NotFound, "I/O error while reading PLY");
+  const uint64_t file_size = (uint64_t)st.st_size;
+  std::vector<unsigned char> head((size_t)std::min<uint64_t>(file_size, kMaxHeaderBytes + 2));
+  f.read(reinterpret_cast<char *>(head.data()), (std::streamsize)head.size());
+  if (f.bad() || (uint64_t)f.gcount() != head.size()) fail(Code::NotFound, "I/O error while reading PLY");
+  size_t body_off = 0;
+  Header h = split_header(head, body_off);
+  Analysis a = analyze(h);
+  if (h.format == Fmt::Ascii) return false;
+  const uint64_t n = h.vertex_count;
+  check_binary_body(n, a.stride, file_size - body_off);
+  check_scene_bytes(n, a.rest_stride);
+  auto field = [&](const char *name) {
+    const size_t k = a.idx.at(name);
+    return PlyField{(uint32_t)a.offsets[k], ply_type(h.props[k].ty)};
+  };
+  out = PlyBinaryLayout{};
+  out.big_endian = h.format == Fmt::BinBE;
+  out.vertices = n;
+  out.stride = a.stride;
+  out.body_offset = body_off;
+  out.sh_degree = a.degree;
+  out.has_rest = a.has_rest;
+  out.rot_xyzw = rot_layout_xyzw();
+  const char *pos[3] = {"x", "y", "z"}, *scale[3] = {"scale_0", "scale_1", "scale_2"};
+  const char *rot[4] = {"rot_0", "rot_1", "rot_2", "rot_3"};
+  const char *dc[3] = {"f_dc_0", "f_dc_1", "f_dc_2"};
+  for (int k = 0; k < 3; ++k) {
+    out.pos[k] = field(pos[k]);
+    out.scale[k] = field(scale[k]);
+    out.dc[k] = field(dc[k]);
+  }
+  for (int k = 0; k < 4; ++k) out.rot[k] = field(rot[k]);
+  out.opacity = field("opacity");
+  if (a.has_rest)
+    for (size_t k : a.rest_props) out.rest.push_back({(uint32_t)a.offsets[k], ply_type(h.props[k].ty)});
+  return true;
+}
 
 // lib.rs:178-181, 199-288 (load_ply, parse_ply_bytes_with_limits)
 HostScene load_ply(const std::string &path) {
@@ -287,31 +405,18 @@ HostScene load_ply(const std::string &path) {
 
   size_t body_off = 0;
   Header h = split_header(in, body_off);
-  std::map<std::string, size_t> idx;
-  for (size_t k = 0; k < h.props.size(); ++k) idx.emplace(h.props[k].name, k);
-  static const char *kRequired[14] = {"x", "y", "z", "opacity", "scale_0", "scale_1", "scale_2",
-                                      "rot_0", "rot_1", "rot_2", "rot_3", "f_dc_0", "f_dc_1",
-                                      "f_dc_2"};
-  for (const char *r : kRequired)
-    if (!idx.count(r)) fail(Code::ParseFailed, std::string("missing required field `") + r + "`");
-  // A later duplicate property name overrides the earlier one (HashMap insert).
-  for (size_t k = 0; k < h.props.size(); ++k) idx[h.props[k].name] = k;
-
-  std::vector<size_t> rest_props;
-  uint32_t degree = infer_sh(h, rest_props);
-  bool has_rest = degree > 0 && !rest_props.empty();
-  uint64_t rest_stride = has_rest ? sh_rest_stride(degree) : 0;
+  Analysis an = analyze(h);
+  std::map<std::string, size_t> &idx = an.idx;
+  const std::vector<size_t> &rest_props = an.rest_props;
+  const uint32_t degree = an.degree;
+  const bool has_rest = an.has_rest;
+  const uint64_t rest_stride = an.rest_stride;
+  const std::vector<size_t> &offsets = an.offsets;
+  const size_t stride = an.stride;
   const uint64_t n = h.vertex_count;
   const unsigned char *body = in.data() + body_off;
   const size_t body_len = in.size() - body_off;
 
-  // lib.rs:376-404 (validate_body_before_allocation)
-  std::vector<size_t> offsets(h.props.size());
-  size_t stride = 0;
-  for (size_t k = 0; k < h.props.size(); ++k) {
-    offsets[k] = stride;
-    stride += ty_size(h.props[k].ty);
-  }
   std::vector<std::string> rows;
   if (h.format == Fmt::Ascii) {
     if (!valid_utf8(body, body_len))
@@ -328,13 +433,9 @@ HostScene load_ply(const std::string &path) {
     }
     if (rows.size() < n) fail(Code::ParseFailed, "vertex rows do not match declared vertex count");
   } else {
-    if (stride != 0 && n > (uint64_t)-1 / stride)
-      fail(Code::Unsupported, "PLY resource size overflow while computing binary body bytes");
-    if (body_len < n * stride) fail(Code::ParseFailed, "vertex rows do not match declared vertex count");
+    check_binary_body(n, stride, body_len);
   }
-  // lib.rs:323-374 (allocate_scene): decoded bytes limit.
-  uint64_t scene_bytes = n * (12 + 4 + 12 + 12 + 16) + n * rest_stride * 4;
-  limit("decoded scene bytes", scene_bytes, kMaxSceneBytes);
+  check_scene_bytes(n, rest_stride);
 
   HostScene s;
   s.sh_degree = degree;

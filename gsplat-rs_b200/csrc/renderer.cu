@@ -68,6 +68,16 @@ void Renderer::load_scene(const HostScene &s) {
   force_sort_ = true;
 }
 
+void Renderer::load_scene_path(const std::string &path) {
+  GSR_CUDA(cudaSetDevice(device_));
+  GSR_CUDA(cudaStreamSynchronize(stream_));
+  // The current scene stays loaded until the new one is complete.
+  std::unique_ptr<DeviceScene> sc = load_scene_file(path, stream_, {});
+  scene_ = std::move(sc);
+  has_frame_ = false;
+  force_sort_ = true;
+}
+
 void Renderer::ensure_image() {
   const uint64_t need = 4ull * width_ * height_;
   if (image_.size() < need || image_.size() > 2 * need) {

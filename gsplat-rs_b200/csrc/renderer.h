@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "pipeline.h"
@@ -43,6 +44,8 @@ class Renderer {
   uint32_t sort_interval() const { return sort_interval_; }
 
   void load_scene(const HostScene &s);
+  // PLY file; a binary body is decoded on the device (load_scene_file).
+  void load_scene_path(const std::string &path);
   bool has_scene() const { return scene_ != nullptr; }
   const DeviceScene *scene() const { return scene_.get(); }
 

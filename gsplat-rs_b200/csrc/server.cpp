@@ -103,6 +103,17 @@ uint32_t Server::add_scene(const HostScene &s) {
   return scenes_.insert(std::move(sc));
 }
 
+uint32_t Server::add_scene_path(const std::string &path) {
+  GSR_CUDA(cudaSetDevice(device_));
+  auto admit = [this](uint64_t bytes) {
+    std::lock_guard<std::mutex> g(mu_);
+    scenes_.check_budget(bytes);
+  };
+  auto sc = load_scene_file(path, upload_stream_, admit);
+  std::lock_guard<std::mutex> g(mu_);
+  return scenes_.insert(std::move(sc));
+}
+
 uint64_t Server::submit(const BatchView &v) {
   std::lock_guard<std::mutex> g(mu_);
   if (stop_) throw Error(Code::Internal, "server is stopping");

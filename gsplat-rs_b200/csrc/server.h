@@ -81,6 +81,7 @@ class Server {
   Server &operator=(const Server &) = delete;
 
   uint32_t add_scene(const HostScene &s);
+  uint32_t add_scene_path(const std::string &path);  // PLY, binary bodies decoded on the device
   // Thread-safe. Validates the view and queues it; returns its request id.
   uint64_t submit(const BatchView &v);
   RequestInfo poll(uint64_t id);

@@ -216,6 +216,8 @@ _SIGS = [
     ("gsplat_context_get_stream", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     ("gsplat_context_debug_order", ctypes.c_int32,
      [ctypes.c_void_p, _u32p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
+    ("gsplat_context_debug_scene", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
     ("gsplat_context_debug_projected", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
     ("gsplat_context_debug_tile_pairs", ctypes.c_int32,
@@ -448,6 +450,16 @@ class Context:
         check(lib().gsplat_context_debug_order(self.ptr, None, 0, ctypes.byref(n)))
         out = np.empty(max(n.value, 1), np.uint32)
         check(lib().gsplat_context_debug_order(self.ptr, out.ctypes.data_as(_u32p), n.value,
+                                               ctypes.byref(n)))
+        return out[:n.value]
+
+    def debug_scene(self):
+        """The resident scene planes as float32: pos_alpha (n, 4), cov_a (n, 4),
+        cov_b (n, 4) and the colour planes (planes, n, 4)."""
+        n = ctypes.c_uint64()
+        check(lib().gsplat_context_debug_scene(self.ptr, None, 0, ctypes.byref(n)))
+        out = np.zeros(max(n.value, 1), np.float32)
+        check(lib().gsplat_context_debug_scene(self.ptr, out.ctypes.data, n.value,
                                                ctypes.byref(n)))
         return out[:n.value]
 

@@ -194,6 +194,48 @@ def scene_from_json(obj):
     return scene
 
 
+# SH rest sign flips of the RDF <-> RUF reflection per coefficient (an
+# involution: the loader applies the same signs).
+_SH_FLIP = np.array([-1, 1, 1, -1, -1, 1, 1, 1, -1, -1, -1, 1, 1, 1, 1], np.float32)
+
+
+def write_ply(path, scene, big_endian=False):
+    """Writes a SceneBuffers-shaped dict (RUF) as a standard 3DGS binary PLY
+    (RDF, rot_0..3 = w x y z, f_rest_* channel-major), so that loading the
+    file gives back the same scene bit for bit: every conversion is a sign
+    flip or a permutation."""
+    pos = np.asarray(scene["positions"], np.float32).reshape(-1, 3)
+    n = pos.shape[0]
+    q = np.asarray(scene["rotation_xyzw"], np.float32).reshape(-1, 4)
+    degree = int(scene.get("sh_degree", 0))
+    per_channel = (degree + 1) ** 2 - 1
+    rest = scene.get("sh_rest")
+    cols = [("x", pos[:, 0]), ("y", -pos[:, 1]), ("z", pos[:, 2])]
+    dc = np.asarray(scene["color_dc"], np.float32).reshape(-1, 3)
+    cols += [(f"f_dc_{c}", dc[:, c]) for c in range(3)]
+    if degree > 0 and rest is not None:
+        r = np.asarray(rest, np.float32).reshape(n, 3, per_channel)
+        flip = np.ones(per_channel, np.float32)
+        flip[:min(15, per_channel)] = _SH_FLIP[:min(15, per_channel)]
+        r = r * flip
+        cols += [(f"f_rest_{ch * per_channel + k}", r[:, ch, k])
+                 for ch in range(3) for k in range(per_channel)]
+    cols += [("opacity", np.asarray(scene["opacity"], np.float32).reshape(-1))]
+    sc = np.asarray(scene["scale_xyz"], np.float32).reshape(-1, 3)
+    cols += [(f"scale_{k}", sc[:, k]) for k in range(3)]
+    cols += [("rot_0", q[:, 3]), ("rot_1", -q[:, 0]), ("rot_2", q[:, 1]), ("rot_3", -q[:, 2])]
+    order = ">" if big_endian else "<"
+    body = np.empty((n, len(cols)), np.dtype(order + "f4"))
+    for k, (_, v) in enumerate(cols):
+        body[:, k] = v
+    fmt = "binary_big_endian" if big_endian else "binary_little_endian"
+    head = f"ply\nformat {fmt} 1.0\nelement vertex {n}\n"
+    head += "".join(f"property float {name}\n" for name, _ in cols) + "end_header\n"
+    with open(path, "wb") as f:
+        f.write(head.encode())
+        f.write(body.tobytes())
+
+
 def default_camera():
     """gsplat_camera_default(): origin, identity rotation, fov 60, near 0.01, far 1000."""
     return {"position": [0.0, 0.0, 0.0], "rotation_xyzw": [0.0, 0.0, 0.0, 1.0],

@@ -157,6 +157,13 @@ int32_t gsplat_context_debug_tile_ranges(GsplatContext *ctx, uint32_t *ranges,
                                          uint64_t ranges_capacity, uint32_t *ids,
                                          uint64_t ids_capacity, uint64_t *out_keys);
 
+/* The loaded scene's resident planes as floats: pos_alpha (4n), cov_a (4n),
+ * cov_b (4n), then the colour planes (4 * planes * n); *out_len = total.
+ * No reference counterpart: lets tests compare the device PLY decode with
+ * the host load path bit for bit. */
+int32_t gsplat_context_debug_scene(GsplatContext *ctx, float *out, uint64_t capacity,
+                                   uint64_t *out_len);
+
 /* ---- standalone GPU sort (replaces gsplat-sort's CPU and GPU backends) ---- */
 
 /* CpuSortBackend::sort_values_by_keys (crates/gsplat-sort/src/lib.rs:36-61):
