@@ -519,6 +519,41 @@ def measure_ingest(ffi, splats=279_199, repeats=3):
             "speedup": min(host) / min(dev)}
 
 
+def measure_packed(ffi, torch, frames=60):
+    """The 1080p workload with its scene in the packed resident format (20-byte
+    hot record + 48-byte SH sidecar, decoded by the preprocess kernel) against
+    the plane format: per-phase device times (median over `frames`, L2 flushed
+    between frames), bytes per splat, and the image difference."""
+    scene, cam, w, h = gsplat_scenes.config2()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
+    out = {"workload": "1080p frame, 279,199 SH3 splats, scene in the plane vs the packed format",
+           "bytes_per_splat": {"planes": 240, "packed": 68}}
+    images = {}
+    for fmt in ("planes", "packed"):
+        with ffi.Context(w, h) as ctx:
+            (ctx.load_scene if fmt == "planes" else ctx.load_scene_packed)(scene)
+            ctx.set_camera(cam)
+            for _ in range(5):
+                ctx.render_frame()
+            stream = torch.cuda.ExternalStream(ctx.stream())
+            acc = {}
+            for i in range(frames):
+                with torch.cuda.stream(stream):
+                    flush.fill_(i)
+                ctx.render_frame()
+                for k, v in ctx.phase_times().items():
+                    acc.setdefault(k, []).append(v)
+            images[fmt] = ctx.readback_rgba8().astype(np.int32)
+            ph = {k: float(np.median(v)) for k, v in acc.items()}
+            out[fmt] = {"phases_ms": ph, "frame_ms": sum(ph.values())}
+    d = np.abs(images["planes"] - images["packed"])[..., :3] / 255.0
+    out["image_mean_abs_diff"] = float(d.mean())
+    out["image_frac_over_3"] = float((d > 3.0 / 255.0).any(axis=-1).mean())
+    out["preprocess_speedup"] = (out["planes"]["phases_ms"]["preprocess"] /
+                                 out["packed"]["phases_ms"]["preprocess"])
+    return out
+
+
 def run_sections_only(args, ffi, torch):
     """The batched and/or served sections alone (no plain-frame line), for
     profiling those workloads by themselves."""
@@ -531,6 +566,8 @@ def run_sections_only(args, ffi, torch):
                                        args.serve_seconds, 4000)
     if "ingest" in args.only:
         out["ingest"] = measure_ingest(ffi, args.ingest_splats)
+    if "packed" in args.only:
+        out["packed"] = measure_packed(ffi, torch)
     print(json.dumps(out), flush=True)
 
 
@@ -668,6 +705,8 @@ def run_cuda(args, world, rank, local):
                                         args.serve_seconds, 4000)
     if not args.no_ingest and world == 1:
         line["ingest"] = measure_ingest(ffi, args.ingest_splats)
+    if not args.no_packed and world == 1:
+        line["packed"] = measure_packed(ffi, torch)
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:
@@ -692,10 +731,11 @@ def main():
     ap.add_argument("--artifact", default="",
                     help="also write the plain frames as a v1 benchmark artifact into this folder")
     ap.add_argument("--no-ingest", action="store_true")
+    ap.add_argument("--no-packed", action="store_true")
     ap.add_argument("--ingest-splats", type=int, default=279_199,
                     help="splats of the PLY ingestion workload")
     ap.add_argument("--only", default="",
-                    help="comma list of batched,served,ingest: run just those sections (profiling)")
+                    help="comma list of batched,served,ingest,packed: run just those sections")
     args = ap.parse_args()
     args.only = [x for x in args.only.split(",") if x]
     world, rank, local = dist_setup()

@@ -33,6 +33,12 @@ uint32_t SceneStore::add(const HostScene &s, cudaStream_t stream) {
   return insert(upload_scene(s, stream));
 }
 
+uint32_t SceneStore::add_packed(const HostScene &s, cudaStream_t stream) {
+  if (scene_validate(s) != Code::Ok) throw Error(Code::InvalidArgument, "invalid scene buffers");
+  check_budget(packed_device_bytes(s.size(), s.sh_degree));
+  return insert(upload_scene_packed(s, stream));
+}
+
 uint32_t SceneStore::add_path(const std::string &path, cudaStream_t stream) {
   return insert(load_scene_file(path, stream, [this](uint64_t bytes) { check_budget(bytes); }));
 }

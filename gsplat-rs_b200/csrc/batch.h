@@ -32,6 +32,8 @@ class SceneStore {
   uint32_t add(const HostScene &s, cudaStream_t stream);
   // Throws Unsupported if `bytes` more would exceed the budget.
   void check_budget(uint64_t bytes) const;
+  // Uploads the scene in the packed resident format (SH degree <= 3).
+  uint32_t add_packed(const HostScene &s, cudaStream_t stream);
   // Loads a PLY file (a binary body decoded on the device), budget checked
   // before any allocation.
   uint32_t add_path(const std::string &path, cudaStream_t stream);

@@ -391,6 +391,16 @@ int32_t gsplat_context_load_scene_buffers(GsplatContext *ctx, const GsplatSceneD
   });
 }
 
+int32_t gsplat_context_load_scene_packed(GsplatContext *ctx, const GsplatSceneDesc *scene) {
+  return guarded("gsplat_context_load_scene_packed", [&]() -> int32_t {
+    if (!ctx || !scene)
+      return fail(Code::InvalidArgument, "gsplat_context_load_scene_packed: null argument");
+    gsr::HostScene s = host_scene_from_desc(*scene);
+    ctx->renderer->load_scene_packed(s);
+    return ok();
+  });
+}
+
 int32_t gsplat_context_readback_rgba8(GsplatContext *ctx, uint8_t *out, uint64_t out_len) {
   return guarded("gsplat_context_readback_rgba8", [&]() -> int32_t {
     if (!ctx || !out) return fail(Code::InvalidArgument, "gsplat_context_readback_rgba8: null argument");
@@ -482,6 +492,8 @@ int32_t gsplat_context_debug_scene(GsplatContext *ctx, float *out, uint64_t capa
     if (!ctx || !out_len) return fail(Code::InvalidArgument, "gsplat_context_debug_scene: null argument");
     const gsr::DeviceScene *sc = ctx->renderer->scene();
     if (!sc) return fail(Code::SceneNotLoaded, "gsplat_context_debug_scene: no scene loaded");
+    if (sc->dev.hot)
+      return fail(Code::InvalidArgument, "gsplat_context_debug_scene: scene is packed");
     const uint64_t n = sc->n, planes = sc->dev.planes;
     *out_len = 4 * n * (3 + planes);
     if (!out || n == 0) return ok();
@@ -493,6 +505,26 @@ int32_t gsplat_context_debug_scene(GsplatContext *ctx, float *out, uint64_t capa
       GSR_CUDA(cudaMemcpy(out + at, src[k], 4 * floats, cudaMemcpyDeviceToHost));
       at += floats;
     }
+    return ok();
+  });
+}
+
+int32_t gsplat_context_debug_packed_scene(GsplatContext *ctx, float *table, uint32_t *hot,
+                                          int8_t *sidecar, uint64_t *out_splats) {
+  return guarded("gsplat_context_debug_packed_scene", [&]() -> int32_t {
+    if (!ctx || !out_splats)
+      return fail(Code::InvalidArgument, "gsplat_context_debug_packed_scene: null argument");
+    const gsr::DeviceScene *sc = ctx->renderer->scene();
+    if (!sc) return fail(Code::SceneNotLoaded, "gsplat_context_debug_packed_scene: no scene loaded");
+    if (!sc->dev.hot)
+      return fail(Code::InvalidArgument, "gsplat_context_debug_packed_scene: scene is not packed");
+    const uint64_t n = sc->n;
+    *out_splats = n;
+    if (table)
+      GSR_CUDA(cudaMemcpy(table, sc->dev.packed, 4 * gsr::kPackedFloats, cudaMemcpyDeviceToHost));
+    if (hot && n) GSR_CUDA(cudaMemcpy(hot, sc->dev.hot, 20 * n, cudaMemcpyDeviceToHost));
+    if (sidecar && n && sc->dev.sidecar)
+      GSR_CUDA(cudaMemcpy(sidecar, sc->dev.sidecar, 48 * n, cudaMemcpyDeviceToHost));
     return ok();
   });
 }
@@ -660,6 +692,18 @@ int32_t gsplat_batch_add_scene_buffers(GsplatBatch *batch, const GsplatSceneDesc
       return fail(Code::InvalidArgument, "gsplat_batch_add_scene_buffers: null argument");
     gsr::HostScene s = host_scene_from_desc(*scene);
     *out_scene = batch->batch->scenes().add(s, batch->batch->stream());
+    return ok();
+  });
+}
+
+int32_t gsplat_batch_add_scene_packed(GsplatBatch *batch, const GsplatSceneDesc *scene,
+                                      uint32_t *out_scene) {
+  return guarded("gsplat_batch_add_scene_packed", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_add_scene_packed");
+    if (!scene || !out_scene)
+      return fail(Code::InvalidArgument, "gsplat_batch_add_scene_packed: null argument");
+    gsr::HostScene s = host_scene_from_desc(*scene);
+    *out_scene = batch->batch->scenes().add_packed(s, batch->batch->stream());
     return ok();
   });
 }
@@ -838,6 +882,18 @@ void gsplat_server_destroy(GsplatServer *server) {
 
 #define GSR_SERVER_CHECK(op) \
   if (!server || !server->server) return fail(Code::InvalidArgument, op ": server is null")
+
+int32_t gsplat_server_add_scene_packed(GsplatServer *server, const GsplatSceneDesc *scene,
+                                       uint32_t *out_scene) {
+  return guarded("gsplat_server_add_scene_packed", [&]() -> int32_t {
+    GSR_SERVER_CHECK("gsplat_server_add_scene_packed");
+    if (!scene || !out_scene)
+      return fail(Code::InvalidArgument, "gsplat_server_add_scene_packed: null argument");
+    gsr::HostScene s = host_scene_from_desc(*scene);
+    *out_scene = server->server->add_scene_packed(s);
+    return ok();
+  });
+}
 
 int32_t gsplat_server_add_scene_buffers(GsplatServer *server, const GsplatSceneDesc *scene,
                                         uint32_t *out_scene) {

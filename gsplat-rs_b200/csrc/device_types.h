@@ -14,6 +14,17 @@ namespace gsr {
 //   cov_a[i]     = (xx, xy, xz, yy)         world covariance
 //   cov_b[i]     = (yz, zz, extent_scale, 0)
 //   color[p*n+i] = floats 4p..4p+3 of (DC rgb, rest coefficient 1 rgb, ...)
+//
+// A packed scene (packed_atlas.rs: the 20-byte hot record, an i8 SH sidecar)
+// has no planes; the preprocess kernel decodes it into the same per-block
+// values instead:
+//   hot[5i .. 5i+4]  = u16 x, y | u16 z, u8 opacity | 3 x u10 log scale |
+//                      smallest-three quaternion | RGB10 baked colour
+//   sidecar[48i ..]  = 45 i8 rest coefficients (channel-major, 15 per channel)
+//   packed           = bounds min (3), span (3), log-scale min, extent, SH
+//                      scales (3), pad, then the 1,024 axis variances
+//                      exp(2 log_scale(u)) and the 256 extent scales
+// Both arrays are padded to whole 256-splat slices.
 struct SceneDev {
   const float4 *pos_alpha;
   const float4 *cov_a;
@@ -21,7 +32,14 @@ struct SceneDev {
   const float4 *color;
   uint32_t n;
   uint32_t planes;
+  const uint32_t *hot;     // packed scenes only (else null)
+  const int8_t *sidecar;   // packed scenes of SH degree >= 1
+  const float *packed;     // header and tables of a packed scene
 };
+constexpr uint32_t kPackedHeaderFloats = 12;
+constexpr uint32_t kPackedVarLut = 1024;
+constexpr uint32_t kPackedExtLut = 256;
+constexpr uint32_t kPackedFloats = kPackedHeaderFloats + kPackedVarLut + kPackedExtLut;
 
 // Pixel-space raster record of a drawn splat (48 bytes):
 //   a = (cx, cy, ax, ay)  centre in pixel-centre coordinates, first row of

@@ -254,6 +254,10 @@ __device__ __forceinline__ bool project(const FrameParams &p, const float4 &pa, 
 }
 
 constexpr int kK1Warps = kK1Threads / 32;
+constexpr uint32_t kPackedHotBytes = 20u * kK1Threads;   // one slice of hot records
+constexpr uint32_t kPackedSideBytes = 48u * kK1Threads;  // one slice of SH sidecars
+constexpr uint32_t kPackedTableBytes = 4u * kPackedFloats;  // header and tables
+static_assert(kPackedTableBytes % 16 == 0, "the table is one bulk copy");
 // Resident blocks per SM the register allocation must allow (tuning knob).
 #ifndef GSR_K1_MIN_BLOCKS
 #define GSR_K1_MIN_BLOCKS 3
@@ -269,6 +273,98 @@ struct K1Stage {
   float4 color[kPlanes][kK1Threads];
   uint64_t bar[2];  // [0]: positions, [1]: covariance and colour
 };
+
+// Decode of a packed splat into the thread's column of the stage, the values
+// a plane-format scene would hold there: position + alpha, the covariance
+// terms + extent scale, and the colour planes (the DC as (rgb10 - 0.5) / C0,
+// rest coefficients i8 / 127 * scale). Follows splat_surface_packed.wgsl:
+// 128-241 (position, opacity, smallest-three quaternion, rotation and
+// covariance from log scales); the axis variances exp(2 log_scale) and the
+// extent scales come from the scene's tables (computed on the host, staged
+// in shared memory with the slice).
+// x / d for the values the packed decode divides by a constant (integers in
+// [-127, 127], [0, 255], [0, 1023], [0, 65535] and the 1,024 RGB10 levels
+// less one half over C0): the product with RN(1/d) and one fma correction,
+// equal to the IEEE quotient for every such x (checked exhaustively by the
+// tests), three instructions instead of a division.
+__device__ __forceinline__ float div_const(float x, float d, float r) {
+  const float q = __fmul_rn(x, r);
+  return __fmaf_rn(__fmaf_rn(-q, d, x), r, q);
+}
+
+struct PackedIn {
+  uint32_t w[5];      // hot record
+  uint32_t side[12];  // SH sidecar (zero without one)
+  float h[11];        // bounds min, span, log-scale min, extent, SH scales
+  float var[3];       // the axis variances of the three scale codes
+  float ext;          // the extent scale of the opacity code
+};
+
+template <int kPlanes>
+__device__ __forceinline__ void decode_packed(uint32_t planes, const PackedIn &in,
+                                              K1Stage<kPlanes> &st) {
+  const uint32_t *w = in.w;
+  const uint32_t *side = in.side;
+  const float *h = in.h;
+  const uint32_t t = threadIdx.x;
+  const uint32_t pu[3] = {w[0] & 0xffffu, w[0] >> 16, w[1] & 0xffffu};
+  float pos[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+    pos[a] = h[a] + div_const((float)pu[a], 65535.0f, 1.0f / 65535.0f) * h[3 + a];
+  const uint32_t op = (w[1] >> 16) & 0xffu;
+  const float alpha = fminf(fmaxf(div_const((float)op, 255.0f, 1.0f / 255.0f), 1e-4f), 1.0f - 1e-4f);
+  st.pos[t] = make_float4(pos[0], pos[1], pos[2], alpha);
+  const float sx2 = in.var[0], sy2 = in.var[1], sz2 = in.var[2];
+  const uint32_t mi = w[3] & 3u;
+  const float inv_sqrt2 = 0.70710678118654752440f;
+  float c[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    c[k] = (div_const((float)((w[3] >> (2 + 10 * k)) & 0x3ffu), 1023.0f, 1.0f / 1023.0f) * 2.0f -
+            1.0f) * inv_sqrt2;
+  const float sum_sq = c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
+  const float dropped = sqrtf(fmaxf(1.0f - sum_sq, 0.0f));
+  float q[4];
+  q[0] = mi == 0 ? dropped : c[0];
+  q[1] = mi == 0 ? c[0] : (mi == 1 ? dropped : c[1]);
+  q[2] = mi <= 1 ? c[1] : (mi == 2 ? dropped : c[2]);
+  q[3] = mi <= 2 ? c[2] : dropped;
+  const float len = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  const float x = q[0] / len, y = q[1] / len, z = q[2] / len, ww = q[3] / len;
+  const float x2 = x + x, y2 = y + y, z2 = z + z;
+  const float xx = x * x2, yy = y * y2, zz = z * z2;
+  const float xy = x * y2, xz = x * z2, yz = y * z2;
+  const float wx = ww * x2, wy = ww * y2, wz = ww * z2;
+  const float r[9] = {1.0f - (yy + zz), xy - wz, xz + wy,
+                      xy + wz, 1.0f - (xx + zz), yz - wx,
+                      xz - wy, yz + wx, 1.0f - (xx + yy)};
+  auto term = [&](int a, int b) {
+    return sx2 * r[3 * a] * r[3 * b] + sy2 * r[3 * a + 1] * r[3 * b + 1] +
+           sz2 * r[3 * a + 2] * r[3 * b + 2];
+  };
+  st.cov_a[t] = make_float4(term(0, 0), term(0, 1), term(0, 2), term(1, 1));
+  st.cov_b[t] = make_float4(term(1, 2), term(2, 2), in.ext, 0.0f);
+  // Colour: float f = 3 c + ch is coefficient c (0 = DC) of channel ch.
+  const uint32_t pc = planes == 1 ? 0u : planes == 3 ? 3u : planes == 7 ? 8u : 15u;
+  auto coeff = [&](uint32_t f) {
+    constexpr float kC0 = 0.28209479177387814f;
+    if (f < 3) {
+      const float v = div_const((float)((w[4] >> (10 * f)) & 0x3ffu), 1023.0f, 1.0f / 1023.0f);
+      return div_const(v - 0.5f, kC0, 1.0f / kC0);
+    }
+    const uint32_t k = f / 3 - 1, ch = f % 3;
+    if (k >= pc) return 0.0f;
+    const uint32_t byte = ch * 15 + k;
+    const int8_t v = (int8_t)((side[byte >> 2] >> (8 * (byte & 3))) & 0xffu);
+    return div_const((float)v, 127.0f, 1.0f / 127.0f) * h[8 + ch];
+  };
+#pragma unroll
+  for (int pl = 0; pl < kPlanes; ++pl)
+    if ((uint32_t)pl < planes)
+      st.color[pl][t] = make_float4(coeff(4 * pl), coeff(4 * pl + 1), coeff(4 * pl + 2),
+                                    coeff(4 * pl + 3));
+}
 
 // One block covers 256 consecutive splats of one scene for every view of a
 // view set (up to kMaxSetViews views of that scene). One thread stages the
@@ -304,13 +400,26 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
     mbar_init(&st.bar[0], 1);
     mbar_init(&st.bar[1], 1);
     fence_barrier_init();
-    mbar_arrive_expect_tx(&st.bar[0], bytes);
-    bulk_copy_g2s(st.pos, sc0.pos_alpha + i0, bytes, &st.bar[0]);
-    mbar_arrive_expect_tx(&st.bar[1], bytes * (2u + sc0.planes));
-    bulk_copy_g2s(st.cov_a, sc0.cov_a + i0, bytes, &st.bar[1]);
-    bulk_copy_g2s(st.cov_b, sc0.cov_b + i0, bytes, &st.bar[1]);
-    for (uint32_t q = 0; q < sc0.planes && q < (uint32_t)kPlanes; ++q)
-      bulk_copy_g2s(st.color[q], sc0.color + (size_t)q * sc0.n + i0, bytes, &st.bar[1]);
+    if (sc0.hot) {
+      // Packed scene: the slice's hot records and SH sidecars (whole slices;
+      // the arrays are padded), staged at the start of the block's stage.
+      // The scene's header and tables follow them.
+      unsigned char *raw = reinterpret_cast<unsigned char *>(&st);
+      const uint32_t side = sc0.sidecar ? kPackedSideBytes : 0u;
+      mbar_arrive_expect_tx(&st.bar[0], kPackedHotBytes + kPackedTableBytes);
+      bulk_copy_g2s(raw, sc0.hot + (size_t)i0 * 5, kPackedHotBytes, &st.bar[0]);
+      bulk_copy_g2s(raw + kPackedHotBytes + side, sc0.packed, kPackedTableBytes, &st.bar[0]);
+      mbar_arrive_expect_tx(&st.bar[1], side);
+      if (side) bulk_copy_g2s(raw + kPackedHotBytes, sc0.sidecar + (size_t)i0 * 48, side, &st.bar[1]);
+    } else {
+      mbar_arrive_expect_tx(&st.bar[0], bytes);
+      bulk_copy_g2s(st.pos, sc0.pos_alpha + i0, bytes, &st.bar[0]);
+      mbar_arrive_expect_tx(&st.bar[1], bytes * (2u + sc0.planes));
+      bulk_copy_g2s(st.cov_a, sc0.cov_a + i0, bytes, &st.bar[1]);
+      bulk_copy_g2s(st.cov_b, sc0.cov_b + i0, bytes, &st.bar[1]);
+      for (uint32_t q = 0; q < sc0.planes && q < (uint32_t)kPlanes; ++q)
+        bulk_copy_g2s(st.color[q], sc0.color + (size_t)q * sc0.n + i0, bytes, &st.bar[1]);
+    }
   }
   for (uint32_t k = threadIdx.x; k < 4 * 256; k += kK1Threads) (&s_hist[0][0])[k] = 0;
   __syncthreads();
@@ -329,6 +438,32 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
   const SceneDev sc = views[set.first_view].sc;
   const uint32_t i = (block - set.block_base) * kK1Threads + threadIdx.x;
   const bool valid = i < sc.n;
+  if (sc.hot) {
+    // Every thread takes its packed record, the scene constants and its table
+    // entries into registers, then the block overwrites the stage with the
+    // decoded planes.
+    if (!mbar_wait(&st.bar[0], 0, &b.counters->error)) mbar_wait(&st.bar[0], 0, &b.counters->error);
+    if (!mbar_wait(&st.bar[1], 0, &b.counters->error)) mbar_wait(&st.bar[1], 0, &b.counters->error);
+    const uint32_t *raw = reinterpret_cast<const uint32_t *>(&st);
+    PackedIn in;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) in.w[k] = raw[5 * threadIdx.x + k];
+    const uint32_t side_words = sc.sidecar ? kPackedSideBytes / 4 : 0u;
+#pragma unroll
+    for (int k = 0; k < 12; ++k)
+      in.side[k] = side_words ? raw[kPackedHotBytes / 4 + 12 * threadIdx.x + k] : 0u;
+    const float *table = reinterpret_cast<const float *>(raw + kPackedHotBytes / 4 + side_words);
+#pragma unroll
+    for (int k = 0; k < 11; ++k) in.h[k] = table[k];
+    const float *var = table + kPackedHeaderFloats;
+    in.var[0] = var[in.w[2] & 0x3ffu];
+    in.var[1] = var[(in.w[2] >> 10) & 0x3ffu];
+    in.var[2] = var[(in.w[2] >> 20) & 0x3ffu];
+    in.ext = table[kPackedHeaderFloats + kPackedVarLut + ((in.w[1] >> 16) & 0xffu)];
+    __syncthreads();
+    decode_packed<kPlanes>(sc.planes, in, st);
+    __syncthreads();
+  }
   // A wait that expires leaves the error bit set (the frame reports an
   // internal error) after a second bounded wait for the copies in flight.
   if (!mbar_wait(&st.bar[0], 0, &b.counters->error)) mbar_wait(&st.bar[0], 0, &b.counters->error);

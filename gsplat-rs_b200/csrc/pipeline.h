@@ -44,6 +44,19 @@ struct DeviceScene {
   std::vector<float> positions;  // host copy for automatic camera framing
   uint64_t bytes() const { return mem.size(); }
 };
+// A scene encoded in the packed resident format (packed.cpp): hot words and
+// sidecar padded to whole 256-splat slices, and the header with its tables.
+struct PackedHost {
+  uint64_t n = 0;
+  uint32_t sh_degree = 0;
+  std::vector<uint32_t> hot;     // 5 words per slot
+  std::vector<int8_t> sidecar;   // 48 bytes per slot (SH degree >= 1)
+  std::vector<float> table;      // kPackedFloats
+};
+PackedHost pack_scene_packed(const HostScene &s);  // Unsupported above SH degree 3
+uint64_t packed_device_bytes(uint64_t n, uint32_t sh_degree);
+std::unique_ptr<DeviceScene> upload_scene_packed(const HostScene &s, cudaStream_t stream);
+
 // Allocates the planes of an n-splat scene (Unsupported above 2^30 - 1 splats).
 std::unique_ptr<DeviceScene> alloc_scene(uint64_t n, uint32_t sh_degree);
 std::unique_ptr<DeviceScene> upload_scene(const HostScene &s, cudaStream_t stream);

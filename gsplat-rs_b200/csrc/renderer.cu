@@ -68,6 +68,17 @@ void Renderer::load_scene(const HostScene &s) {
   force_sort_ = true;
 }
 
+void Renderer::load_scene_packed(const HostScene &s) {
+  Code c = scene_validate(s);
+  if (c != Code::Ok) throw Error(Code::InvalidArgument, "invalid scene buffers");
+  GSR_CUDA(cudaSetDevice(device_));
+  GSR_CUDA(cudaStreamSynchronize(stream_));
+  std::unique_ptr<DeviceScene> sc = upload_scene_packed(s, stream_);
+  scene_ = std::move(sc);
+  has_frame_ = false;
+  force_sort_ = true;
+}
+
 void Renderer::load_scene_path(const std::string &path) {
   GSR_CUDA(cudaSetDevice(device_));
   GSR_CUDA(cudaStreamSynchronize(stream_));

@@ -44,6 +44,8 @@ class Renderer {
   uint32_t sort_interval() const { return sort_interval_; }
 
   void load_scene(const HostScene &s);
+  // The scene in the packed resident format (68 bytes per SH3 splat; SH degree <= 3).
+  void load_scene_packed(const HostScene &s);
   // PLY file; a binary body is decoded on the device (load_scene_file).
   void load_scene_path(const std::string &path);
   bool has_scene() const { return scene_ != nullptr; }

@@ -103,6 +103,18 @@ uint32_t Server::add_scene(const HostScene &s) {
   return scenes_.insert(std::move(sc));
 }
 
+uint32_t Server::add_scene_packed(const HostScene &s) {
+  GSR_CUDA(cudaSetDevice(device_));
+  if (scene_validate(s) != Code::Ok) throw Error(Code::InvalidArgument, "invalid scene buffers");
+  {
+    std::lock_guard<std::mutex> g(mu_);
+    scenes_.check_budget(packed_device_bytes(s.size(), s.sh_degree));
+  }
+  auto sc = upload_scene_packed(s, upload_stream_);
+  std::lock_guard<std::mutex> g(mu_);
+  return scenes_.insert(std::move(sc));
+}
+
 uint32_t Server::add_scene_path(const std::string &path) {
   GSR_CUDA(cudaSetDevice(device_));
   auto admit = [this](uint64_t bytes) {

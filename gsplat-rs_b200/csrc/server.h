@@ -82,6 +82,7 @@ class Server {
 
   uint32_t add_scene(const HostScene &s);
   uint32_t add_scene_path(const std::string &path);  // PLY, binary bodies decoded on the device
+  uint32_t add_scene_packed(const HostScene &s);      // packed resident format, SH degree <= 3
   // Thread-safe. Validates the view and queues it; returns its request id.
   uint64_t submit(const BatchView &v);
   RequestInfo poll(uint64_t id);

@@ -218,6 +218,14 @@ _SIGS = [
      [ctypes.c_void_p, _u32p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
     ("gsplat_context_debug_scene", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
+    ("gsplat_context_debug_packed_scene", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.POINTER(ctypes.c_uint64)]),
+    ("gsplat_context_load_scene_packed", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p]),
+    ("gsplat_batch_add_scene_packed", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32)]),
+    ("gsplat_server_add_scene_packed", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32)]),
     ("gsplat_context_debug_projected", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
     ("gsplat_context_debug_tile_pairs", ctypes.c_int32,
@@ -406,6 +414,23 @@ class Context:
         sd = SceneDesc(scene)
         check(lib().gsplat_context_load_scene_buffers(self.ptr, ctypes.byref(sd.desc)))
 
+    def load_scene_packed(self, scene):
+        """The scene in the packed resident format (SH degree <= 3)."""
+        sd = SceneDesc(scene)
+        check(lib().gsplat_context_load_scene_packed(self.ptr, ctypes.byref(sd.desc)))
+
+    def debug_packed_scene(self):
+        """(table[1292] float32, hot (n, 5) uint32, sidecar (n, 48) int8 or None)."""
+        n = ctypes.c_uint64()
+        check(lib().gsplat_context_debug_packed_scene(self.ptr, None, None, None,
+                                                      ctypes.byref(n)))
+        table = np.zeros(1292, np.float32)
+        hot = np.zeros((max(n.value, 1), 5), np.uint32)
+        side = np.zeros((max(n.value, 1), 48), np.int8)
+        check(lib().gsplat_context_debug_packed_scene(self.ptr, table.ctypes.data, hot.ctypes.data,
+                                                      side.ctypes.data, ctypes.byref(n)))
+        return table, hot[:n.value], side[:n.value]
+
     def render_frame(self):
         check(lib().gsplat_context_render_frame(self.ptr))
 
@@ -527,6 +552,12 @@ class Batch:
         check(lib().gsplat_batch_add_scene_buffers(self.ptr, ctypes.byref(sd.desc), ctypes.byref(sid)))
         return sid.value
 
+    def add_scene_packed(self, scene):
+        sd = SceneDesc(scene)
+        sid = ctypes.c_uint32()
+        check(lib().gsplat_batch_add_scene_packed(self.ptr, ctypes.byref(sd.desc), ctypes.byref(sid)))
+        return sid.value
+
     def add_scene_path(self, path):
         sid = ctypes.c_uint32()
         check(lib().gsplat_batch_add_scene_path(self.ptr, os.fsencode(path), ctypes.byref(sid)))
@@ -628,6 +659,12 @@ class Server:
         sd = SceneDesc(scene)
         sid = ctypes.c_uint32()
         check(lib().gsplat_server_add_scene_buffers(self.ptr, ctypes.byref(sd.desc), ctypes.byref(sid)))
+        return sid.value
+
+    def add_scene_packed(self, scene):
+        sd = SceneDesc(scene)
+        sid = ctypes.c_uint32()
+        check(lib().gsplat_server_add_scene_packed(self.ptr, ctypes.byref(sd.desc), ctypes.byref(sid)))
         return sid.value
 
     def submit(self, scene, cam, width, height):

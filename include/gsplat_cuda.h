@@ -115,6 +115,15 @@ int32_t gsplat_context_set_sort_interval(GsplatContext *ctx, uint32_t interval);
  * crates/gsplat-core/src/lib.rs:224-276). Replaces any loaded scene. */
 int32_t gsplat_context_load_scene_buffers(GsplatContext *ctx, const GsplatSceneDesc *scene);
 
+/* Load a scene in the packed resident format of the reference's packed atlas
+ * (crates/gsplat-render-wgpu/src/packed_atlas.rs: 20-byte hot record of
+ * quantised position, opacity, log scales, rotation and baked colour, plus a
+ * 48-byte i8 SH sidecar): 68 instead of 240 bytes per SH3 splat, decoded per
+ * frame by the preprocess kernel. SH degree <= 3 (else UNSUPPORTED). No
+ * reference counterpart in the C ABI (the reference's packed path is a
+ * renderer-internal diagnostic). */
+int32_t gsplat_context_load_scene_packed(GsplatContext *ctx, const GsplatSceneDesc *scene);
+
 /* Copy the last frame's RGBA8 image (row 0 = top, tight rows of width*4
  * bytes) into `out`, which must hold width*height*4 bytes. Stands in for
  * Renderer::readback_rgba8 (lib.rs:779-795). */
@@ -157,6 +166,13 @@ int32_t gsplat_context_debug_tile_ranges(GsplatContext *ctx, uint32_t *ranges,
                                          uint64_t ranges_capacity, uint32_t *ids,
                                          uint64_t ids_capacity, uint64_t *out_keys);
 
+/* A packed scene's resident data: the header and tables (1,292 floats: bounds
+ * min and span, log-scale min and extent, SH scales, pad, 1,024 axis
+ * variances, 256 extent scales), the hot records (5 words per splat) and the
+ * SH sidecars (48 bytes per splat, when the degree is >= 1). Any output may be
+ * null; *out_splats = n. No reference counterpart. */
+int32_t gsplat_context_debug_packed_scene(GsplatContext *ctx, float *table, uint32_t *hot,
+                                          int8_t *sidecar, uint64_t *out_splats);
 /* The loaded scene's resident planes as floats: pos_alpha (4n), cov_a (4n),
  * cov_b (4n), then the colour planes (4 * planes * n); *out_len = total.
  * No reference counterpart: lets tests compare the device PLY decode with
@@ -240,6 +256,9 @@ int32_t gsplat_batch_set_scene_budget(GsplatBatch *batch, uint64_t bytes);
 int32_t gsplat_batch_add_scene_buffers(GsplatBatch *batch, const GsplatSceneDesc *scene,
                                        uint32_t *out_scene);
 int32_t gsplat_batch_add_scene_path(GsplatBatch *batch, const char *path, uint32_t *out_scene);
+/* As gsplat_batch_add_scene_buffers, stored in the packed resident format. */
+int32_t gsplat_batch_add_scene_packed(GsplatBatch *batch, const GsplatSceneDesc *scene,
+                                      uint32_t *out_scene);
 int32_t gsplat_batch_set_tile_size(GsplatBatch *batch, uint32_t tile);       /* 8 or 16 */
 int32_t gsplat_batch_set_blend_mode(GsplatBatch *batch, uint32_t mode);      /* GsplatBlendMode */
 /* Launch-group limits: views (1..1024), predicted tile pairs, splats and
@@ -345,6 +364,8 @@ void gsplat_server_destroy(GsplatServer *server);
 int32_t gsplat_server_add_scene_buffers(GsplatServer *server, const GsplatSceneDesc *scene,
                                         uint32_t *out_scene);
 int32_t gsplat_server_add_scene_path(GsplatServer *server, const char *path, uint32_t *out_scene);
+int32_t gsplat_server_add_scene_packed(GsplatServer *server, const GsplatSceneDesc *scene,
+                                       uint32_t *out_scene);
 /* Validates the view (scene id, camera, size) and queues it. */
 int32_t gsplat_server_submit(GsplatServer *server, const GsplatBatchView *view,
                              uint64_t *out_request);

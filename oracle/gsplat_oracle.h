@@ -96,6 +96,21 @@ void orc_frame_params(const OrcCamera *camera, uint32_t width, uint32_t height,
                       uint32_t tile, uint32_t sh_degree, OrcFrameParams *out);
 
 /* ---- load-time precompute ---- */
+/* ---- packed resident format (packed_atlas.rs; decode of the CUDA design) ---- */
+/* header[11]: bounds min (3), bounds span (3), log-scale min, log-scale
+ * extent, SH scales (3). hot: 5 words per splat; sidecar: 48 bytes per splat
+ * (or NULL). SH degree <= 3. */
+void orc_pack_scene(const OrcScene *sc, float *header, uint32_t *hot, int8_t *sidecar);
+/* The packed scene decoded to positions (3n), alpha (n), extent scale (n),
+ * covariance (6n), DC (3n) and rest coefficients (n*3*((d+1)^2-1)). */
+void orc_unpack_scene(uint64_t n, uint32_t sh_degree, const float *header, const uint32_t *hot,
+                      const int8_t *sidecar, float *positions, float *alpha, float *extent,
+                      float *cov6, float *color_dc, float *sh_rest);
+
+/* Test helper: dividends whose refined constant division (product with
+ * RN(1/d) and one fma correction) differs from the IEEE quotient. */
+uint64_t orc_const_div_mismatches(float d, const float *x, uint64_t n);
+
 void orc_precompute_alpha(const float *opacity, uint64_t n, float *alpha);
 void orc_precompute_extent_scale(const float *alpha, uint64_t n, float *s);
 void orc_precompute_cov(const float *scale_xyz, const float *rotation_xyzw, uint64_t n,

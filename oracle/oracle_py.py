@@ -81,6 +81,13 @@ def lib():
         L.orc_frame_params.argtypes = [ctypes.POINTER(OrcCamera), ctypes.c_uint32, ctypes.c_uint32,
                                        ctypes.c_uint32, ctypes.c_uint32,
                                        ctypes.POINTER(OrcFrameParams)]
+        L.orc_pack_scene.argtypes = [ctypes.c_void_p, _f32p, _u32p, ctypes.c_void_p]
+        L.orc_pack_scene.restype = None
+        L.orc_unpack_scene.argtypes = [ctypes.c_uint64, ctypes.c_uint32, _f32p, _u32p,
+                                       ctypes.c_void_p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p]
+        L.orc_unpack_scene.restype = None
+        L.orc_const_div_mismatches.argtypes = [ctypes.c_float, _f32p, ctypes.c_uint64]
+        L.orc_const_div_mismatches.restype = ctypes.c_uint64
         L.orc_precompute_alpha.argtypes = [_f32p, ctypes.c_uint64, _f32p]
         L.orc_precompute_extent_scale.argtypes = [_f32p, ctypes.c_uint64, _f32p]
         L.orc_precompute_cov.argtypes = [_f32p, _f32p, ctypes.c_uint64, _f32p]
@@ -173,6 +180,36 @@ class SceneView:
     def validate(self):
         rest_len = 0 if self.rest is None else self.rest.size
         return lib().orc_scene_validate(ctypes.byref(self.c), rest_len)
+
+
+class PackedSceneView(SceneView):
+    """A scene in the packed resident format (20-byte hot record + i8 SH
+    sidecar, packed_atlas.rs), decoded as the CUDA renderer decodes it: the
+    frame stages then see an ordinary scene with the decoded values."""
+
+    def __init__(self, scene):
+        super().__init__(scene)
+        if self.degree > 3:
+            raise ValueError("the packed format holds SH degree <= 3")
+        L = lib()
+        n1 = max(self.n, 1)
+        self.header = np.zeros(11, np.float32)
+        self.hot = np.zeros(5 * n1, np.uint32)
+        self.sidecar = np.zeros(48 * n1, np.int8)
+        L.orc_pack_scene(ctypes.byref(self.c), _p(self.header, _f32p), _p(self.hot, _u32p),
+                         self.sidecar.ctypes.data)
+        pc = (self.degree + 1) ** 2 - 1
+        self.pos = np.zeros(3 * n1, np.float32)
+        self.dc = np.zeros(3 * n1, np.float32)
+        self.rest = np.zeros(3 * pc * n1, np.float32) if pc else None
+        L.orc_unpack_scene(self.n, self.degree, _p(self.header, _f32p), _p(self.hot, _u32p),
+                           self.sidecar.ctypes.data, _p(self.pos, _f32p), _p(self.alpha, _f32p),
+                           _p(self.extent, _f32p), _p(self.cov, _f32p), _p(self.dc, _f32p),
+                           _p(self.rest, _f32p) if pc else None)
+        self.pos = self.pos[:3 * self.n]
+        self.c.positions = _p(self.pos, _f32p)
+        self.c.color_dc = _p(self.dc, _f32p)
+        self.c.sh_rest = _p(self.rest, _f32p) if pc else None
 
 
 def camera_validate(cam):
@@ -337,3 +374,8 @@ def render_reference_frame(sv, cam, width, height, threads=8, rows=0):
 
 def exp_neg(x):
     return lib().orc_exp_neg(float(x))
+
+
+def const_div_mismatches(d, x):
+    x = np.ascontiguousarray(x, np.float32)
+    return int(lib().orc_const_div_mismatches(float(d), _p(x, _f32p), x.size))
