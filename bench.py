@@ -11,8 +11,9 @@ value: frames/s with the scene resident in HBM, device time of K frames
   measured with CUDA events on the renderer's stream; L2 is flushed (a
   256 MiB write) between frames, outside the timed spans.
 e2e: the same frames through the public C ABI from host memory: camera upload,
-  gsplat_context_render_frame and an RGBA8 readback into pinned host memory
-  every step, host wall clock.
+  gsplat_context_render_frame_async and an asynchronous RGBA8 readback into
+  pinned host memory every step (the copy of one frame overlaps the render
+  of the next), host wall clock until the last image is on the host.
 --impl reference: the reference's SortedAlpha frame restated on the host CPU
   (depth preprocess and 8-bit LSD radix sort on one thread, vertex stage and
   UNORM8 blending on every host thread), on the same workload.
@@ -634,9 +635,12 @@ def run_cuda(args, world, rank, local):
     ms_per_frame = device_ms / args.steps
     value = world * args.steps / (device_ms / 1000.0)
 
-    # End to end through the C ABI: camera in, frame, RGBA8 readback to pinned memory.
-    pinned = torch.empty(w * h * 4, dtype=torch.uint8, pin_memory=True)
-    out = pinned.numpy()
+    # End to end through the C ABI: camera in, frame, RGBA8 readback to pinned
+    # memory every step. Frames are enqueued back to back and each image is
+    # read back asynchronously while the next frame renders (two device images
+    # alternate), into two pinned host buffers in turn.
+    pinned = [torch.empty(w * h * 4, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+    outs = [p.numpy() for p in pinned]
     cams = []
     rng = np.random.default_rng(5)
     for i in range(args.steps):
@@ -648,9 +652,11 @@ def run_cuda(args, world, rank, local):
     t0 = time.perf_counter()
     for i in range(args.steps):
         ctx.set_camera(cams[i])
-        ctx.render_frame()
-        ctx.readback_rgba8(out)
+        ctx.render_frame_async()
+        ctx.readback_rgba8_async(outs[i % 2])
+    ctx.sync()
     e2e_s = time.perf_counter() - t0
+    out = outs[(args.steps - 1) % 2]
     if world > 1:
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)

@@ -409,6 +409,15 @@ int32_t gsplat_context_readback_rgba8(GsplatContext *ctx, uint8_t *out, uint64_t
   });
 }
 
+int32_t gsplat_context_readback_rgba8_async(GsplatContext *ctx, uint8_t *out, uint64_t out_len) {
+  return guarded("gsplat_context_readback_rgba8_async", [&]() -> int32_t {
+    if (!ctx || !out)
+      return fail(Code::InvalidArgument, "gsplat_context_readback_rgba8_async: null argument");
+    ctx->renderer->readback_rgba8_async(out, out_len);
+    return ok();
+  });
+}
+
 int32_t gsplat_context_get_frame_counts(const GsplatContext *ctx, GsplatFrameCounts *out) {
   return guarded("gsplat_context_get_frame_counts", [&]() -> int32_t {
     if (!ctx || !out) return fail(Code::InvalidArgument, "gsplat_context_get_frame_counts: null argument");

@@ -342,7 +342,7 @@ void launch_sort(const SortBuffers &b, cudaStream_t stream) {
   uint32_t *hist = b.work + 64;
   uint32_t *status = b.work + 64 + 4 * 256;
   // tickets and histograms; the status words are zeroed by the plan kernel
-  cudaMemsetAsync(b.work, 0, (64 + 4 * 256) * sizeof(uint32_t), stream);
+  if (!b.scratch_zeroed) cudaMemsetAsync(b.work, 0, kSortScratchHeadWords * sizeof(uint32_t), stream);
   const uint32_t grid = tiles ? tiles : 1;
   if (!b.hist) {
     if (ipt == 8)

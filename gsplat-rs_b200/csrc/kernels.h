@@ -57,7 +57,10 @@ struct SortBuffers {
   // Digit histograms [passes][256] already accumulated by the producer of
   // the keys (then no histogram kernel runs), or null.
   const uint32_t *hist;
+  // The scratch's tickets and histograms are already zero (else one memset).
+  bool scratch_zeroed = false;
 };
+constexpr uint32_t kSortScratchHeadWords = 64 + 4 * 256;  // tickets and histograms
 uint64_t sort_work_words(uint32_t capacity, uint32_t passes);
 // Zeroes the scratch (one memset) and launches the histogram (unless given),
 // plan and pass kernels on `stream`.
@@ -121,6 +124,21 @@ struct RasterConfig {
 bool raster_config_valid(uint32_t tile, const RasterConfig &cfg);
 void launch_raster(const RasterArgs &a, uint32_t tile, uint32_t blend_mode,
                    const RasterConfig &cfg, uint32_t sm_count, cudaStream_t stream);
+
+// ---- run start and end ----------------------------------------------------
+// A run issues no copy-engine work and reads no host memory, so a caller's
+// own host<->device copies (an image readback while the next frame renders)
+// never stall it: one kernel zeroes the run's scratch, and when the run has
+// host sinks another writes the counters there.
+constexpr int kRunZeroRegions = 5;
+struct RunInit {
+  uint32_t *zero[kRunZeroRegions];       // regions zeroed at the start of a run
+  uint64_t zero_words[kRunZeroRegions];
+};
+void launch_run_init(const RunInit &a, cudaStream_t stream);
+void launch_run_finish(const FrameCounters *counters, FrameCounters *host_counters,
+                       const ViewCounters *views, ViewCounters *host_views, uint32_t num_views,
+                       cudaStream_t stream);
 
 // ---- small helpers ----------------------------------------------------------
 void launch_fill_u32(uint32_t *dst, uint32_t value, uint64_t count, cudaStream_t stream);

@@ -98,8 +98,15 @@ Pipeline::Pipeline(int device, cudaStream_t stream) : device_(device), stream_(s
   int sms = 0;
   GSR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
   sm_count_ = (uint32_t)sms;
+  // Runs read the view table from, and write their counters to, pinned host
+  // memory through its host address (unified addressing).
+  int uva = 0;
+  GSR_CUDA(cudaDeviceGetAttribute(&uva, cudaDevAttrUnifiedAddressing, device_));
+  if (!uva) throw Error(Code::Unsupported, "the CUDA device lacks unified addressing");
   for (auto &ev : ev_) GSR_CUDA(cudaEventCreate(&ev));
   for (auto &ev : slot_ev_) GSR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  for (auto &ev : upload_ev_) GSR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  GSR_CUDA(cudaStreamCreateWithFlags(&upload_stream_, cudaStreamNonBlocking));
   GSR_CUDA(cudaMallocHost(&counters_host_, sizeof(FrameCounters)));
   std::memset(counters_host_, 0, sizeof(FrameCounters));
   // fixed scratch: [counters | key hist | tile hist] zeroed per run, then
@@ -126,11 +133,15 @@ Pipeline::Pipeline(int device, cudaStream_t stream) : device_(device), stream_(s
 Pipeline::~Pipeline() {
   cudaSetDevice(device_);
   cudaStreamSynchronize(stream_);
+  if (upload_stream_) cudaStreamSynchronize(upload_stream_);
   drop_graph();
   for (auto &ev : ev_)
     if (ev) cudaEventDestroy(ev);
   for (auto &ev : slot_ev_)
     if (ev) cudaEventDestroy(ev);
+  for (auto &ev : upload_ev_)
+    if (ev) cudaEventDestroy(ev);
+  if (upload_stream_) cudaStreamDestroy(upload_stream_);
   if (counters_host_) cudaFreeHost(counters_host_);
   if (view_counters_pinned_) cudaFreeHost(view_counters_pinned_);
   if (views_pinned_) cudaFreeHost(views_pinned_);
@@ -213,6 +224,7 @@ void Pipeline::ensure_workspace(const Layout &l) {
   const uint32_t n = std::max<uint32_t>(l.total_splats, 1);
   if (l.views > view_cap_ || n > splat_cap_ || !view_ws_.get()) {
     GSR_CUDA(cudaStreamSynchronize(stream_));  // earlier runs may still use the old buffers
+    GSR_CUDA(cudaStreamSynchronize(upload_stream_));
     drop_graph();
     // Growth is geometric: a reallocation synchronises the device (cudaFree),
     // so a stream of batches of varying size must not regrow every time.
@@ -234,8 +246,9 @@ void Pipeline::ensure_workspace(const Layout &l) {
     const uint64_t o_k1 = off; off += align256(8 * k1_total);
     const uint64_t o_em = off; off += align256(8 * emit_words);
     view_zero_bytes_ = off;
-    const uint64_t o_tab = off; off += align256(sizeof(ViewDev) * vcap);
-    const uint64_t o_sets = off; off += align256(sizeof(ViewSetDev) * vcap);
+    // one table and set list per ring slot, uploaded ahead of their run
+    const uint64_t o_tab = off; off += align256(sizeof(ViewDev) * vcap * kViewSlots);
+    const uint64_t o_sets = off; off += align256(sizeof(ViewSetDev) * vcap * kViewSlots);
     view_ws_.reset(off);
     sets_dev_ = view_ws_.as<ViewSetDev>(o_sets);
     view_counters_ = view_ws_.as<ViewCounters>(o_vc);
@@ -336,31 +349,39 @@ void Pipeline::ensure_key_workspace(uint64_t capacity) {
 }
 
 void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &sinks,
-                          bool reuse) {
+                          bool reuse, const ViewDev *views_dev, const ViewSetDev *sets_dev) {
   const uint32_t n = std::max<uint32_t>(l.total_splats, 1);
-  GSR_CUDA(cudaMemsetAsync(fixed_.get(), 0,
-                           (char *)depth_plan_ - (char *)fixed_.get(), stream_));
-  GSR_CUDA(cudaMemsetAsync(view_ws_.get(), 0, view_zero_bytes_, stream_));
-  GSR_CUDA(cudaMemsetAsync(ranges_, 0, 8ull * l.total_tiles, stream_));
+  RunInit init{};
+  init.zero[0] = fixed_.as<uint32_t>();
+  init.zero_words[0] = ((char *)depth_plan_ - (char *)fixed_.get()) / 4;
+  init.zero[1] = view_ws_.as<uint32_t>();
+  init.zero_words[1] = view_zero_bytes_ / 4;
+  init.zero[2] = reinterpret_cast<uint32_t *>(ranges_);
+  init.zero_words[2] = 2ull * l.total_tiles;
+  init.zero[3] = depth_sort_work_;
+  init.zero_words[3] = kSortScratchHeadWords;
+  init.zero[4] = tile_sort_work_;
+  init.zero_words[4] = kSortScratchHeadWords;
+  launch_run_init(init, stream_);
   record(0);
 
   K1Buffers k1{vis_keys0_, vis_vals0_, rects_,         records_,
                k1_status_, counters_,  key_hist_,      view_counters_,
                debug_ ? projected_.as<ProjectedDev>() : nullptr, reuse};
-  launch_preprocess(views_dev_, sets_dev_, l.sets, l.total_blocks, l.max_planes, k1, debug_,
+  launch_preprocess(views_dev, sets_dev, l.sets, l.total_blocks, l.max_planes, k1, debug_,
                     stream_);
   record(1);
 
   if (!reuse) {  // a reused order keeps the last sort's ids and plan
     SortBuffers ds{vis_keys0_, vis_vals0_, vis_keys1_, vis_vals1_, &counters_->visible, n, 0, 4,
-                   depth_plan_, depth_sort_work_, &counters_->error, key_hist_};
+                   depth_plan_, depth_sort_work_, &counters_->error, key_hist_, true};
     launch_sort(ds, stream_);
   }
   record(2);
 
   EmitBuffers eb{depth_plan_, vis_vals0_,  vis_vals1_, rects_,        records_,
                  tile_keys0_, tile_vals0_, key_cap_,   emit_status_,  counters_,
-                 tile_hist_,  l.tile_passes, l.total_splats, views_dev_, l.views,
+                 tile_hist_,  l.tile_passes, l.total_splats, views_dev,  l.views,
                  tile_};
   launch_emit(eb, stream_);
   if (debug_) {
@@ -372,20 +393,20 @@ void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &si
   record(3);
   SortBuffers ts{tile_keys0_, tile_vals0_, tile_keys1_, tile_vals1_, &counters_->pairs,
                  (uint32_t)key_cap_, 0, l.tile_passes, tile_plan_, tile_sort_work_,
-                 &counters_->error, tile_hist_};
+                 &counters_->error, tile_hist_, true};
   launch_sort(ts, stream_);
   record(4);
   launch_ranges(tile_plan_, tile_keys0_, tile_keys1_, counters_, (uint32_t)key_cap_, ranges_,
-                views_dev_, l.views, view_counters_, stream_);
+                views_dev, l.views, view_counters_, stream_);
   record(5);
-  RasterArgs ra{views_dev_, l.views,  l.total_tiles, ranges_,   tile_plan_,
+  RasterArgs ra{views_dev,  l.views,  l.total_tiles, ranges_,   tile_plan_,
                 tile_vals0_, tile_vals1_, records_,  images, counters_, sticky_};
   launch_raster(ra, tile_, blend_mode_, raster_cfg_, sm_count_, stream_);
   record(6);
-  GSR_CUDA(cudaMemcpyAsync(sinks.counters, counters_, sizeof(FrameCounters),
-                           cudaMemcpyDeviceToHost, stream_));
-  GSR_CUDA(cudaMemcpyAsync(sinks.views, view_counters_, sizeof(ViewCounters) * l.views,
-                           cudaMemcpyDeviceToHost, stream_));
+  // Runs with host sinks write their counters there; the others leave them in
+  // device memory, read after the stream is synchronised.
+  if (sinks.counters)
+    launch_run_finish(counters_, sinks.counters, view_counters_, sinks.views, l.views, stream_);
 }
 
 void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
@@ -393,32 +414,42 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
   GSR_CUDA(cudaSetDevice(device_));
   const Layout l = plan_views(views, count, image_bases);
   ensure_workspace(l);
-  if (!sinks.counters) sinks.counters = counters_host_;
-  if (!sinks.views) sinks.views = view_counters_pinned_;
+  // No sinks given: the counters stay in device memory until the host reads
+  // them after a synchronisation (no host memory traffic inside the run).
+  const bool device_sinks = !sinks.counters;
+  if (device_sinks) sinks = HostSinks{};
   // The last sorted order can be reused only for the identical layout (same
   // scenes, sizes and tile grid) and while its buffers are intact.
   const bool reuse = reuse_request_ && sorted_valid_ && l == sorted_layout_ &&
                      std::equal(views, views + count, sorted_scenes_.begin(), sorted_scenes_.end(),
                                 [](const ViewSpec &v, const DeviceScene *s) { return v.scene == s; });
-  // The view table goes up from a pinned ring slot, asynchronously; the
-  // slot's previous copy is long done in steady state.
-  GSR_CUDA(cudaEventSynchronize(slot_ev_[slot_]));
-  ViewDev *staged = views_pinned_ + (uint64_t)slot_ * view_cap_;
+  // The view table goes up through a pinned ring slot into the slot's device
+  // table on the upload stream, as soon as the run is enqueued (runs ahead of
+  // the device upload theirs long before they start, so no host-memory read
+  // sits in a run's path); the run waits for its upload. A slot is reused
+  // once its previous run is done.
+  const uint32_t slot = slot_;
+  GSR_CUDA(cudaEventSynchronize(slot_ev_[slot]));
+  ViewDev *staged = views_pinned_ + (uint64_t)slot * view_cap_;
   std::memcpy(staged, views_host_.data(), sizeof(ViewDev) * l.views);
-  GSR_CUDA(cudaMemcpyAsync(views_dev_, staged, sizeof(ViewDev) * l.views, cudaMemcpyHostToDevice,
-                           stream_));
-  ViewSetDev *staged_sets = sets_pinned_ + (uint64_t)slot_ * view_cap_;
+  ViewSetDev *staged_sets = sets_pinned_ + (uint64_t)slot * view_cap_;
   std::memcpy(staged_sets, sets_host_.data(), sizeof(ViewSetDev) * l.sets);
-  GSR_CUDA(cudaMemcpyAsync(sets_dev_, staged_sets, sizeof(ViewSetDev) * l.sets,
-                           cudaMemcpyHostToDevice, stream_));
-  GSR_CUDA(cudaEventRecord(slot_ev_[slot_], stream_));
+  ViewDev *run_views = views_dev_ + (uint64_t)slot * view_cap_;
+  ViewSetDev *run_sets = sets_dev_ + (uint64_t)slot * view_cap_;
+  GSR_CUDA(cudaMemcpyAsync(run_views, staged, sizeof(ViewDev) * l.views, cudaMemcpyHostToDevice,
+                           upload_stream_));
+  GSR_CUDA(cudaMemcpyAsync(run_sets, staged_sets, sizeof(ViewSetDev) * l.sets,
+                           cudaMemcpyHostToDevice, upload_stream_));
+  GSR_CUDA(cudaEventRecord(upload_ev_[slot], upload_stream_));
+  GSR_CUDA(cudaStreamWaitEvent(stream_, upload_ev_[slot], 0));
   slot_ = (slot_ + 1) % kViewSlots;
 
   if (!use_graph_) {
-    launch_all(l, images, sinks, reuse);
+    launch_all(l, images, sinks, reuse, run_views, run_sets);
   } else {
-    const GraphKey key{l,     images,      key_cap_,       tile_,       blend_mode_,
-                       debug_, raster_cfg_, sinks.counters, sinks.views, reuse};
+    const GraphKey key{l,      images,      key_cap_,       tile_,       blend_mode_,
+                       debug_, raster_cfg_, sinks.counters, sinks.views, reuse,
+                       run_views};
     GraphEntry *hit = nullptr;
     for (auto &g : graphs_)
       if (g.key == key) hit = &g;
@@ -435,7 +466,7 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
       }
     }
     if (!hit && !seen) {
-      launch_all(l, images, sinks, reuse);
+      launch_all(l, images, sinks, reuse, run_views, run_sets);
     } else if (!hit) {
       if (graphs_.size() >= kGraphCacheSize) {
         auto lru = std::min_element(graphs_.begin(), graphs_.end(),
@@ -449,7 +480,7 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
       GSR_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
       capturing_ = true;
       try {
-        launch_all(l, images, sinks, reuse);
+        launch_all(l, images, sinks, reuse, run_views, run_sets);
       } catch (...) {
         capturing_ = false;
         cudaStreamEndCapture(stream_, &g);
@@ -474,8 +505,11 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
     }
   }
   GSR_CUDA(cudaGetLastError());
+  // The slot may be written again once this run (its first kernel) is done.
+  GSR_CUDA(cudaEventRecord(slot_ev_[slot], stream_));
   last_layout_ = l;
   last_sinks_ = sinks;
+  last_device_sinks_ = device_sinks;
   has_run_ = true;
   last_reused_ = reuse;
   if (!reuse) {
@@ -484,6 +518,15 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
     sorted_scenes_.clear();
     for (uint32_t v = 0; v < count; ++v) sorted_scenes_.push_back(views[v].scene);
   }
+}
+
+void Pipeline::fetch_counters() {
+  if (!last_device_sinks_) return;
+  // the stream is synchronised: counters_ hold the last run's values
+  GSR_CUDA(cudaMemcpy(counters_host_, counters_, sizeof(FrameCounters), cudaMemcpyDeviceToHost));
+  GSR_CUDA(cudaMemcpy(view_counters_pinned_, view_counters_,
+                      sizeof(ViewCounters) * last_layout_.views, cudaMemcpyDeviceToHost));
+  last_sinks_ = HostSinks{counters_host_, view_counters_pinned_};
 }
 
 void Pipeline::collect(RunResult &r) {
@@ -507,6 +550,7 @@ RunResult Pipeline::run(const ViewSpec *views, uint32_t count, uint32_t *images,
   for (;;) {
     enqueue(views, count, images, image_bases);
     GSR_CUDA(cudaStreamSynchronize(stream_));
+    fetch_counters();
     if (counters_host_->error)
       throw Error(Code::Internal, "device wait limit reached in a look-back scan (error bits " +
                                       std::to_string(counters_host_->error) + ")");
@@ -535,6 +579,7 @@ RunResult Pipeline::sync() {
   GSR_CUDA(cudaStreamSynchronize(stream_));
   RunResult r;
   if (!has_run_) return r;
+  fetch_counters();
   collect(r);
   r.frame_ms = r.preprocess_ms + r.sort_ms + r.raster_ms;
   last_ = r;

@@ -167,7 +167,15 @@ class Pipeline {
   Layout plan_views(const ViewSpec *views, uint32_t count, const uint64_t *image_bases);
   void ensure_workspace(const Layout &l);
   void ensure_key_workspace(uint64_t capacity);
-  void launch_all(const Layout &l, uint32_t *images, const HostSinks &sinks, bool reuse);
+  void launch_all(const Layout &l, uint32_t *images, const HostSinks &sinks, bool reuse,
+                  const ViewDev *views_dev, const ViewSetDev *sets_dev);
+  void fetch_counters();  // device-resident counters of the last run -> host (stream synchronised)
+
+ public:
+  // Recorded, in the last enqueued run, just before its raster launch.
+  cudaEvent_t raster_start_event() const { return ev_[kPhaseRaster]; }
+
+ private:
   void collect(RunResult &r);
   SortPlan read_plan(int which);
   void drop_graph();
@@ -225,6 +233,9 @@ class Pipeline {
   ViewDev *views_pinned_ = nullptr;
   ViewSetDev *sets_pinned_ = nullptr;
   cudaEvent_t slot_ev_[kViewSlots] = {};
+  cudaEvent_t upload_ev_[kViewSlots] = {};  // the slot's view table is on the device
+  cudaStream_t upload_stream_ = nullptr;
+  bool last_device_sinks_ = false;
   int slot_ = 0;
   // CUDA graphs of launch_all, one per layout, buffer set and setting.
   struct GraphKey {
@@ -237,10 +248,12 @@ class Pipeline {
     FrameCounters *host_counters;
     ViewCounters *host_views;
     bool reuse;
+    const ViewDev *staged;  // the ring slot's device view table the run reads
     bool operator==(const GraphKey &o) const {
       return layout == o.layout && images == o.images && key_cap == o.key_cap &&
              tile == o.tile && blend == o.blend && debug == o.debug && raster == o.raster &&
-             host_counters == o.host_counters && host_views == o.host_views && reuse == o.reuse;
+             host_counters == o.host_counters && host_views == o.host_views &&
+             reuse == o.reuse && staged == o.staged;
     }
   };
   struct GraphEntry {
@@ -248,7 +261,7 @@ class Pipeline {
     cudaGraphExec_t exec;
     uint64_t last_use;
   };
-  static constexpr size_t kGraphCacheSize = 32;
+  static constexpr size_t kGraphCacheSize = 64;
   std::vector<GraphEntry> graphs_;
   std::vector<GraphKey> seen_keys_;  // layouts launched once without a graph
   uint64_t graph_clock_ = 0;

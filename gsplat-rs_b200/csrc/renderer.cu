@@ -30,15 +30,27 @@ Renderer::Renderer(uint32_t width, uint32_t height) : width_(width), height_(hei
   if (width > kMaxImageDimension || height > kMaxImageDimension)
     throw Error(Code::Unsupported, "requested dimensions exceed the maximum of 16384");
   GSR_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  GSR_CUDA(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+  for (int k = 0; k < 2; ++k) {
+    GSR_CUDA(cudaEventCreateWithFlags(&rendered_[k], cudaEventDisableTiming));
+    GSR_CUDA(cudaEventCreateWithFlags(&copied_[k], cudaEventDisableTiming));
+  }
   pipe_ = std::make_unique<Pipeline>(device_, stream_);
 }
 
 Renderer::~Renderer() {
   cudaSetDevice(device_);
   if (stream_) cudaStreamSynchronize(stream_);
+  if (copy_stream_) cudaStreamSynchronize(copy_stream_);
   pipe_.reset();
   scene_.reset();
-  image_.reset(0);
+  image_[0].reset(0);
+  image_[1].reset(0);
+  for (int k = 0; k < 2; ++k) {
+    if (rendered_[k]) cudaEventDestroy(rendered_[k]);
+    if (copied_[k]) cudaEventDestroy(copied_[k]);
+  }
+  if (copy_stream_) cudaStreamDestroy(copy_stream_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -91,10 +103,45 @@ void Renderer::load_scene_path(const std::string &path) {
 
 void Renderer::ensure_image() {
   const uint64_t need = 4ull * width_ * height_;
-  if (image_.size() < need || image_.size() > 2 * need) {
+  if (image_[0].size() < need || image_[0].size() > 2 * need) {
+    if (deferred_.pending) issue_copy(false);
     GSR_CUDA(cudaStreamSynchronize(stream_));
-    image_.reset(need);
+    GSR_CUDA(cudaStreamSynchronize(copy_stream_));
+    image_[0].reset(need);
+    image_[1].reset(need);
+    copy_pending_[0] = copy_pending_[1] = false;
   }
+}
+
+uint32_t *Renderer::next_image() {
+  const int k = front_ ^ 1;
+  // a requested readback of this buffer has to be issued before it is reused
+  if (deferred_.pending && deferred_.image == k) issue_copy(false);
+  // the buffer's last readback must land before the frame overwrites it
+  if (copy_pending_[k]) {
+    GSR_CUDA(cudaStreamWaitEvent(stream_, copied_[k], 0));
+    copy_pending_[k] = false;
+  }
+  return image_[k].as<uint32_t>();
+}
+
+void Renderer::frame_enqueued() {
+  front_ ^= 1;
+  GSR_CUDA(cudaEventRecord(rendered_[front_], stream_));
+  if (deferred_.pending) issue_copy(true);
+}
+
+void Renderer::issue_copy(bool after_next_raster) {
+  const int k = deferred_.image;
+  // The image is complete once its frame is; with a frame enqueued after it,
+  // that frame's raster start is later still.
+  GSR_CUDA(cudaStreamWaitEvent(copy_stream_,
+                               after_next_raster ? pipe_->raster_start_event() : rendered_[k], 0));
+  GSR_CUDA(cudaMemcpyAsync(deferred_.out, image_[k].get(), deferred_.bytes, cudaMemcpyDeviceToHost,
+                           copy_stream_));
+  GSR_CUDA(cudaEventRecord(copied_[k], copy_stream_));
+  copy_pending_[k] = true;
+  deferred_.pending = false;
 }
 
 std::vector<ViewSpec> Renderer::one_view(const GsplatCamera &cam) {
@@ -131,7 +178,8 @@ void Renderer::finish_order() {
 FrameResult Renderer::render(const GsplatCamera &cam) {
   auto views = one_view(cam);
   plan_order(cam);
-  last_ = pipe_->run(views, image_.as<uint32_t>(), image_base_);
+  last_ = pipe_->run(views, next_image(), image_base_);
+  frame_enqueued();
   finish_order();
   has_frame_ = true;
   return last_;
@@ -140,18 +188,21 @@ FrameResult Renderer::render(const GsplatCamera &cam) {
 void Renderer::render_async(const GsplatCamera &cam) {
   auto views = one_view(cam);
   plan_order(cam);
-  pipe_->enqueue(views, image_.as<uint32_t>(), image_base_);
+  pipe_->enqueue(views, next_image(), image_base_);
+  frame_enqueued();
   finish_order();
   has_frame_ = true;
 }
 
 void Renderer::sync() {
+  if (deferred_.pending) issue_copy(false);
   try {
     last_ = pipe_->sync();
   } catch (const Error &e) {
     if (e.code == Code::Internal) has_frame_ = false;
     throw;
   }
+  GSR_CUDA(cudaStreamSynchronize(copy_stream_));
 }
 
 void Renderer::readback_rgba8(uint8_t *out, uint64_t len) {
@@ -159,8 +210,18 @@ void Renderer::readback_rgba8(uint8_t *out, uint64_t len) {
   if (!has_frame_) throw Error(Code::InvalidArgument, "no rendered frame to read back");
   if (len < need) throw Error(Code::InvalidArgument, "output buffer too small for the RGBA8 image");
   GSR_CUDA(cudaSetDevice(device_));
-  GSR_CUDA(cudaMemcpyAsync(out, image_.get(), need, cudaMemcpyDeviceToHost, stream_));
+  if (deferred_.pending) issue_copy(false);
+  GSR_CUDA(cudaMemcpyAsync(out, image_[front_].get(), need, cudaMemcpyDeviceToHost, stream_));
   GSR_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Renderer::readback_rgba8_async(uint8_t *out, uint64_t len) {
+  const uint64_t need = 4ull * width_ * height_;
+  if (!has_frame_) throw Error(Code::InvalidArgument, "no rendered frame to read back");
+  if (len < need) throw Error(Code::InvalidArgument, "output buffer too small for the RGBA8 image");
+  GSR_CUDA(cudaSetDevice(device_));
+  if (deferred_.pending) issue_copy(false);
+  deferred_ = DeferredCopy{true, front_, out, need};
 }
 
 std::vector<uint32_t> Renderer::debug_order() {

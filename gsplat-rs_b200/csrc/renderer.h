@@ -66,6 +66,12 @@ class Renderer {
   bool has_frame() const { return has_frame_; }
 
   void readback_rgba8(uint8_t *out, uint64_t len);
+  // Requests the copy of the last frame's image into `out` (pinned host
+  // memory, kept valid until sync()) and returns. The copy runs on a copy
+  // stream while the next frame renders: it is issued with that frame, timed
+  // to its raster, or at sync(). Frames alternate between two image buffers;
+  // a buffer is rendered into again only after its copy.
+  void readback_rgba8_async(uint8_t *out, uint64_t len);
   std::vector<uint32_t> debug_order();
   std::vector<ProjectedDev> debug_projected();
   void debug_tile_pairs(std::vector<uint32_t> &tiles, std::vector<uint32_t> &ids);
@@ -90,7 +96,25 @@ class Renderer {
   std::unique_ptr<Pipeline> pipe_;
   std::unique_ptr<DeviceScene> scene_;
   FrameResult last_;
-  DeviceBuffer image_;
+  // Two image buffers: frames alternate between them (front_ = last frame's).
+  DeviceBuffer image_[2];
+  int front_ = 1;
+  cudaStream_t copy_stream_ = nullptr;
+  cudaEvent_t rendered_[2] = {nullptr, nullptr};  // frame into image_[k] complete
+  cudaEvent_t copied_[2] = {nullptr, nullptr};    // async readback of image_[k] complete
+  bool copy_pending_[2] = {false, false};
+  // A readback requested but not yet issued: it starts with the next frame's
+  // raster (one long kernel, so the copy's PCIe traffic does not delay that
+  // frame's other launches), or at sync().
+  struct DeferredCopy {
+    bool pending = false;
+    int image = 0;
+    uint8_t *out = nullptr;
+    uint64_t bytes = 0;
+  } deferred_;
+  void issue_copy(bool after_next_raster);
+  uint32_t *next_image();  // the buffer the next frame renders into (waits for its readback)
+  void frame_enqueued();   // marks that buffer as the last frame's
   const std::vector<uint64_t> image_base_{0};
 };
 

@@ -207,6 +207,8 @@ _SIGS = [
     ("gsplat_context_load_scene_buffers", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.POINTER(GsplatSceneDesc)]),
     ("gsplat_context_readback_rgba8", ctypes.c_int32, [ctypes.c_void_p, _u8p, ctypes.c_uint64]),
+    ("gsplat_context_readback_rgba8_async", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64]),
     ("gsplat_context_get_frame_counts", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.POINTER(GsplatFrameCounts)]),
     ("gsplat_context_get_phase_times", ctypes.c_int32,
@@ -451,6 +453,11 @@ class Context:
         n = ctypes.c_uint32()
         check(lib().gsplat_context_get_phase_times(self.ptr, out, 16, ctypes.byref(n)))
         return dict(zip(self.PHASES, [out[k] for k in range(n.value)]))
+
+    def readback_rgba8_async(self, out):
+        """Enqueue the last frame's RGBA8 copy into `out` (a uint8 array of
+        width*height*4 bytes, ideally pinned); it lands by the next sync()."""
+        check(lib().gsplat_context_readback_rgba8_async(self.ptr, out.ctypes.data, out.nbytes))
 
     def render_frame_async(self):
         check(lib().gsplat_context_render_frame_async(self.ptr))

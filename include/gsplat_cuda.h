@@ -128,6 +128,11 @@ int32_t gsplat_context_load_scene_packed(GsplatContext *ctx, const GsplatSceneDe
  * bytes) into `out`, which must hold width*height*4 bytes. Stands in for
  * Renderer::readback_rgba8 (lib.rs:779-795). */
 int32_t gsplat_context_readback_rgba8(GsplatContext *ctx, uint8_t *out, uint64_t out_len);
+/* Enqueue that copy on the context's copy stream and return: `out` (pinned
+ * host memory for an asynchronous copy) must stay valid until
+ * gsplat_context_sync. Frames alternate between two device images, so the
+ * next frame renders while this one is copied. No reference counterpart. */
+int32_t gsplat_context_readback_rgba8_async(GsplatContext *ctx, uint8_t *out, uint64_t out_len);
 
 int32_t gsplat_context_get_frame_counts(const GsplatContext *ctx, GsplatFrameCounts *out);
 
