@@ -346,14 +346,6 @@ __global__ void run_init_kernel(RunInit a) {
     for (uint64_t i = t; i < a.zero_words[r]; i += stride) a.zero[r][i] = 0u;
 }
 
-__global__ void run_finish_kernel(const uint32_t *counters, uint32_t *host_counters,
-                                  uint32_t counter_words, const uint32_t *views,
-                                  uint32_t *host_views, uint32_t view_words) {
-  for (uint32_t i = threadIdx.x; i < counter_words; i += blockDim.x) host_counters[i] = counters[i];
-  for (uint32_t i = threadIdx.x; i < view_words; i += blockDim.x) host_views[i] = views[i];
-  __threadfence_system();
-}
-
 __global__ void fill_kernel(uint32_t *dst, uint32_t value, uint64_t count) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
        i += (uint64_t)gridDim.x * blockDim.x)
@@ -397,16 +389,6 @@ void launch_run_init(const RunInit &a, cudaStream_t stream) {
   for (int r = 0; r < kRunZeroRegions; ++r) words = std::max(words, a.zero_words[r]);
   const uint64_t blocks = std::min<uint64_t>(std::max<uint64_t>((words + 255) / 256, 1), 148 * 8);
   run_init_kernel<<<(uint32_t)blocks, 256, 0, stream>>>(a);
-}
-
-void launch_run_finish(const FrameCounters *counters, FrameCounters *host_counters,
-                       const ViewCounters *views, ViewCounters *host_views, uint32_t num_views,
-                       cudaStream_t stream) {
-  static_assert(sizeof(FrameCounters) % 4 == 0 && sizeof(ViewCounters) % 4 == 0, "word copies");
-  run_finish_kernel<<<1, 256, 0, stream>>>(
-      reinterpret_cast<const uint32_t *>(counters), reinterpret_cast<uint32_t *>(host_counters),
-      sizeof(FrameCounters) / 4, reinterpret_cast<const uint32_t *>(views),
-      reinterpret_cast<uint32_t *>(host_views), num_views * (uint32_t)(sizeof(ViewCounters) / 4));
 }
 
 void launch_fill_u32(uint32_t *dst, uint32_t value, uint64_t count, cudaStream_t stream) {

@@ -125,20 +125,16 @@ bool raster_config_valid(uint32_t tile, const RasterConfig &cfg);
 void launch_raster(const RasterArgs &a, uint32_t tile, uint32_t blend_mode,
                    const RasterConfig &cfg, uint32_t sm_count, cudaStream_t stream);
 
-// ---- run start and end ----------------------------------------------------
-// A run issues no copy-engine work and reads no host memory, so a caller's
-// own host<->device copies (an image readback while the next frame renders)
-// never stall it: one kernel zeroes the run's scratch, and when the run has
-// host sinks another writes the counters there.
+// ---- run start ------------------------------------------------------------
+// One kernel zeroes a run's scratch (in place of memsets: a plain frame then
+// issues no copy-engine work, so a caller's own host<->device copies never
+// queue in front of it).
 constexpr int kRunZeroRegions = 5;
 struct RunInit {
   uint32_t *zero[kRunZeroRegions];       // regions zeroed at the start of a run
   uint64_t zero_words[kRunZeroRegions];
 };
 void launch_run_init(const RunInit &a, cudaStream_t stream);
-void launch_run_finish(const FrameCounters *counters, FrameCounters *host_counters,
-                       const ViewCounters *views, ViewCounters *host_views, uint32_t num_views,
-                       cudaStream_t stream);
 
 // ---- small helpers ----------------------------------------------------------
 void launch_fill_u32(uint32_t *dst, uint32_t value, uint64_t count, cudaStream_t stream);

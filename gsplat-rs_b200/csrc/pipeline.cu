@@ -98,15 +98,9 @@ Pipeline::Pipeline(int device, cudaStream_t stream) : device_(device), stream_(s
   int sms = 0;
   GSR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
   sm_count_ = (uint32_t)sms;
-  // Runs read the view table from, and write their counters to, pinned host
-  // memory through its host address (unified addressing).
-  int uva = 0;
-  GSR_CUDA(cudaDeviceGetAttribute(&uva, cudaDevAttrUnifiedAddressing, device_));
-  if (!uva) throw Error(Code::Unsupported, "the CUDA device lacks unified addressing");
   for (auto &ev : ev_) GSR_CUDA(cudaEventCreate(&ev));
   for (auto &ev : slot_ev_) GSR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-  for (auto &ev : upload_ev_) GSR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-  GSR_CUDA(cudaStreamCreateWithFlags(&upload_stream_, cudaStreamNonBlocking));
+
   GSR_CUDA(cudaMallocHost(&counters_host_, sizeof(FrameCounters)));
   std::memset(counters_host_, 0, sizeof(FrameCounters));
   // fixed scratch: [counters | key hist | tile hist] zeroed per run, then
@@ -133,15 +127,12 @@ Pipeline::Pipeline(int device, cudaStream_t stream) : device_(device), stream_(s
 Pipeline::~Pipeline() {
   cudaSetDevice(device_);
   cudaStreamSynchronize(stream_);
-  if (upload_stream_) cudaStreamSynchronize(upload_stream_);
   drop_graph();
   for (auto &ev : ev_)
     if (ev) cudaEventDestroy(ev);
   for (auto &ev : slot_ev_)
     if (ev) cudaEventDestroy(ev);
-  for (auto &ev : upload_ev_)
-    if (ev) cudaEventDestroy(ev);
-  if (upload_stream_) cudaStreamDestroy(upload_stream_);
+
   if (counters_host_) cudaFreeHost(counters_host_);
   if (view_counters_pinned_) cudaFreeHost(view_counters_pinned_);
   if (views_pinned_) cudaFreeHost(views_pinned_);
@@ -224,7 +215,6 @@ void Pipeline::ensure_workspace(const Layout &l) {
   const uint32_t n = std::max<uint32_t>(l.total_splats, 1);
   if (l.views > view_cap_ || n > splat_cap_ || !view_ws_.get()) {
     GSR_CUDA(cudaStreamSynchronize(stream_));  // earlier runs may still use the old buffers
-    GSR_CUDA(cudaStreamSynchronize(upload_stream_));
     drop_graph();
     // Growth is geometric: a reallocation synchronises the device (cudaFree),
     // so a stream of batches of varying size must not regrow every time.
@@ -246,9 +236,8 @@ void Pipeline::ensure_workspace(const Layout &l) {
     const uint64_t o_k1 = off; off += align256(8 * k1_total);
     const uint64_t o_em = off; off += align256(8 * emit_words);
     view_zero_bytes_ = off;
-    // one table and set list per ring slot, uploaded ahead of their run
-    const uint64_t o_tab = off; off += align256(sizeof(ViewDev) * vcap * kViewSlots);
-    const uint64_t o_sets = off; off += align256(sizeof(ViewSetDev) * vcap * kViewSlots);
+    const uint64_t o_tab = off; off += align256(sizeof(ViewDev) * vcap);
+    const uint64_t o_sets = off; off += align256(sizeof(ViewSetDev) * vcap);
     view_ws_.reset(off);
     sets_dev_ = view_ws_.as<ViewSetDev>(o_sets);
     view_counters_ = view_ws_.as<ViewCounters>(o_vc);
@@ -403,10 +392,14 @@ void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &si
                 tile_vals0_, tile_vals1_, records_,  images, counters_, sticky_};
   launch_raster(ra, tile_, blend_mode_, raster_cfg_, sm_count_, stream_);
   record(6);
-  // Runs with host sinks write their counters there; the others leave them in
+  // Runs with host sinks copy their counters there; the others leave them in
   // device memory, read after the stream is synchronised.
-  if (sinks.counters)
-    launch_run_finish(counters_, sinks.counters, view_counters_, sinks.views, l.views, stream_);
+  if (sinks.counters) {
+    GSR_CUDA(cudaMemcpyAsync(sinks.counters, counters_, sizeof(FrameCounters),
+                             cudaMemcpyDeviceToHost, stream_));
+    GSR_CUDA(cudaMemcpyAsync(sinks.views, view_counters_, sizeof(ViewCounters) * l.views,
+                             cudaMemcpyDeviceToHost, stream_));
+  }
 }
 
 void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
@@ -423,33 +416,29 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
   const bool reuse = reuse_request_ && sorted_valid_ && l == sorted_layout_ &&
                      std::equal(views, views + count, sorted_scenes_.begin(), sorted_scenes_.end(),
                                 [](const ViewSpec &v, const DeviceScene *s) { return v.scene == s; });
-  // The view table goes up through a pinned ring slot into the slot's device
-  // table on the upload stream, as soon as the run is enqueued (runs ahead of
-  // the device upload theirs long before they start, so no host-memory read
-  // sits in a run's path); the run waits for its upload. A slot is reused
-  // once its previous run is done.
+  // The view table goes up from a pinned ring slot, ahead of the run on its
+  // stream (outside the run's graph, so the graph serves every frame of the
+  // layout); the slot's previous copy is long done in steady state.
   const uint32_t slot = slot_;
   GSR_CUDA(cudaEventSynchronize(slot_ev_[slot]));
   ViewDev *staged = views_pinned_ + (uint64_t)slot * view_cap_;
   std::memcpy(staged, views_host_.data(), sizeof(ViewDev) * l.views);
+  GSR_CUDA(cudaMemcpyAsync(views_dev_, staged, sizeof(ViewDev) * l.views, cudaMemcpyHostToDevice,
+                           stream_));
   ViewSetDev *staged_sets = sets_pinned_ + (uint64_t)slot * view_cap_;
   std::memcpy(staged_sets, sets_host_.data(), sizeof(ViewSetDev) * l.sets);
-  ViewDev *run_views = views_dev_ + (uint64_t)slot * view_cap_;
-  ViewSetDev *run_sets = sets_dev_ + (uint64_t)slot * view_cap_;
-  GSR_CUDA(cudaMemcpyAsync(run_views, staged, sizeof(ViewDev) * l.views, cudaMemcpyHostToDevice,
-                           upload_stream_));
-  GSR_CUDA(cudaMemcpyAsync(run_sets, staged_sets, sizeof(ViewSetDev) * l.sets,
-                           cudaMemcpyHostToDevice, upload_stream_));
-  GSR_CUDA(cudaEventRecord(upload_ev_[slot], upload_stream_));
-  GSR_CUDA(cudaStreamWaitEvent(stream_, upload_ev_[slot], 0));
+  GSR_CUDA(cudaMemcpyAsync(sets_dev_, staged_sets, sizeof(ViewSetDev) * l.sets,
+                           cudaMemcpyHostToDevice, stream_));
+  GSR_CUDA(cudaEventRecord(slot_ev_[slot], stream_));
   slot_ = (slot_ + 1) % kViewSlots;
+  ViewDev *run_views = views_dev_;
+  ViewSetDev *run_sets = sets_dev_;
 
   if (!use_graph_) {
     launch_all(l, images, sinks, reuse, run_views, run_sets);
   } else {
-    const GraphKey key{l,      images,      key_cap_,       tile_,       blend_mode_,
-                       debug_, raster_cfg_, sinks.counters, sinks.views, reuse,
-                       run_views};
+    const GraphKey key{l,     images,      key_cap_,       tile_,       blend_mode_,
+                       debug_, raster_cfg_, sinks.counters, sinks.views, reuse};
     GraphEntry *hit = nullptr;
     for (auto &g : graphs_)
       if (g.key == key) hit = &g;
@@ -505,8 +494,6 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
     }
   }
   GSR_CUDA(cudaGetLastError());
-  // The slot may be written again once this run (its first kernel) is done.
-  GSR_CUDA(cudaEventRecord(slot_ev_[slot], stream_));
   last_layout_ = l;
   last_sinks_ = sinks;
   last_device_sinks_ = device_sinks;

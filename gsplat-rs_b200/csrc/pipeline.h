@@ -233,8 +233,6 @@ class Pipeline {
   ViewDev *views_pinned_ = nullptr;
   ViewSetDev *sets_pinned_ = nullptr;
   cudaEvent_t slot_ev_[kViewSlots] = {};
-  cudaEvent_t upload_ev_[kViewSlots] = {};  // the slot's view table is on the device
-  cudaStream_t upload_stream_ = nullptr;
   bool last_device_sinks_ = false;
   int slot_ = 0;
   // CUDA graphs of launch_all, one per layout, buffer set and setting.
@@ -248,12 +246,11 @@ class Pipeline {
     FrameCounters *host_counters;
     ViewCounters *host_views;
     bool reuse;
-    const ViewDev *staged;  // the ring slot's device view table the run reads
     bool operator==(const GraphKey &o) const {
       return layout == o.layout && images == o.images && key_cap == o.key_cap &&
              tile == o.tile && blend == o.blend && debug == o.debug && raster == o.raster &&
              host_counters == o.host_counters && host_views == o.host_views &&
-             reuse == o.reuse && staged == o.staged;
+             reuse == o.reuse;
     }
   };
   struct GraphEntry {
