@@ -50,6 +50,51 @@ def dist_setup():
     return world, rank, local
 
 
+class Replicas:
+    """The replicas of a multi-GPU run (one process per GPU under torchrun,
+    no data-path collective): a barrier around each timed region and the max
+    of the ranks' times, over `backend` (nccl for the GPUs; gloo in the CPU
+    tests). A single process needs no process group."""
+
+    def __init__(self, world, rank, backend="nccl", device=None, timeout_s=120.0):
+        self.world, self.rank = world, rank
+        self.dist = None
+        if world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            kw = {"device_id": device} if device is not None else {}
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
+            self.dist = dist
+            self.device = device
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def max(self, value):
+        """The max over ranks of a per-rank time."""
+        if not self.dist:
+            return value
+        import torch
+
+        t = torch.tensor([value], dtype=torch.float64,
+                         device=self.device if self.device is not None else "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist:
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def whole_job_rate(world, units_per_rank, max_seconds):
+    """Units all ranks processed per second of the slowest rank."""
+    return world * units_per_rank / max_seconds
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons, sampled every 100 ms from before
     the warm-up until after the timed region; stop() keeps the samples whose
@@ -581,13 +626,7 @@ def run_cuda(args, world, rank, local):
     if args.only:
         run_sections_only(args, ffi, torch)
         return
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    replicas = Replicas(world, rank, "nccl", torch.device("cuda", local))
     scene, cam, w, h = gsplat_scenes.config2()
     clocks = ClockSampler(local)
     clocks.start()
@@ -612,8 +651,7 @@ def run_cuda(args, world, rank, local):
 
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    if world > 1:
-        torch.distributed.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     t_begin = time.time()
     for i in range(args.steps):
@@ -626,14 +664,10 @@ def run_cuda(args, world, rank, local):
     ctx.sync()
     torch.cuda.synchronize()
     clocks.mark(t_begin, time.time())
-    device_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    if world > 1:
-        t = torch.tensor([device_ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        device_ms = float(t.item())
-        torch.distributed.barrier()
+    device_ms = replicas.max(sum(s.elapsed_time(e) for s, e in zip(starts, ends)))
+    replicas.barrier()
     ms_per_frame = device_ms / args.steps
-    value = world * args.steps / (device_ms / 1000.0)
+    value = whole_job_rate(world, args.steps, device_ms / 1000.0)
 
     # End to end through the C ABI: camera in, frame, RGBA8 readback to pinned
     # memory every step. Frames are enqueued back to back and each image is
@@ -647,8 +681,7 @@ def run_cuda(args, world, rank, local):
         yaw = 0.7 + 0.002 * i
         cams.append(ffi.GsplatCamera.from_dict(gsplat_scenes.camera(
             (4.0 * math.sin(yaw), 0.5, -4.0 * math.cos(yaw)), (0, 0, 0), 45.0)))
-    if world > 1:
-        torch.distributed.barrier()
+    replicas.barrier()
     t0 = time.perf_counter()
     for i in range(args.steps):
         ctx.set_camera(cams[i])
@@ -657,14 +690,11 @@ def run_cuda(args, world, rank, local):
     ctx.sync()
     e2e_s = time.perf_counter() - t0
     out = outs[(args.steps - 1) % 2]
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = replicas.max(e2e_s)
     if args.artifact and rank == 0:
         write_plain_artifact(args, ffi, ctx, scene, cams, out, w, h)
     clk = clocks.stop()
-    e2e = {"value": world * args.steps / e2e_s, "unit": "frames/s",
+    e2e = {"value": whole_job_rate(world, args.steps, e2e_s), "unit": "frames/s",
            "h2d_bytes_per_step": 40, "d2h_bytes_per_step": w * h * 4 + 64}
 
     tiles = ((w + 15) // 16) * ((h + 15) // 16)
@@ -713,8 +743,7 @@ def run_cuda(args, world, rank, local):
         line["ingest"] = measure_ingest(ffi, args.ingest_splats)
     if not args.no_packed and world == 1:
         line["packed"] = measure_packed(ffi, torch)
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    replicas.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
 
