@@ -164,16 +164,17 @@ __device__ __forceinline__ float exp_neg(float x) {
   return __int_as_float(__float_as_int(p) + e * (1 << 23));
 }
 
-// e^(-4.5 r2) for r2 in [0, 1], the FP32 raster's weight: one multiply by
-// -4.5 log2(e) and the hardware base-2 exponential (ex2.approx, a few ulp;
-// the argument lies in [-6.5, 0], so no subnormal is involved). The CPU
-// model of this raster evaluates 2^t with a degree-6 polynomial instead;
-// the two images agree to the last UNORM8 step except where a weight sits
-// on the 1/256 threshold or a channel on a rounding boundary.
-__device__ __forceinline__ float gauss_weight(float r2) {
-  float g;
-  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(g) : "f"(r2 * -6.49212768f));
-  return g;
+// alpha e^(-4.5 r2) for r2 in [0, 1], the FP32 raster's weight: one fma of
+// r2 by -4.5 log2(e) onto log2(alpha) and the hardware base-2 exponential
+// (ex2.approx, a few ulp; the argument lies in [-14.5, 0], so no subnormal is
+// involved). The CPU model of this raster evaluates 2^t with a degree-6
+// polynomial instead; the two images agree to the last UNORM8 step except
+// where a weight sits on the 1/256 threshold or a channel on a rounding
+// boundary.
+__device__ __forceinline__ float blend_weight(float r2, float log2_alpha) {
+  float w;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(w) : "f"(fmaf(r2, -6.49212768f, log2_alpha)));
+  return w;
 }
 
 __device__ __forceinline__ uint32_t to_unorm8(float x) {

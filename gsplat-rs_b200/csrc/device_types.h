@@ -45,7 +45,7 @@ constexpr uint32_t kPackedFloats = kPackedHeaderFloats + kPackedVarLut + kPacked
 //   a = (cx, cy, ax, ay)  centre in pixel-centre coordinates, first row of
 //                         the inverse axis matrix (local x = ax*dx + ay*dy)
 //   b = (bx, by, s, alpha) second row, quad extent scale, opacity
-//   c = (r*alpha, g*alpha, b*alpha, 0) premultiplied colour
+//   c = (r, g, b, log2(alpha))  colour before alpha (premultiplied: r*alpha)
 struct Record {
   float4 a, b, c;
 };

@@ -214,7 +214,9 @@ __device__ __forceinline__ bool project(const FrameParams &p, const float4 &pa, 
   float vv = av0 * av0 + av1 * av1;
   rec.a = make_float4(cxp, cyp, (au0 * p.sx) / uu, (au1 * p.sy) / uu);
   rec.b = make_float4((av0 * p.sx) / vv, (av1 * p.sy) / vv, s, al);
-  rec.c = make_float4(pr, pg, pb, 0.0f);
+  // colour before alpha and log2(alpha) (hardware logarithm): the FP32
+  // raster's weight is 2^(log2 alpha - 4.5 log2(e) r2)
+  rec.c = make_float4(rgb[0], rgb[1], rgb[2], __log2f(al));
 
   rect = make_uint2(0u, 0u);
   if (al > 1.0f / 256.0f) {

@@ -14,9 +14,9 @@
 // w = alpha * exp(-4.5 r^2) > 1/256; the source is (premult rgb * g, w).
 //   FP32 mode: front to back (walks the list from its end); coverage is
 //     r^2 <= s^2 and w > 1/256 (in exact arithmetic the same set as the quad
-//     clip, r^2 <= 1 and the alpha threshold); C += premult * (g T),
-//     T *= 1 - w; a pixel finishes once T < 1e-4, a warp when all its pixels
-//     have, the block stops loading once all are done.
+//     clip, r^2 <= 1 and the alpha threshold); C += rgb * (w T), T -= w T;
+//     a pixel finishes once T < 1e-4, a warp when all its pixels have, the
+//     block stops loading once all are done.
 //   UNORM8 mode: back to front, dst = src + dst * (1 - w) rounded to UNORM8
 //     after every splat (the reference's Rgba8Unorm premultiplied blend).
 
@@ -106,9 +106,10 @@ __global__ void __launch_bounds__(kTile *kTile) raster_unorm8_kernel(RasterArgs 
         float w = rb.w * g;
         if (!(w > 1.0f / 256.0f)) continue;
         float om = 1.0f - w;
-        d0 = to_unorm8(fmaf((float)d0 / 255.0f, om, col.x * g));
-        d1 = to_unorm8(fmaf((float)d1 / 255.0f, om, col.y * g));
-        d2 = to_unorm8(fmaf((float)d2 / 255.0f, om, col.z * g));
+        // premultiplied colour: the vertex stage's rgb * alpha
+        d0 = to_unorm8(fmaf((float)d0 / 255.0f, om, (col.x * rb.w) * g));
+        d1 = to_unorm8(fmaf((float)d1 / 255.0f, om, (col.y * rb.w) * g));
+        d2 = to_unorm8(fmaf((float)d2 / 255.0f, om, (col.z * rb.w) * g));
         d3 = to_unorm8(fmaf((float)d3 / 255.0f, om, w));
       }
     }
@@ -263,26 +264,27 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
     __syncwarp();
     // Two list entries per step (one early-out vote, one packed index
     // load); each pixel still takes them strictly in list order.
-    auto blend = [&](uint32_t j, float r2, float s2, float w_alpha) {
+    // w = alpha e^(-4.5 r2) = 2^(log2 alpha - 4.5 log2(e) r2) (the entry's
+    // log2 alpha in its colour's w), so the colour takes rgb * (w T) and the
+    // transmittance loses w T.
+    auto blend = [&](uint32_t j, float r2, float s2) {
       if (done || !(r2 <= s2)) return;
-      const float g = gauss_weight(r2);
-      const float w = w_alpha * g;
-      if (!(w > 1.0f / 256.0f)) return;
       const float4 col = sm.d2[j];
-      const float gT = g * T;
-      c0 = fmaf(col.x, gT, c0);
-      c1 = fmaf(col.y, gT, c1);
-      c2 = fmaf(col.z, gT, c2);
-      T = T * (1.0f - w);
+      const float w = blend_weight(r2, col.w);
+      if (!(w > 1.0f / 256.0f)) return;
+      const float wT = w * T;
+      c0 = fmaf(col.x, wT, c0);
+      c1 = fmaf(col.y, wT, c1);
+      c2 = fmaf(col.z, wT, c2);
+      T = T - wT;
       if (T < 1e-4f) done = true;
     };
-    auto local_r2 = [&](uint32_t j, float &s2, float &alpha) {
+    auto local_r2 = [&](uint32_t j, float &s2) {
       const float4 d0 = sm.d0[j];
       const float4 d1 = sm.d1[j];
       const float lx = fmaf(d0.x, fx, fmaf(d0.y, fy, d0.z));
       const float ly = fmaf(d1.x, fx, fmaf(d1.y, fy, d1.z));
       s2 = d0.w;
-      alpha = d1.w;
       return fmaf(lx, lx, ly * ly);
     };
     uint32_t i = 0;
@@ -290,17 +292,17 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
       if (__all_sync(0xffffffffu, done)) break;
       const uint32_t jj = *reinterpret_cast<const uint32_t *>(&sm.list[warp][i]);
       const uint32_t ja = jj & 0xffffu, jb = jj >> 16;
-      float sa, aa, sb, ab;
-      const float r2a = local_r2(ja, sa, aa);
-      const float r2b = local_r2(jb, sb, ab);
-      blend(ja, r2a, sa, aa);
-      blend(jb, r2b, sb, ab);
+      float sa, sb;
+      const float r2a = local_r2(ja, sa);
+      const float r2b = local_r2(jb, sb);
+      blend(ja, r2a, sa);
+      blend(jb, r2b, sb);
     }
     if (i < n_w && !__all_sync(0xffffffffu, done)) {
       const uint32_t ja = sm.list[warp][i];
-      float sa, aa;
-      const float r2a = local_r2(ja, sa, aa);
-      blend(ja, r2a, sa, aa);
+      float sa;
+      const float r2a = local_r2(ja, sa);
+      blend(ja, r2a, sa);
     }
     if (__syncthreads_count(done) == kTile * kTile) break;
   }

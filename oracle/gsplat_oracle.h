@@ -71,7 +71,7 @@ typedef struct OrcProjected {
 typedef struct OrcRecord {
   float cx, cy, ax, ay;
   float bx, by, s, alpha;
-  float pr, pg, pb, pad;
+  float cr, cg, cb, log2a;  /* colour (not premultiplied) and log2(alpha) */
 } OrcRecord;
 
 typedef struct OrcFrameParams {

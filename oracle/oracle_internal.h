@@ -51,16 +51,17 @@ inline float exp_neg(float x) {
   return bits_to_float(float_to_bits(p) + (uint32_t)(e * (1 << 23)));
 }
 
-// e^(-4.5 r2) for r2 in [0, 1] in the FP32 tile model: one folded constant
-// (-4.5 log2 e), the 1.5 * 2^23 shifter for the nearest integer n, the
-// degree-6 Taylor polynomial of 2^f, and n added to the exponent bits
-// (relative error about 2e-7). The CUDA raster takes 2^t from the hardware
-// base-2 exponential (a few ulp), so its images equal this model's up to
-// rare single UNORM8 steps: a weight on the 1/256 threshold, or a channel on
-// a rounding boundary.
-inline float gauss_weight(float r2) {
+// The FP32 tile model's blend weight alpha e^(-4.5 r2) = 2^t with
+// t = fma(r2, -4.5 log2 e, log2 alpha): the 1.5 * 2^23 shifter gives the
+// nearest integer n of t, f = t - n in [-0.5, 0.5] feeds the degree-6 Taylor
+// polynomial of 2^f, and n is added to the exponent bits (relative error about
+// 2e-7). The CUDA raster takes 2^t from the hardware base-2 exponential (a few
+// ulp) and log2 alpha from the hardware logarithm, so its images equal this
+// model's up to rare single UNORM8 steps: a weight on the 1/256 threshold, or
+// a channel on a rounding boundary.
+inline float blend_weight(float r2, float log2_alpha) {
   const float kShift = 12582912.0f;
-  float t = r2 * -6.49212768f;
+  float t = std::fma(r2, -6.49212768f, log2_alpha);
   float tr = t + kShift;
   float n = tr - kShift;
   float f = t - n;

@@ -55,7 +55,7 @@ PROJECTED_DTYPE = np.dtype([("center_ndc", "<f4", 2), ("axis_u", "<f4", 2), ("ax
                             ("flags", "<u4"), ("tile_x0", "<u2"), ("tile_y0", "<u2"),
                             ("tile_x1", "<u2"), ("tile_y1", "<u2"), ("reserved", "<u4")])
 RECORD_DTYPE = np.dtype([(n, "<f4") for n in ("cx", "cy", "ax", "ay", "bx", "by", "s", "alpha",
-                                               "pr", "pg", "pb", "pad")])
+                                               "cr", "cg", "cb", "log2a")])
 assert PROJECTED_DTYPE.itemsize == 64 and RECORD_DTYPE.itemsize == 48
 
 _lib = None

@@ -191,7 +191,8 @@ static void project_one(const OrcScene &sc, const float *alpha, const float *ext
   rec.ax = (au0 * p.sx) / uu; rec.ay = (au1 * p.sy) / uu;
   rec.bx = (av0 * p.sx) / vv; rec.by = (av1 * p.sy) / vv;
   rec.s = s; rec.alpha = al;
-  rec.pr = out.color[0]; rec.pg = out.color[1]; rec.pb = out.color[2];
+  rec.cr = rgb[0]; rec.cg = rgb[1]; rec.cb = rgb[2];
+  rec.log2a = std::log2(al);
 
   // Tile rect: pixel bbox of the ellipse |local| <= s, widened by a small
   // margin, clamped to the image. Splats with alpha <= 1/256 never pass the
@@ -374,7 +375,8 @@ __attribute__((target_clones("fma", "default"))) static void unorm8_band(
         if (!pixel_weight(r, px, py, g, w)) continue;
         uint8_t *d = &rgba[((size_t)py * width + px) * 4];
         float one_minus = 1.0f - w;
-        float src[3] = {r.pr * g, r.pg * g, r.pb * g};
+        // premultiplied colour: the vertex stage's rgb * alpha
+        float src[3] = {(r.cr * r.alpha) * g, (r.cg * r.alpha) * g, (r.cb * r.alpha) * g};
         for (int ch = 0; ch < 3; ++ch) d[ch] = to_unorm8(std::fma(g_inv255[d[ch]], one_minus, src[ch]));
         d[3] = to_unorm8(std::fma(g_inv255[d[3]], one_minus, w));
       }
@@ -384,8 +386,8 @@ __attribute__((target_clones("fma", "default"))) static void unorm8_band(
 // The CUDA FP32 tile raster, pixel by pixel: per (splat, 16-pixel grid cell)
 // the local offsets ox, oy and s^2; per pixel local = (ax*lx + ay*ly + ox,
 // bx*lx + by*ly + oy) in pixel coordinates relative to the cell corner,
-// coverage r^2 <= s^2 and w > 1/256, C += premult * (g T), T *= 1 - w, stop
-// once T < 1e-4.
+// coverage r^2 <= s^2 and w = alpha e^(-4.5 r^2) > 1/256, C += rgb * (w T),
+// T -= w T, stop once T < 1e-4.
 __attribute__((target_clones("fma", "default"))) static void tiles_fp32_band(
     const OrcRecord *records, const uint32_t *ranges, const uint32_t *sorted_ids, uint32_t width,
     uint32_t tile, uint32_t tiles_x, uint8_t *rgba, uint32_t ya, uint32_t yb) {
@@ -409,14 +411,13 @@ __attribute__((target_clones("fma", "default"))) static void tiles_fp32_band(
         float ly = std::fma(r.bx, fx, std::fma(r.by, fy, oy));
         float r2 = std::fma(lx, lx, ly * ly);
         if (!(r2 <= s2)) continue;
-        float g = gauss_weight(r2);
-        float w = r.alpha * g;
+        float w = blend_weight(r2, r.log2a);
         if (!(w > 1.0f / 256.0f)) continue;
-        float gT = g * T;
-        c[0] = std::fma(r.pr, gT, c[0]);
-        c[1] = std::fma(r.pg, gT, c[1]);
-        c[2] = std::fma(r.pb, gT, c[2]);
-        T = T * (1.0f - w);
+        float wT = w * T;
+        c[0] = std::fma(r.cr, wT, c[0]);
+        c[1] = std::fma(r.cg, wT, c[1]);
+        c[2] = std::fma(r.cb, wT, c[2]);
+        T = T - wT;
         if (T < 1e-4f) break;
       }
       uint8_t *d = &rgba[((size_t)py * width + px) * 4];
