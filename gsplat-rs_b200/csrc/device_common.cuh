@@ -166,7 +166,7 @@ __device__ __forceinline__ float exp_neg(float x) {
 
 // alpha e^(-4.5 r2) for r2 in [0, 1], the FP32 raster's weight: one fma of
 // r2 by -4.5 log2(e) onto log2(alpha) and the hardware base-2 exponential
-// (ex2.approx, a few ulp; the argument lies in [-14.5, 0], so no subnormal is
+// (ex2.approx, a few ulp; the argument lies in [-8, 0] on covered pixels, so no subnormal is
 // involved). The CPU model of this raster evaluates 2^t with a degree-6
 // polynomial instead; the two images agree to the last UNORM8 step except
 // where a weight sits on the 1/256 threshold or a channel on a rounding

@@ -13,8 +13,9 @@
 // |local.x|, |local.y| <= s (the quad), r^2 = |local|^2 <= 1, and
 // w = alpha * exp(-4.5 r^2) > 1/256; the source is (premult rgb * g, w).
 //   FP32 mode: front to back (walks the list from its end); coverage is
-//     r^2 <= s^2 and w > 1/256 (in exact arithmetic the same set as the quad
-//     clip, r^2 <= 1 and the alpha threshold); C += rgb * (w T), T -= w T;
+//     r^2 <= s^2 and r^2 below the bound where w = 1/256 (in exact arithmetic
+//     the same set as the quad clip, r^2 <= 1 and the alpha threshold);
+//     C += rgb * (w T), T -= w T;
 //     a pixel finishes once T < 1e-4, a warp when all its pixels have, the
 //     block stops loading once all are done.
 //   UNORM8 mode: back to front, dst = src + dst * (1 - w) rounded to UNORM8
@@ -137,9 +138,9 @@ template <int kTile, int kChunk>
 struct Fp32Smem {
   static constexpr int kWarps = kTile * kTile / 32;
   float4 raw[2][3][kChunk];
-  float4 d0[kChunk];  // ax, ay, ox, s2
-  float4 d1[kChunk];  // bx, by, oy, alpha
-  float4 d2[kChunk];  // r*alpha, g*alpha, b*alpha, -
+  float4 d0[kChunk];  // ax, ay, ox, thr (coverage bound on r^2)
+  float4 d1[kChunk];  // bx, by, oy, -
+  float4 d2[kChunk];  // r, g, b, log2 alpha
   uint8_t mask[kChunk];
   uint16_t list[kWarps][kChunk];
   uint32_t view;
@@ -203,29 +204,34 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
       float ox = -fmaf(ra.z, cxa, ra.w * cya);
       float oy = -fmaf(rb.x, cxa, rb.y * cya);
       float cxl = ra.x - ftx, cyl = ra.y - fty;
-      sm.d0[tid] = make_float4(ra.z, ra.w, ox, rb.z * rb.z);
+      // w > 1/256 exactly when r2 < (log2 alpha + 8) / (4.5 log2 e), so a
+      // pixel is covered when r2 <= thr: the largest float below that bound,
+      // capped at s^2 (nothing is covered when the bound is not positive).
+      const float s2 = rb.z * rb.z;
+      const float wlim = __fdiv_rn(col.w + 8.0f, 6.49212768f);
+      const float thr = wlim > 0.0f ? fminf(s2, __int_as_float(__float_as_int(wlim) - 1)) : -1.0f;
+      sm.d0[tid] = make_float4(ra.z, ra.w, ox, thr);
       sm.d1[tid] = make_float4(rb.x, rb.y, oy, rb.w);
       sm.d2[tid] = col;
-      // Which 8x4 warp blocks the ellipse |local| <= s reaches: for each
+      // Which 8x4 warp blocks the ellipse |local|^2 <= thr reaches: for each
       // 4-row band, the x-interval the ellipse spans within the band (plus
       // half a pixel on every side), tested against the 8-column blocks.
       // q(dx, dy) = A dx^2 + 2B dx dy + C dy^2 is |local|^2 in pixel units.
       const float qa = fmaf(ra.z, ra.z, rb.x * rb.x);
       const float qb = fmaf(ra.z, ra.w, rb.x * rb.y);
       const float qc = fmaf(ra.w, ra.w, rb.y * rb.y);
-      const float s2 = rb.z * rb.z;
       const float det = fmaf(qa, qc, -qb * qb);
       // The mask only culls: hardware reciprocal/rsqrt (a few ulp) plus an
       // inflation of the extents far above their error keeps it conservative.
       const float inv_a = __fdividef(1.0f, qa);
       const float inv_det = __fdividef(1.0f, det);
-      const float hx2 = s2 * qc * inv_det, hy2 = s2 * qa * inv_det;
+      const float hx2 = thr * qc * inv_det, hy2 = thr * qa * inv_det;
       const float hx_raw = hx2 * rsqrtf(fmaxf(hx2, 1e-30f));
       const float hx = fmaf(hx_raw, 1.0001f, 1e-3f);
       const float hy = fmaf(hy2 * rsqrtf(fmaxf(hy2, 1e-30f)), 1.0001f, 1e-3f);
       // dy of the leftmost point (rightmost at -dy_left), from the unpadded extent
       const float dy_left = qb * hx_raw * __fdividef(1.0f, qc);
-      const float s2a = s2 * qa;
+      const float s2a = thr * qa;
       constexpr float kPad = 0.5f + 1.0f / 64.0f;
       uint32_t mask = 0;
 #pragma unroll
@@ -249,6 +255,7 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
       // A degenerate conic (never expected: axes are clamped to an
       // anisotropy of 64) falls back to every block.
       if (!(det > 0.0f) || !(hx < 3.0e38f) || !(hy < 3.0e38f)) mask = (1u << kWarps) - 1u;
+      if (!(thr >= 0.0f)) mask = 0;
       sm.mask[tid] = (uint8_t)mask;
     }
     __syncthreads();
@@ -262,16 +269,15 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
       n_w += __popc(bal);
     }
     __syncwarp();
-    // Two list entries per step (one early-out vote, one packed index
+    // Four list entries per step (one early-out vote, one packed index
     // load); each pixel still takes them strictly in list order.
     // w = alpha e^(-4.5 r2) = 2^(log2 alpha - 4.5 log2(e) r2) (the entry's
     // log2 alpha in its colour's w), so the colour takes rgb * (w T) and the
     // transmittance loses w T.
-    auto blend = [&](uint32_t j, float r2, float s2) {
-      if (done || !(r2 <= s2)) return;
+    auto blend = [&](uint32_t j, float r2, float thr) {
+      if (done || !(r2 <= thr)) return;
       const float4 col = sm.d2[j];
       const float w = blend_weight(r2, col.w);
-      if (!(w > 1.0f / 256.0f)) return;
       const float wT = w * T;
       c0 = fmaf(col.x, wT, c0);
       c1 = fmaf(col.y, wT, c1);
@@ -288,17 +294,22 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
       return fmaf(lx, lx, ly * ly);
     };
     uint32_t i = 0;
-    for (; i + 1 < n_w; i += 2) {
+    for (; i + 3 < n_w; i += 4) {
       if (__all_sync(0xffffffffu, done)) break;
-      const uint32_t jj = *reinterpret_cast<const uint32_t *>(&sm.list[warp][i]);
-      const uint32_t ja = jj & 0xffffu, jb = jj >> 16;
-      float sa, sb;
+      const uint2 jj = *reinterpret_cast<const uint2 *>(&sm.list[warp][i]);
+      const uint32_t ja = jj.x & 0xffffu, jb = jj.x >> 16, jc = jj.y & 0xffffu, jd = jj.y >> 16;
+      float sa, sb, sc, sd;
       const float r2a = local_r2(ja, sa);
       const float r2b = local_r2(jb, sb);
+      const float r2c = local_r2(jc, sc);
+      const float r2d = local_r2(jd, sd);
       blend(ja, r2a, sa);
       blend(jb, r2b, sb);
+      blend(jc, r2c, sc);
+      blend(jd, r2d, sd);
     }
-    if (i < n_w && !__all_sync(0xffffffffu, done)) {
+    for (; i < n_w; ++i) {
+      if (__all_sync(0xffffffffu, done)) break;
       const uint32_t ja = sm.list[warp][i];
       float sa;
       const float r2a = local_r2(ja, sa);

@@ -386,8 +386,8 @@ __attribute__((target_clones("fma", "default"))) static void unorm8_band(
 // The CUDA FP32 tile raster, pixel by pixel: per (splat, 16-pixel grid cell)
 // the local offsets ox, oy and s^2; per pixel local = (ax*lx + ay*ly + ox,
 // bx*lx + by*ly + oy) in pixel coordinates relative to the cell corner,
-// coverage r^2 <= s^2 and w = alpha e^(-4.5 r^2) > 1/256, C += rgb * (w T),
-// T -= w T, stop once T < 1e-4.
+// coverage r^2 <= s^2 and w = alpha e^(-4.5 r^2) > 1/256 (the latter as a
+// bound on r^2), C += rgb * (w T), T -= w T, stop once T < 1e-4.
 __attribute__((target_clones("fma", "default"))) static void tiles_fp32_band(
     const OrcRecord *records, const uint32_t *ranges, const uint32_t *sorted_ids, uint32_t width,
     uint32_t tile, uint32_t tiles_x, uint8_t *rgba, uint32_t ya, uint32_t yb) {
@@ -407,12 +407,15 @@ __attribute__((target_clones("fma", "default"))) static void tiles_fp32_band(
         float ox = -std::fma(r.ax, cxl, r.ay * cyl);
         float oy = -std::fma(r.bx, cxl, r.by * cyl);
         float s2 = r.s * r.s;
+        // w > 1/256 exactly when r2 < (log2 alpha + 8) / (4.5 log2 e): covered
+        // when r2 <= the largest float below that bound, capped at s^2
+        float wlim = (r.log2a + 8.0f) / 6.49212768f;
+        float thr = wlim > 0.0f ? std::fmin(s2, std::nextafterf(wlim, 0.0f)) : -1.0f;
         float lx = std::fma(r.ax, fx, std::fma(r.ay, fy, ox));
         float ly = std::fma(r.bx, fx, std::fma(r.by, fy, oy));
         float r2 = std::fma(lx, lx, ly * ly);
-        if (!(r2 <= s2)) continue;
+        if (!(r2 <= thr)) continue;
         float w = blend_weight(r2, r.log2a);
-        if (!(w > 1.0f / 256.0f)) continue;
         float wT = w * T;
         c[0] = std::fma(r.cr, wT, c[0]);
         c[1] = std::fma(r.cg, wT, c[1]);
