@@ -10,7 +10,7 @@
 //   3. one kernel per pass: each block takes the next tile of 256*IPT keys
 //      from an atomic ticket (launch order, so look-back never waits on a
 //      block that has not started), ranks its keys stably per digit with warp
-//      match votes, publishes its digit counts, resolves its global digit
+//      ballots, publishes its digit counts, resolves its global digit
 //      offsets by decoupled look-back over the predecessor tiles (bounded
 //      waits), reorders the tile in shared memory and writes digit runs
 //      contiguously.
@@ -176,13 +176,21 @@ __device__ __forceinline__ void pass_tile(const SortPlan *__restrict__ plan, uin
     }
   }
   // Stable per-warp ranking: items are visited in position order
-  // (i outer, lane inner), peers with the same digit are found by match vote.
+  // (i outer, lane inner); the lanes holding the same digit are the AND of
+  // one ballot per digit bit (or its complement), a fixed 8 votes whatever
+  // the number of distinct digits in the warp.
   uint32_t *wh = s_warp_hist[warp];
   const uint32_t lt = lanemask_lt();
 #pragma unroll
   for (int i = 0; i < kIpt; ++i) {
     uint32_t d = (key[i] >> shift) & 255u;
-    uint32_t peers = __match_any_sync(0xffffffffu, d);
+    uint32_t peers = 0xffffffffu;
+#pragma unroll
+    for (int bit = 0; bit < 8; ++bit) {
+      const bool set = (d >> bit) & 1u;
+      const uint32_t bal = __ballot_sync(0xffffffffu, set);
+      peers &= set ? bal : ~bal;
+    }
     uint32_t before = wh[d];
     rank[i] = before + __popc(peers & lt);
     __syncwarp();
