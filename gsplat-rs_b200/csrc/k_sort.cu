@@ -163,16 +163,23 @@ __device__ __forceinline__ void pass_tile(const SortPlan *__restrict__ plan, uin
 
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t warp_base = base + warp * 32 * kIpt;
-  uint32_t key[kIpt], val[kIpt], rank[kIpt];
+  // Large tiles (16 keys per thread) place their keys in shared memory
+  // before the look-back and read the values from global memory only then,
+  // which keeps keys, ranks and values from being live at once (fewer
+  // registers and spills); small tiles load the values with the keys and
+  // place both after the look-back (their look-back is short, and the
+  // value loads stay off the critical path).
+  constexpr bool kEarlyReorder = kIpt >= 16;
+  uint32_t key[kIpt], val[kEarlyReorder ? 1 : kIpt], rank[kIpt];
 #pragma unroll
   for (int i = 0; i < kIpt; ++i) {
     uint32_t idx = warp_base + i * 32 + lane;
     if (idx < n) {
       key[i] = in_k[idx];
-      val[i] = in_v[idx];
+      if constexpr (!kEarlyReorder) val[i] = in_v[idx];
     } else {
       key[i] = 0xffffffffu;  // ranks after every real key of digit 255
-      val[i] = 0;
+      if constexpr (!kEarlyReorder) val[i] = 0;
     }
   }
   // Stable per-warp ranking: items are visited in position order
@@ -212,6 +219,17 @@ __device__ __forceinline__ void pass_tile(const SortPlan *__restrict__ plan, uin
   st_relaxed_u32(&my_status[d], (tile == 0 ? kFlagP : kFlagA) | block_count);
   uint32_t total;
   s_block_start[d] = block_exclusive_scan(block_count, sm.wsum, total);
+  if constexpr (kEarlyReorder) {
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kIpt; ++i) {
+      uint32_t idx = warp_base + i * 32 + lane;
+      uint32_t dg = (key[i] >> shift) & 255u;
+      uint32_t pos = s_block_start[dg] + s_warp_hist[warp][dg] + rank[i];
+      s_keys[pos] = key[i];
+      s_vals[pos] = idx < n ? in_v[idx] : 0u;
+    }
+  }
 
   // Look back over the predecessor tiles, kLookback status words per step:
   // add aggregates until the nearest inclusive prefix; restart a step when
@@ -256,15 +274,17 @@ __device__ __forceinline__ void pass_tile(const SortPlan *__restrict__ plan, uin
   s_global[d] = plan->digit_offset[pass][d] + exclusive;
   __syncthreads();
 
-  // Reorder the tile by digit in shared memory.
+  // Reorder the tile by digit in shared memory (small tiles).
+  if constexpr (!kEarlyReorder) {
 #pragma unroll
-  for (int i = 0; i < kIpt; ++i) {
-    uint32_t dg = (key[i] >> shift) & 255u;
-    uint32_t pos = s_block_start[dg] + s_warp_hist[warp][dg] + rank[i];
-    s_keys[pos] = key[i];
-    s_vals[pos] = val[i];
+    for (int i = 0; i < kIpt; ++i) {
+      uint32_t dg = (key[i] >> shift) & 255u;
+      uint32_t pos = s_block_start[dg] + s_warp_hist[warp][dg] + rank[i];
+      s_keys[pos] = key[i];
+      s_vals[pos] = val[i];
+    }
+    __syncthreads();
   }
-  __syncthreads();
   // Each digit run lands contiguously in the output.
 #pragma unroll 4
   for (uint32_t s = threadIdx.x; s < kTile; s += kThreads) {
