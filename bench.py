@@ -393,6 +393,15 @@ def measure_served(ffi, rates, seconds, max_requests):
         for rid in warm:
             srv.wait(rid)
             srv.release(rid)
+    # ... and single requests, one at a time, twice for every (scene, size):
+    # a light load runs one-view batches, whose launch graphs the lanes
+    # capture on a layout's second run, as a server in steady state has.
+    for _ in range(2):
+        for sid in range(len(scenes)):
+            for w, h in gsplat_scenes.RESOLUTIONS:
+                rid = srv.submit(sid, cam0, w, h)
+                srv.wait(rid)
+                srv.release(rid)
     out = []
     for rate in rates:
         count = int(min(max_requests, max(50, rate * seconds)))

@@ -30,9 +30,13 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 // Tuning knobs: resident pass blocks per SM the register allocation must
-// allow, and predecessor tiles read per look-back step.
+// allow (for 8 keys per thread, and for the large tile), and predecessor
+// tiles read per look-back step.
 #ifndef GSR_SORT_MIN_BLOCKS
 #define GSR_SORT_MIN_BLOCKS 3
+#endif
+#ifndef GSR_SORT_MIN_BLOCKS_LARGE
+#define GSR_SORT_MIN_BLOCKS_LARGE GSR_SORT_MIN_BLOCKS
 #endif
 #ifndef GSR_LOOKBACK_WIDTH
 #define GSR_LOOKBACK_WIDTH 4
@@ -302,7 +306,7 @@ __device__ __forceinline__ void pass_tile(const SortPlan *__restrict__ plan, uin
 // (so look-back only ever waits on tiles already taken by running blocks)
 // until the item count, read on the device, is covered.
 template <int kIpt>
-__global__ void __launch_bounds__(kThreads, GSR_SORT_MIN_BLOCKS)
+__global__ void __launch_bounds__(kThreads, kIpt > 8 ? GSR_SORT_MIN_BLOCKS_LARGE : GSR_SORT_MIN_BLOCKS)
     pass_kernel(const SortPlan *__restrict__ plan, uint32_t pass, uint32_t shift, uint32_t *k0,
                 uint32_t *v0, uint32_t *k1, uint32_t *v1, uint32_t *status, uint32_t *ticket,
                 uint32_t *error) {
@@ -329,8 +333,10 @@ __global__ void __launch_bounds__(kThreads, GSR_SORT_MIN_BLOCKS)
 #ifndef GSR_SORT_IPT_LARGE
 #define GSR_SORT_IPT_LARGE 16
 #endif
+constexpr int kIptLarge = GSR_SORT_IPT_LARGE;
+static_assert(kIptLarge > 8, "the large tile must hold more keys per thread than the small one");
 inline uint32_t ipt_for(uint32_t capacity) {
-  return capacity <= (1u << 21) ? 8u : (uint32_t)GSR_SORT_IPT_LARGE;
+  return capacity <= (1u << 21) ? 8u : (uint32_t)kIptLarge;
 }
 inline uint32_t tiles_for(uint32_t capacity) {
   uint32_t tile = kThreads * ipt_for(capacity);
@@ -376,7 +382,8 @@ void launch_sort(const SortBuffers &b, cudaStream_t stream) {
     if (ipt == 8)
       hist_kernel<8><<<grid, kThreads, 0, stream>>>(b.keys0, b.count, b.begin_bit, b.passes, hist);
     else
-      hist_kernel<16><<<grid, kThreads, 0, stream>>>(b.keys0, b.count, b.begin_bit, b.passes, hist);
+      hist_kernel<kIptLarge>
+          <<<grid, kThreads, 0, stream>>>(b.keys0, b.count, b.begin_bit, b.passes, hist);
   }
   const uint32_t zero_blocks = std::min<uint32_t>(grid, 296);
   plan_kernel<<<zero_blocks, kThreads, 0, stream>>>(b.count, b.hist ? b.hist : hist, b.passes,
@@ -388,10 +395,10 @@ void launch_sort(const SortBuffers &b, cudaStream_t stream) {
       pass_kernel<8><<<g, kThreads, 0, stream>>>(b.plan, p, b.begin_bit + 8 * p, b.keys0, b.vals0,
                                                  b.keys1, b.vals1, st, tickets + p, b.error);
     } else {
-      const uint32_t g = std::min(grid, resident_pass_blocks<16>());
-      pass_kernel<16><<<g, kThreads, 0, stream>>>(b.plan, p, b.begin_bit + 8 * p, b.keys0,
-                                                  b.vals0, b.keys1, b.vals1, st, tickets + p,
-                                                  b.error);
+      const uint32_t g = std::min(grid, resident_pass_blocks<kIptLarge>());
+      pass_kernel<kIptLarge><<<g, kThreads, 0, stream>>>(b.plan, p, b.begin_bit + 8 * p, b.keys0,
+                                                         b.vals0, b.keys1, b.vals1, st,
+                                                         tickets + p, b.error);
     }
   }
 }
