@@ -135,8 +135,7 @@ Pipeline::~Pipeline() {
 
   if (counters_host_) cudaFreeHost(counters_host_);
   if (view_counters_pinned_) cudaFreeHost(view_counters_pinned_);
-  if (views_pinned_) cudaFreeHost(views_pinned_);
-  if (sets_pinned_) cudaFreeHost(sets_pinned_);
+  if (table_pinned_) cudaFreeHost(table_pinned_);
 }
 
 void Pipeline::record(int k) {
@@ -236,8 +235,9 @@ void Pipeline::ensure_workspace(const Layout &l) {
     const uint64_t o_k1 = off; off += align256(8 * k1_total);
     const uint64_t o_em = off; off += align256(8 * emit_words);
     view_zero_bytes_ = off;
-    const uint64_t o_tab = off; off += align256(sizeof(ViewDev) * vcap);
+    // the table: view sets, then views (one host-to-device copy per run)
     const uint64_t o_sets = off; off += align256(sizeof(ViewSetDev) * vcap);
+    const uint64_t o_tab = off; off += align256(sizeof(ViewDev) * vcap);
     view_ws_.reset(off);
     sets_dev_ = view_ws_.as<ViewSetDev>(o_sets);
     view_counters_ = view_ws_.as<ViewCounters>(o_vc);
@@ -245,20 +245,21 @@ void Pipeline::ensure_workspace(const Layout &l) {
     emit_status_ = view_ws_.as<unsigned long long>(o_em);
     views_dev_ = view_ws_.as<ViewDev>(o_tab);
     view_cap_ = vcap;
-    if (view_counters_pinned_cap_ < vcap) {
+    // a staging slot has the device table's layout (sets, then views at o_tab)
+    const uint64_t slot_bytes = off - o_sets;
+    if (view_counters_pinned_cap_ < vcap || table_slot_bytes_ != slot_bytes) {
       // in-flight runs may still read or write the pinned host arrays
       GSR_CUDA(cudaStreamSynchronize(stream_));
       if (view_counters_pinned_) cudaFreeHost(view_counters_pinned_);
-      if (views_pinned_) cudaFreeHost(views_pinned_);
-      if (sets_pinned_) cudaFreeHost(sets_pinned_);
+      if (table_pinned_) cudaFreeHost(table_pinned_);
       view_counters_pinned_ = nullptr;
-      views_pinned_ = nullptr;
-      sets_pinned_ = nullptr;
+      table_pinned_ = nullptr;
       GSR_CUDA(cudaMallocHost(&view_counters_pinned_, sizeof(ViewCounters) * vcap));
-      GSR_CUDA(cudaMallocHost(&views_pinned_, sizeof(ViewDev) * vcap * kViewSlots));
-      GSR_CUDA(cudaMallocHost(&sets_pinned_, sizeof(ViewSetDev) * vcap * kViewSlots));
+      GSR_CUDA(cudaMallocHost((void **)&table_pinned_, slot_bytes * kViewSlots));
       view_counters_pinned_cap_ = vcap;
+      table_slot_bytes_ = slot_bytes;
     }
+    table_sets_bytes_ = o_tab - o_sets;
     if (n > splat_cap_) {
       const uint64_t words = sort_work_words(ncap, 4);
       off = 0;
@@ -421,13 +422,10 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
   // layout); the slot's previous copy is long done in steady state.
   const uint32_t slot = slot_;
   GSR_CUDA(cudaEventSynchronize(slot_ev_[slot]));
-  ViewDev *staged = views_pinned_ + (uint64_t)slot * view_cap_;
-  std::memcpy(staged, views_host_.data(), sizeof(ViewDev) * l.views);
-  GSR_CUDA(cudaMemcpyAsync(views_dev_, staged, sizeof(ViewDev) * l.views, cudaMemcpyHostToDevice,
-                           stream_));
-  ViewSetDev *staged_sets = sets_pinned_ + (uint64_t)slot * view_cap_;
-  std::memcpy(staged_sets, sets_host_.data(), sizeof(ViewSetDev) * l.sets);
-  GSR_CUDA(cudaMemcpyAsync(sets_dev_, staged_sets, sizeof(ViewSetDev) * l.sets,
+  unsigned char *staged = table_pinned_ + (uint64_t)slot * table_slot_bytes_;
+  std::memcpy(staged, sets_host_.data(), sizeof(ViewSetDev) * l.sets);
+  std::memcpy(staged + table_sets_bytes_, views_host_.data(), sizeof(ViewDev) * l.views);
+  GSR_CUDA(cudaMemcpyAsync(sets_dev_, staged, table_sets_bytes_ + sizeof(ViewDev) * l.views,
                            cudaMemcpyHostToDevice, stream_));
   GSR_CUDA(cudaEventRecord(slot_ev_[slot], stream_));
   slot_ = (slot_ + 1) % kViewSlots;

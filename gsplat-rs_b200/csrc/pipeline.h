@@ -228,10 +228,13 @@ class Pipeline {
   ViewCounters *view_counters_pinned_ = nullptr;
   uint32_t view_counters_pinned_cap_ = 0;
   // Pinned staging ring for the view table: slot s is rewritten only after
-  // the copy that last read it has completed (slot_ev_[s]).
+  // the copy that last read it has completed (slot_ev_[s]). A slot mirrors
+  // the device table: the view sets (table_sets_bytes_) and then the views,
+  // so one copy moves both.
   static constexpr int kViewSlots = 4;
-  ViewDev *views_pinned_ = nullptr;
-  ViewSetDev *sets_pinned_ = nullptr;
+  unsigned char *table_pinned_ = nullptr;
+  uint64_t table_slot_bytes_ = 0;
+  uint64_t table_sets_bytes_ = 0;
   cudaEvent_t slot_ev_[kViewSlots] = {};
   bool last_device_sinks_ = false;
   int slot_ = 0;
