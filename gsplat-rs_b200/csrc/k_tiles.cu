@@ -341,6 +341,17 @@ __global__ void ranges_kernel(const SortPlan *__restrict__ plan, const uint32_t 
 __global__ void run_init_kernel(RunInit a) {
   const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  if (blockIdx.x == 0 && a.inline_views) {
+    static_assert(sizeof(ViewSetDev) % 4 == 0 && sizeof(ViewDev) % 4 == 0, "word copies");
+    const uint32_t sw = a.inline_sets * (uint32_t)(sizeof(ViewSetDev) / 4);
+    const uint32_t vw = a.inline_views * (uint32_t)(sizeof(ViewDev) / 4);
+    const uint32_t *ss = reinterpret_cast<const uint32_t *>(a.sets);
+    const uint32_t *vs = reinterpret_cast<const uint32_t *>(a.views);
+    uint32_t *sd = reinterpret_cast<uint32_t *>(a.sets_dst);
+    uint32_t *vd = reinterpret_cast<uint32_t *>(a.views_dst);
+    for (uint32_t i = threadIdx.x; i < sw; i += blockDim.x) sd[i] = ss[i];
+    for (uint32_t i = threadIdx.x; i < vw; i += blockDim.x) vd[i] = vs[i];
+  }
 #pragma unroll
   for (int r = 0; r < kRunZeroRegions; ++r)
     for (uint64_t i = t; i < a.zero_words[r]; i += stride) a.zero[r][i] = 0u;
@@ -383,6 +394,8 @@ void launch_ranges(const SortPlan *tile_plan, const uint32_t *keys0, const uint3
   ranges_kernel<<<blocks, 256, 0, stream>>>(tile_plan, keys0, keys1, counters, ranges, views,
                                             num_views, view_counters);
 }
+
+const void *run_init_kernel_entry() { return reinterpret_cast<const void *>(&run_init_kernel); }
 
 void launch_run_init(const RunInit &a, cudaStream_t stream) {
   uint64_t words = 0;

@@ -4,6 +4,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "device_types.h"
 #include "gsr_host.h"
 
 namespace gsr {
@@ -130,11 +131,24 @@ void launch_raster(const RasterArgs &a, uint32_t tile, uint32_t blend_mode,
 // issues no copy-engine work, so a caller's own host<->device copies never
 // queue in front of it).
 constexpr int kRunZeroRegions = 5;
+// Runs of up to kRunInlineViews views carry their view table in the
+// zeroing kernel's parameters, which writes it to the device table: no
+// host-to-device copy precedes the run (a replayed graph gets the new table
+// by a parameter update of that one kernel node).
+constexpr uint32_t kRunInlineViews = 8;
 struct RunInit {
   uint32_t *zero[kRunZeroRegions];       // regions zeroed at the start of a run
   uint64_t zero_words[kRunZeroRegions];
+  uint32_t inline_views = 0;  // 0: the table was copied to the device beforehand
+  uint32_t inline_sets = 0;
+  ViewSetDev *sets_dst = nullptr;
+  ViewDev *views_dst = nullptr;
+  ViewSetDev sets[kRunInlineViews];
+  ViewDev views[kRunInlineViews];
 };
 void launch_run_init(const RunInit &a, cudaStream_t stream);
+// The zeroing kernel's entry, to find its node in a captured graph.
+const void *run_init_kernel_entry();
 
 // ---- small helpers ----------------------------------------------------------
 void launch_fill_u32(uint32_t *dst, uint32_t value, uint64_t count, cudaStream_t stream);

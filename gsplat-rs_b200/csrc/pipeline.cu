@@ -159,7 +159,10 @@ void Pipeline::set_raster_config(const RasterConfig &c) {
 }
 
 void Pipeline::drop_graph() {
-  for (auto &g : graphs_) cudaGraphExecDestroy(g.exec);
+  for (auto &g : graphs_) {
+    cudaGraphExecDestroy(g.exec);
+    cudaGraphDestroy(g.graph);
+  }
   graphs_.clear();
   seen_keys_.clear();
 }
@@ -338,9 +341,7 @@ void Pipeline::ensure_key_workspace(uint64_t capacity) {
   debug_pairs_.reset(0);
 }
 
-void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &sinks,
-                          bool reuse, const ViewDev *views_dev, const ViewSetDev *sets_dev) {
-  const uint32_t n = std::max<uint32_t>(l.total_splats, 1);
+RunInit Pipeline::make_run_init(const Layout &l) const {
   RunInit init{};
   init.zero[0] = fixed_.as<uint32_t>();
   init.zero_words[0] = ((char *)depth_plan_ - (char *)fixed_.get()) / 4;
@@ -352,7 +353,21 @@ void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &si
   init.zero_words[3] = kSortScratchHeadWords;
   init.zero[4] = tile_sort_work_;
   init.zero_words[4] = kSortScratchHeadWords;
-  launch_run_init(init, stream_);
+  if (l.views <= kRunInlineViews) {
+    init.inline_views = l.views;
+    init.inline_sets = l.sets;
+    init.sets_dst = sets_dev_;
+    init.views_dst = views_dev_;
+    std::memcpy(init.sets, sets_host_.data(), sizeof(ViewSetDev) * l.sets);
+    std::memcpy(init.views, views_host_.data(), sizeof(ViewDev) * l.views);
+  }
+  return init;
+}
+
+void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &sinks,
+                          bool reuse, const ViewDev *views_dev, const ViewSetDev *sets_dev) {
+  const uint32_t n = std::max<uint32_t>(l.total_splats, 1);
+  launch_run_init(make_run_init(l), stream_);
   record(0);
 
   K1Buffers k1{vis_keys0_, vis_vals0_, rects_,         records_,
@@ -417,18 +432,22 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
   const bool reuse = reuse_request_ && sorted_valid_ && l == sorted_layout_ &&
                      std::equal(views, views + count, sorted_scenes_.begin(), sorted_scenes_.end(),
                                 [](const ViewSpec &v, const DeviceScene *s) { return v.scene == s; });
-  // The view table goes up from a pinned ring slot, ahead of the run on its
-  // stream (outside the run's graph, so the graph serves every frame of the
+  // A small view table rides in the zeroing kernel's parameters. A larger
+  // one goes up from a pinned ring slot, ahead of the run on its stream
+  // (outside the run's graph, so the graph serves every frame of the
   // layout); the slot's previous copy is long done in steady state.
-  const uint32_t slot = slot_;
-  GSR_CUDA(cudaEventSynchronize(slot_ev_[slot]));
-  unsigned char *staged = table_pinned_ + (uint64_t)slot * table_slot_bytes_;
-  std::memcpy(staged, sets_host_.data(), sizeof(ViewSetDev) * l.sets);
-  std::memcpy(staged + table_sets_bytes_, views_host_.data(), sizeof(ViewDev) * l.views);
-  GSR_CUDA(cudaMemcpyAsync(sets_dev_, staged, table_sets_bytes_ + sizeof(ViewDev) * l.views,
-                           cudaMemcpyHostToDevice, stream_));
-  GSR_CUDA(cudaEventRecord(slot_ev_[slot], stream_));
-  slot_ = (slot_ + 1) % kViewSlots;
+  const bool inline_table = l.views <= kRunInlineViews;
+  if (!inline_table) {
+    const uint32_t slot = slot_;
+    GSR_CUDA(cudaEventSynchronize(slot_ev_[slot]));
+    unsigned char *staged = table_pinned_ + (uint64_t)slot * table_slot_bytes_;
+    std::memcpy(staged, sets_host_.data(), sizeof(ViewSetDev) * l.sets);
+    std::memcpy(staged + table_sets_bytes_, views_host_.data(), sizeof(ViewDev) * l.views);
+    GSR_CUDA(cudaMemcpyAsync(sets_dev_, staged, table_sets_bytes_ + sizeof(ViewDev) * l.views,
+                             cudaMemcpyHostToDevice, stream_));
+    GSR_CUDA(cudaEventRecord(slot_ev_[slot], stream_));
+    slot_ = (slot_ + 1) % kViewSlots;
+  }
   ViewDev *run_views = views_dev_;
   ViewSetDev *run_sets = sets_dev_;
 
@@ -461,6 +480,7 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
                                       return a.last_use < b.last_use;
                                     });
         cudaGraphExecDestroy(lru->exec);
+        cudaGraphDestroy(lru->graph);
         graphs_.erase(lru);
       }
       cudaGraph_t g = nullptr;
@@ -479,15 +499,47 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
       GSR_CUDA(cudaStreamEndCapture(stream_, &g));
       cudaGraphExec_t exec = nullptr;
       cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
-      cudaGraphDestroy(g);
-      if (e != cudaSuccess)
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
         throw Error(Code::Internal, std::string("CUDA graph instantiation failed: ") +
                                         cudaGetErrorString(e));
-      graphs_.push_back(GraphEntry{key, exec, 0});
+      }
+      GraphEntry entry{key, exec, 0, g, nullptr, {}};
+      size_t count = 0;
+      GSR_CUDA(cudaGraphGetNodes(g, nullptr, &count));
+      std::vector<cudaGraphNode_t> nodes(count);
+      GSR_CUDA(cudaGraphGetNodes(g, nodes.data(), &count));
+      for (cudaGraphNode_t node : nodes) {
+        cudaGraphNodeType type;
+        GSR_CUDA(cudaGraphNodeGetType(node, &type));
+        if (type != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp{};
+        GSR_CUDA(cudaGraphKernelNodeGetParams(node, &kp));
+        if (kp.func == run_init_kernel_entry()) {
+          entry.init_node = node;
+          entry.init_params = kp;
+          break;
+        }
+      }
+      if (inline_table && !entry.init_node) {
+        cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(g);
+        throw Error(Code::Internal, "captured run has no zeroing kernel node");
+      }
+      graphs_.push_back(entry);
       hit = &graphs_.back();
     }
     if (hit) {
       hit->last_use = ++graph_clock_;
+      if (inline_table) {
+        // this run's view table, in the zeroing node's parameters
+        RunInit init = make_run_init(l);
+        void *args[] = {&init};
+        cudaKernelNodeParams kp = hit->init_params;
+        kp.kernelParams = args;
+        kp.extra = nullptr;
+        GSR_CUDA(cudaGraphExecKernelNodeSetParams(hit->exec, hit->init_node, &kp));
+      }
       GSR_CUDA(cudaGraphLaunch(hit->exec, stream_));
     }
   }

@@ -179,6 +179,9 @@ class Pipeline {
   void collect(RunResult &r);
   SortPlan read_plan(int which);
   void drop_graph();
+  // The zeroing kernel's parameters for a run of layout l (with the view
+  // table inline when the layout is small enough).
+  RunInit make_run_init(const Layout &l) const;
   void record(int k);  // phase event k (a graph node while capturing)
 
   int device_;
@@ -260,6 +263,9 @@ class Pipeline {
     GraphKey key;
     cudaGraphExec_t exec;
     uint64_t last_use;
+    cudaGraph_t graph;             // kept: its zeroing node takes parameter updates
+    cudaGraphNode_t init_node;     // the zeroing kernel (null if not found)
+    cudaKernelNodeParams init_params;
   };
   static constexpr size_t kGraphCacheSize = 64;
   std::vector<GraphEntry> graphs_;
