@@ -199,3 +199,23 @@ def test_batch_autotune_and_cache(tmp_path):
         b.render(views)
         for k in range(len(views)):
             assert np.array_equal(b.readback_rgba8(k), before[k]), k
+
+
+@pytest.mark.parametrize("count", [1, 8, 9])
+def test_view_table_inline_and_copied_over_graph_replays(count):
+    """Runs of up to 8 views carry the view table in the first kernel's
+    parameters (a replayed graph gets each run's table by a node update),
+    larger runs copy it to the device: over repeated runs of one layout (the
+    same scenes and sizes, so the graph is captured and replayed) with new
+    cameras each time, every view equals its plain render."""
+    scenes = _scenes()
+    rng = np.random.default_rng(40 + count)
+    layout = [(k % len(scenes), SIZES[k % len(SIZES)]) for k in range(count)]
+    with ffi.Batch() as b:
+        for s in scenes:
+            b.add_scene(s)
+        for _ in range(4):
+            views = [(sid, gsplat_scenes.orbit_camera(rng, (3.0, 7.0)), w, h)
+                     for sid, (w, h) in layout]
+            b.render(views)
+            _check_against_plain(b, scenes, views)
