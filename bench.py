@@ -367,7 +367,9 @@ def measure_served(ffi, rates, seconds, max_requests):
     import torch
 
     scenes = gsplat_scenes.config5_scenes()
-    srv = ffi.Server(lanes=2, max_views=256, work_budget=64 << 30)
+    # 4 GiB of pinned result memory reserved up front: pinning on demand under
+    # load stalls the request loop for tens of milliseconds per 64 MiB slab
+    srv = ffi.Server(lanes=2, max_views=256, work_budget=64 << 30, result_pool_mib=4096)
     for sc in scenes:
         srv.add_scene(sc)
     # The plain call gets its best case: one context per (scene, size), so no
@@ -451,6 +453,8 @@ def measure_served(ffi, rates, seconds, max_requests):
                     "mean_batch_views": st.mean_batch_views, "batches": int(st.batches),
                     "reruns": int(st.reruns), "peak_admitted_gb": st.peak_admitted_bytes / 1e9,
                     "device_ms": st.device_ms, "host_launch_ms": st.launch_ms,
+                    "graph_captures": int(st.graph_captures), "capture_ms": st.capture_ms,
+                    "pinned_slabs": int(st.pinned_slabs), "pinned_alloc_ms": st.pinned_alloc_ms,
                     "plain_views_per_s": count / plain_span,
                     "plain_capacity_views_per_s": count / busy,
                     "plain_p50_ms": float(lat[int(math.ceil(0.5 * len(lat))) - 1]),

@@ -865,8 +865,7 @@ int32_t gsplat_server_create(const GsplatServeConfig *config, GsplatServer **out
     *out_server = nullptr;
     gsr::ServeConfig c;
     if (config) {
-      if (config->reserved != 0)
-        return fail(Code::InvalidArgument, "gsplat_server_create: reserved field must be 0");
+      c.result_pool_mib = config->result_pool_mib;
       if (config->scene_budget_bytes) c.scene_budget = config->scene_budget_bytes;
       if (config->work_budget_bytes) c.work_budget = config->work_budget_bytes;
       if (config->lanes) c.lanes = config->lanes;
@@ -992,7 +991,8 @@ int32_t gsplat_server_get_stats(GsplatServer *server, GsplatServeStats *out_stat
     *out_stats = GsplatServeStats{s.submitted, s.completed, s.failed, s.batches, s.reruns,
                                   s.peak_admitted_bytes, s.p50_ms, s.p99_ms, s.mean_ms, s.max_ms,
                                   s.views_per_s, s.mean_batch_views, s.device_ms, s.launch_ms,
-                                  s.retire_ms};
+                                  s.retire_ms, s.graph_captures, s.pinned_slabs, s.capture_ms,
+                                  s.pinned_alloc_ms};
     return ok();
   });
 }

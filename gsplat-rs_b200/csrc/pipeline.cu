@@ -484,6 +484,7 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
         graphs_.erase(lru);
       }
       cudaGraph_t g = nullptr;
+      const auto t_capture = std::chrono::steady_clock::now();
       GSR_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
       capturing_ = true;
       try {
@@ -528,6 +529,11 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
       }
       graphs_.push_back(entry);
       hit = &graphs_.back();
+      captures_.fetch_add(1, std::memory_order_relaxed);
+      const double ms = std::chrono::duration<double, std::milli>(
+                            std::chrono::steady_clock::now() - t_capture).count();
+      capture_ms_.store(capture_ms_.load(std::memory_order_relaxed) + ms,
+                        std::memory_order_relaxed);
     }
     if (hit) {
       hit->last_use = ++graph_clock_;

@@ -2,6 +2,8 @@
 // K1 -> depth sort -> K2 -> tile sort -> ranges -> K4 on one CUDA stream.
 #pragma once
 
+#include <atomic>
+
 #include <cstdint>
 #include <cuda_runtime.h>
 #include <functional>
@@ -182,6 +184,16 @@ class Pipeline {
   // The zeroing kernel's parameters for a run of layout l (with the view
   // table inline when the layout is small enough).
   RunInit make_run_init(const Layout &l) const;
+
+ public:
+  // Launch graphs captured so far and the host milliseconds spent capturing
+  // and instantiating them (readable from any thread).
+  uint64_t graph_captures() const { return captures_.load(std::memory_order_relaxed); }
+  double capture_ms() const { return capture_ms_.load(std::memory_order_relaxed); }
+
+ private:
+  std::atomic<uint64_t> captures_{0};
+  std::atomic<double> capture_ms_{0.0};
   void record(int k);  // phase event k (a graph node while capturing)
 
   int device_;

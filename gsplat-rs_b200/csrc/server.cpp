@@ -20,31 +20,111 @@ double now_ms() {
 
 // ---- PinnedPool --------------------------------------------------------------
 
+PinnedPool::PinnedPool() : thread_([this] { grower(); }) {}
+
 PinnedPool::~PinnedPool() {
+  {
+    std::lock_guard<std::mutex> g(mu_);
+    stop_ = true;
+  }
+  cv_.notify_all();
+  thread_.join();
   for (uint8_t *p : slabs_) cudaFreeHost(p);
+}
+
+// One slab of buffers of `bytes` (portable pinned memory: any device's
+// context can copy into it). The buffers go to the free list, except the
+// first when the caller keeps it.
+uint8_t *PinnedPool::allocate_slab(uint64_t bytes, bool keep_one) {
+  const uint64_t stride = (bytes + 255) & ~uint64_t(255);
+  {
+    // a reserved slab first, when the size fits one
+    std::lock_guard<std::mutex> g(mu_);
+    const uint64_t fit = std::min<uint64_t>(64, kSlabBytes / stride);
+    if (fit > 0 && !raw_.empty()) {
+      uint8_t *slab = raw_.back();
+      raw_.pop_back();
+      auto &list = free_[bytes];
+      for (uint64_t k = keep_one ? 1 : 0; k < fit; ++k) list.push_back(slab + k * stride);
+      return keep_one ? slab : nullptr;
+    }
+  }
+  const uint64_t count = std::max<uint64_t>(1, std::min<uint64_t>(64, (kSlabBytes + stride - 1) / stride));
+  void *slab = nullptr;
+  GSR_CUDA(cudaHostAlloc(&slab, stride * count, cudaHostAllocPortable));
+  std::lock_guard<std::mutex> g(mu_);
+  slabs_.push_back((uint8_t *)slab);
+  auto &list = free_[bytes];
+  for (uint64_t k = keep_one ? 1 : 0; k < count; ++k) list.push_back((uint8_t *)slab + k * stride);
+  return keep_one ? (uint8_t *)slab : nullptr;
+}
+
+void PinnedPool::grower() {
+  std::unique_lock<std::mutex> lk(mu_);
+  for (;;) {
+    cv_.wait(lk, [&] { return stop_ || !wanted_.empty(); });
+    if (stop_) return;
+    const uint64_t bytes = wanted_.front();
+    wanted_.pop_front();
+    const int device = device_;
+    lk.unlock();
+    bool ok = true;
+    try {
+      if (device >= 0) GSR_CUDA(cudaSetDevice(device));
+      allocate_slab(bytes, false);
+    } catch (const Error &) {
+      ok = false;  // out of pinned memory: take() allocates (and reports) on demand
+    }
+    lk.lock();
+    // still short of the low-water mark (demand outran the slab): go on
+    if (ok && !stop_ && free_[bytes].size() < kLowWater) wanted_.push_back(bytes);
+    else growing_[bytes] = false;
+  }
 }
 
 uint8_t *PinnedPool::take(uint64_t bytes) {
   {
     std::lock_guard<std::mutex> g(mu_);
-    auto it = free_.find(bytes);
-    if (it != free_.end() && !it->second.empty()) {
-      uint8_t *p = it->second.back();
-      it->second.pop_back();
+    auto &list = free_[bytes];
+    if (!list.empty()) {
+      uint8_t *p = list.back();
+      list.pop_back();
+      if (list.size() < kLowWater && !growing_[bytes]) {
+        growing_[bytes] = true;
+        wanted_.push_back(bytes);
+        cv_.notify_one();
+      }
       return p;
     }
   }
-  // Pinned allocations are slow (milliseconds): allocate a slab of many
-  // buffers of this size at once and hand out the rest later.
-  const uint64_t stride = (bytes + 255) & ~uint64_t(255);
-  const uint64_t count = std::max<uint64_t>(1, std::min<uint64_t>(64, (kSlabBytes + stride - 1) / stride));
-  void *slab = nullptr;
-  GSR_CUDA(cudaMallocHost(&slab, stride * count));
+  // No free buffer of this size: allocate a slab here and keep one buffer.
+  const double t0 = now_ms();
+  uint8_t *p = allocate_slab(bytes, true);
+  const double t1 = now_ms();
   std::lock_guard<std::mutex> g(mu_);
-  slabs_.push_back((uint8_t *)slab);
-  auto &list = free_[bytes];
-  for (uint64_t k = 1; k < count; ++k) list.push_back((uint8_t *)slab + k * stride);
-  return (uint8_t *)slab;
+  wait_ms_ += t1 - t0;
+  return p;
+}
+
+void PinnedPool::reserve(uint64_t bytes) {
+  for (uint64_t k = 0; k < (bytes + kSlabBytes - 1) / kSlabBytes; ++k) {
+    void *slab = nullptr;
+    GSR_CUDA(cudaHostAlloc(&slab, kSlabBytes, cudaHostAllocPortable));
+    std::lock_guard<std::mutex> g(mu_);
+    slabs_.push_back((uint8_t *)slab);
+    raw_.push_back((uint8_t *)slab);
+  }
+}
+
+void PinnedPool::set_device(int device) {
+  std::lock_guard<std::mutex> g(mu_);
+  device_ = device;
+}
+
+void PinnedPool::allocations(uint64_t &slabs, double &wait_ms) {
+  std::lock_guard<std::mutex> g(mu_);
+  slabs = slabs_.size();
+  wait_ms = wait_ms_;
 }
 
 void PinnedPool::give(uint8_t *p, uint64_t bytes) {
@@ -61,6 +141,8 @@ Server::Server(const ServeConfig &cfg) : cfg_(cfg), scenes_(cfg.scene_budget) {
     throw Error(Code::InvalidArgument, "max_views must be 1..1024");
   if (cfg.tile != 8 && cfg.tile != 16) throw Error(Code::InvalidArgument, "tile size must be 8 or 16");
   device_ = require_b200();
+  pool_.set_device(device_);
+  pool_.reserve((uint64_t)cfg.result_pool_mib << 20);
   GSR_CUDA(cudaStreamCreateWithFlags(&upload_stream_, cudaStreamNonBlocking));
   for (uint32_t k = 0; k < cfg.lanes; ++k) {
     auto ls = std::make_unique<LaneState>();
@@ -216,7 +298,25 @@ ServeStats Server::stats() {
   s.device_ms = device_ms_;
   s.launch_ms = launch_ms_;
   s.retire_ms = retire_ms_;
+  uint64_t captures = 0, slabs = 0;
+  double capture_ms = 0, alloc_ms = 0;
+  host_costs(captures, capture_ms, slabs, alloc_ms);
+  s.graph_captures = captures - base_captures_;
+  s.capture_ms = capture_ms - base_capture_ms_;
+  s.pinned_slabs = slabs - base_slabs_;
+  s.pinned_alloc_ms = alloc_ms - base_alloc_ms_;
   return s;
+}
+
+void Server::host_costs(uint64_t &captures, double &capture_ms, uint64_t &slabs,
+                        double &alloc_ms) {
+  captures = 0;
+  capture_ms = 0;
+  for (auto &ls : lanes_) {
+    captures += ls->lane->pipe().graph_captures();
+    capture_ms += ls->lane->pipe().capture_ms();
+  }
+  pool_.allocations(slabs, alloc_ms);
 }
 
 void Server::reset_stats() {
@@ -227,6 +327,7 @@ void Server::reset_stats() {
   first_submit_ = -1;
   last_done_ = 0;
   device_ms_ = launch_ms_ = retire_ms_ = 0;
+  host_costs(base_captures_, base_capture_ms_, base_slabs_, base_alloc_ms_);
 }
 
 uint64_t Server::view_bytes(const ViewSpec &s, uint64_t pairs) const {

@@ -33,6 +33,7 @@ struct ServeConfig {
   uint32_t max_views = 256;              // per batch
   uint32_t tile = 16;
   RasterConfig raster;  // chunk 0 = full tile
+  uint32_t result_pool_mib = 0;  // pinned result memory reserved at creation
 };
 
 enum class RequestStatus : uint32_t { Queued = 0, Running = 1, Done = 2, Failed = 3 };
@@ -56,21 +57,51 @@ struct ServeStats {
   double device_ms = 0;        // CUDA-event time of the batches' pipelines (sum)
   double launch_ms = 0;        // host time spent enqueuing batches (sum)
   double retire_ms = 0;        // host time spent retiring batches (sum)
+  uint64_t graph_captures = 0; // launch graphs the lanes captured
+  uint64_t pinned_slabs = 0;   // pinned result slabs allocated
+  double capture_ms = 0;       // host time in those captures (part of launch_ms)
+  double pinned_alloc_ms = 0;  // host time launches waited on pinned allocations (part of
+                               // launch_ms; slabs added in the background are not counted)
 };
 
 // Pinned host buffers recycled by size, carved from slabs of about 64 MB
-// (at most 64 buffers per slab).
+// (at most 64 buffers per slab). Pinning memory takes milliseconds per slab
+// (tens of milliseconds for 64 MB), so a background thread adds a slab for a
+// size whenever its free buffers fall below a low-water mark; take() only
+// allocates on the caller's thread when a size has no free buffer at all.
 class PinnedPool {
  public:
+  PinnedPool();
   ~PinnedPool();
+  PinnedPool(const PinnedPool &) = delete;
+  PinnedPool &operator=(const PinnedPool &) = delete;
   uint8_t *take(uint64_t bytes);
   void give(uint8_t *p, uint64_t bytes);
+  // slabs allocated so far, and the milliseconds take() callers spent
+  // waiting on allocations (the background thread's time is not counted)
+  void allocations(uint64_t &slabs, double &wait_ms);
+  // the device whose context the background thread allocates in
+  void set_device(int device);
+  // Pins `bytes` now (whole slabs), carved into buffers of whatever sizes
+  // are asked for later before any further allocation happens.
+  void reserve(uint64_t bytes);
 
  private:
   static constexpr uint64_t kSlabBytes = 64ull << 20;
+  static constexpr size_t kLowWater = 8;  // free buffers per size kept ahead of demand
+  uint8_t *allocate_slab(uint64_t bytes, bool keep_one);  // adds the rest to the free list
+  void grower();
   std::mutex mu_;
+  std::condition_variable cv_;
   std::map<uint64_t, std::vector<uint8_t *>> free_;
+  std::map<uint64_t, bool> growing_;  // a background slab for this size is pending
+  std::deque<uint64_t> wanted_;       // sizes for the background thread
   std::vector<uint8_t *> slabs_;
+  std::vector<uint8_t *> raw_;  // reserved slabs (kSlabBytes each), not yet carved
+  double wait_ms_ = 0;
+  int device_ = -1;
+  bool stop_ = false;
+  std::thread thread_;
 };
 
 class Server {
@@ -133,6 +164,10 @@ class Server {
   std::condition_variable done_cv_;  // request completions
   std::deque<uint64_t> queue_;
   std::unordered_map<uint64_t, Request> requests_;
+  // graph captures and pinned allocations over all lanes, so far
+  void host_costs(uint64_t &captures, double &capture_ms, uint64_t &slabs, double &alloc_ms);
+  uint64_t base_captures_ = 0, base_slabs_ = 0;  // at the last reset
+  double base_capture_ms_ = 0, base_alloc_ms_ = 0;
   std::vector<std::unique_ptr<LaneState>> lanes_;
   uint64_t next_id_ = 1;
   bool stop_ = false;

@@ -112,7 +112,7 @@ class GsplatServeConfig(ctypes.Structure):
     _fields_ = [("scene_budget_bytes", ctypes.c_uint64), ("work_budget_bytes", ctypes.c_uint64),
                 ("lanes", ctypes.c_uint32), ("max_views_per_batch", ctypes.c_uint32),
                 ("tile_size", ctypes.c_uint32), ("raster_chunk", ctypes.c_uint32),
-                ("raster_blocks_per_sm", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("raster_blocks_per_sm", ctypes.c_uint32), ("result_pool_mib", ctypes.c_uint32)]
 
 
 class GsplatTuneResult(ctypes.Structure):
@@ -137,7 +137,9 @@ class GsplatServeStats(ctypes.Structure):
                 ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
                 ("views_per_s", ctypes.c_double), ("mean_batch_views", ctypes.c_double),
                 ("device_ms", ctypes.c_double), ("launch_ms", ctypes.c_double),
-                ("retire_ms", ctypes.c_double)]
+                ("retire_ms", ctypes.c_double), ("graph_captures", ctypes.c_uint64),
+                ("pinned_slabs", ctypes.c_uint64), ("capture_ms", ctypes.c_double),
+                ("pinned_alloc_ms", ctypes.c_double)]
 
 
 REQUEST_QUEUED, REQUEST_RUNNING, REQUEST_DONE, REQUEST_FAILED = 0, 1, 2, 3
@@ -638,9 +640,9 @@ class Server:
     """One GsplatServer: resident scenes and a continuous-batching request loop."""
 
     def __init__(self, lanes=0, max_views=0, tile=0, scene_budget=0, work_budget=0,
-                 raster_chunk=0, raster_blocks_per_sm=0):
+                 raster_chunk=0, raster_blocks_per_sm=0, result_pool_mib=0):
         cfg = GsplatServeConfig(scene_budget, work_budget, lanes, max_views, tile, raster_chunk,
-                                raster_blocks_per_sm, 0)
+                                raster_blocks_per_sm, result_pool_mib)
         self.ptr = ctypes.c_void_p()
         check(lib().gsplat_server_create(ctypes.byref(cfg), ctypes.byref(self.ptr)))
         self.sizes = {}

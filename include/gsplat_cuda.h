@@ -331,7 +331,10 @@ typedef struct GsplatServeConfig {
   uint32_t tile_size;           /* 8 or 16; 0 = 16 */
   uint32_t raster_chunk;        /* as gsplat_context_set_raster_config; 0 = full tile */
   uint32_t raster_blocks_per_sm;/* 0 = one block per tile */
-  uint32_t reserved;            /* 0 */
+  uint32_t result_pool_mib;     /* pinned result memory reserved at creation, MiB; 0 = none
+                                   (pinning on demand stalls the request loop for tens of ms
+                                   per 64 MiB, so a server that must keep its latency under
+                                   load reserves what its outstanding results will hold) */
 } GsplatServeConfig;            /* 40 bytes */
 
 typedef enum GsplatRequestStatus {
@@ -361,7 +364,11 @@ typedef struct GsplatServeStats {
   double device_ms;          /* CUDA-event time of the batches' launch sequences, summed */
   double launch_ms;          /* host time spent enqueuing batches, summed */
   double retire_ms;          /* host time spent retiring batches, summed */
-} GsplatServeStats;          /* 120 bytes */
+  uint64_t graph_captures;   /* launch graphs the lanes captured */
+  uint64_t pinned_slabs;     /* pinned result slabs allocated (on demand or in the background) */
+  double capture_ms;         /* host time in those captures (part of launch_ms) */
+  double pinned_alloc_ms;    /* host time launches waited on allocations (part of launch_ms) */
+} GsplatServeStats;          /* 152 bytes */
 
 int32_t gsplat_server_create(const GsplatServeConfig *config, GsplatServer **out_server);
 /* Finishes the batches in flight, fails queued requests and frees everything. */

@@ -50,7 +50,7 @@ def test_abi_struct_sizes():
     assert ctypes.sizeof(ffi.GsplatServeConfig) == 40
     assert ctypes.sizeof(ffi.GsplatTuneResult) == 32
     assert ctypes.sizeof(ffi.GsplatRequestInfo) == 32
-    assert ctypes.sizeof(ffi.GsplatServeStats) == 120
+    assert ctypes.sizeof(ffi.GsplatServeStats) == 152
 
 
 def test_versions_defaults_and_messages(oracle):
@@ -126,11 +126,11 @@ def test_server_null_and_no_gpu_errors():
     rid = ctypes.c_uint64()
     assert L.gsplat_server_submit(None, None, ctypes.byref(rid)) == 1
     assert "server is null" in ffi.last_error()
-    cfg = ffi.GsplatServeConfig(0, 0, 0, 0, 0, 0, 0, 1)
+    cfg = ffi.GsplatServeConfig(0, 0, 9, 0, 0, 0, 0, 0)  # lanes must be 1..8
     out = ctypes.c_void_p(1)
     assert L.gsplat_server_create(ctypes.byref(cfg), ctypes.byref(out)) == 1
     assert not out.value
-    cfg.reserved = 0
+    cfg.lanes = 0
     rc = L.gsplat_server_create(ctypes.byref(cfg), ctypes.byref(out))
     if rc == 4:
         assert not out.value and "unavailable" in ffi.last_error()

@@ -167,3 +167,25 @@ def test_served_errors():
     with pytest.raises(ffi.GsplatError) as e:
         ffi.Server(lanes=9)
     assert e.value.code == ffi.INVALID_ARGUMENT
+
+
+def test_reserved_result_pool_serves_without_pinning_on_demand():
+    """A server created with a pinned result reserve carves its result
+    buffers from the reserved slabs: serving a stream allocates no further
+    pinned memory and no launch waits on an allocation, and the results are
+    still those of the plain render."""
+    scenes = _scenes()
+    reqs = _requests(3, 40, len(scenes))
+    with ffi.Server(lanes=2, max_views=16, result_pool_mib=256) as srv:
+        for s in scenes:
+            srv.add_scene(s)
+        ids = _submit_poisson(srv, reqs, rate=2000.0, seed=4)
+        infos = [srv.wait(i) for i in ids]
+        assert all(i.status == ffi.REQUEST_DONE for i in infos)
+        st = srv.stats()
+        assert st.pinned_slabs == 4  # 256 MiB of 64 MiB slabs, nothing more
+        assert st.pinned_alloc_ms < 5.0  # carving a reserved slab, no pinning
+        plain = _plain_images(scenes, reqs)
+        for k, rid in enumerate(ids):
+            assert np.array_equal(srv.read_rgba8(rid), plain[k][0]), f"request {k}"
+            srv.release(rid)
