@@ -391,7 +391,7 @@ def measure_served(ffi, rates, seconds, max_requests):
     # workspaces, pair predictions and pinned result pools to steady state.
     for burst in range(2):
         warm = [srv.submit(r["scene"], r["camera"], r["width"], r["height"])
-                for r in gsplat_scenes.config5_requests(900 + burst, 1e6, 128, len(scenes))]
+                for r in gsplat_scenes.config5_requests(900 + burst, 1e6, 256, len(scenes))]
         for rid in warm:
             srv.wait(rid)
             srv.release(rid)
