@@ -20,6 +20,7 @@ e2e: the same frames through the public C ABI from host memory: camera upload,
 """
 
 import argparse
+import gc
 import json
 import math
 import os
@@ -423,6 +424,10 @@ def measure_served(ffi, rates, seconds, max_requests):
                 k += 1
             done.set()
 
+        # no garbage-collector pause inside the timed arrival streams (the
+        # process holds the earlier sections' objects)
+        gc.collect()
+        gc.disable()
         th = threading.Thread(target=consumer)
         th.start()
         t0 = time.perf_counter()
@@ -446,8 +451,9 @@ def measure_served(ffi, rates, seconds, max_requests):
             te = time.perf_counter()
             busy += te - ts
             lat.append((te - (t0 + r["arrival_s"])) * 1000.0)
-        lat = np.sort(np.array(lat))
         plain_span = time.perf_counter() - t0
+        gc.enable()
+        lat = np.sort(np.array(lat))
         out.append({"offered_req_per_s": rate, "requests": count,
                     "views_per_s": st.views_per_s, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
                     "mean_batch_views": st.mean_batch_views, "batches": int(st.batches),
