@@ -461,6 +461,8 @@ def measure_served(ffi, rates, seconds, max_requests):
                     "device_ms": st.device_ms, "host_launch_ms": st.launch_ms,
                     "graph_captures": int(st.graph_captures), "capture_ms": st.capture_ms,
                     "pinned_slabs": int(st.pinned_slabs), "pinned_alloc_ms": st.pinned_alloc_ms,
+                    "workspace_regrowths": int(st.workspace_regrowths),
+                    "regrowth_ms": st.regrowth_ms,
                     "plain_views_per_s": count / plain_span,
                     "plain_capacity_views_per_s": count / busy,
                     "plain_p50_ms": float(lat[int(math.ceil(0.5 * len(lat))) - 1]),

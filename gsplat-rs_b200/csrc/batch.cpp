@@ -172,8 +172,11 @@ void Lane::enqueue(const std::vector<ViewSpec> &views, const std::vector<uint64_
   GSR_CUDA(cudaSetDevice(device_));
   const uint64_t need = 4 * std::max<uint64_t>(total_pixels, 1);
   if (images_.size() < need) {
+    const auto t_grow = std::chrono::steady_clock::now();
     GSR_CUDA(cudaStreamSynchronize(stream_));
     images_.reset(need + need / 4);
+    pipe_->note_regrowth(std::chrono::duration<double, std::milli>(
+                             std::chrono::steady_clock::now() - t_grow).count());
   }
   // pinned sinks: the pointers stay put while sizes fit, so the pipeline's
   // captured graphs keep matching

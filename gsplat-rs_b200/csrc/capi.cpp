@@ -992,7 +992,7 @@ int32_t gsplat_server_get_stats(GsplatServer *server, GsplatServeStats *out_stat
                                   s.peak_admitted_bytes, s.p50_ms, s.p99_ms, s.mean_ms, s.max_ms,
                                   s.views_per_s, s.mean_batch_views, s.device_ms, s.launch_ms,
                                   s.retire_ms, s.graph_captures, s.pinned_slabs, s.capture_ms,
-                                  s.pinned_alloc_ms};
+                                  s.pinned_alloc_ms, s.workspace_regrowths, s.regrowth_ms};
     return ok();
   });
 }

@@ -216,6 +216,7 @@ Pipeline::Layout Pipeline::plan_views(const ViewSpec *views, uint32_t count,
 void Pipeline::ensure_workspace(const Layout &l) {
   const uint32_t n = std::max<uint32_t>(l.total_splats, 1);
   if (l.views > view_cap_ || n > splat_cap_ || !view_ws_.get()) {
+    const auto t_grow = std::chrono::steady_clock::now();
     GSR_CUDA(cudaStreamSynchronize(stream_));  // earlier runs may still use the old buffers
     drop_graph();
     // Growth is geometric: a reallocation synchronises the device (cudaFree),
@@ -286,13 +287,18 @@ void Pipeline::ensure_workspace(const Layout &l) {
       splat_cap_ = ncap;
       projected_.reset(0);
     }
+    note_regrowth(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() -
+                                                            t_grow).count());
   }
   if (l.total_tiles > tile_cap_ || !tile_ws_.get()) {
+    const auto t_grow = std::chrono::steady_clock::now();
     GSR_CUDA(cudaStreamSynchronize(stream_));
     drop_graph();
     tile_cap_ = std::max(l.total_tiles, tile_cap_ + tile_cap_ / 2);
     tile_ws_.reset(align256(8ull * std::max<uint32_t>(tile_cap_, 1)));
     ranges_ = tile_ws_.as<uint2>();
+    note_regrowth(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() -
+                                                            t_grow).count());
   }
   if (key_cap_ == 0)
     ensure_key_workspace(std::min<uint64_t>(std::max<uint64_t>(kInitialPairsPerSplat * n, 1u << 20),
@@ -318,6 +324,7 @@ void Pipeline::ensure_key_workspace(uint64_t capacity) {
   if (capacity > kMaxSortItems)
     throw Error(Code::Unsupported, "tile pair count " + std::to_string(capacity) +
                                        " exceeds the renderer's limit of 2^30 - 1");
+  const auto t_grow = std::chrono::steady_clock::now();
   GSR_CUDA(cudaStreamSynchronize(stream_));
   drop_graph();
   // geometric growth, as for the other workspaces
@@ -339,6 +346,8 @@ void Pipeline::ensure_key_workspace(uint64_t capacity) {
   tile_sort_work_ = key_ws_.as<uint32_t>(o_work);
   key_cap_ = cap;
   debug_pairs_.reset(0);
+  note_regrowth(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() -
+                                                          t_grow).count());
 }
 
 RunInit Pipeline::make_run_init(const Layout &l) const {

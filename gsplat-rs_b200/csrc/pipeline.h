@@ -190,8 +190,19 @@ class Pipeline {
   // and instantiating them (readable from any thread).
   uint64_t graph_captures() const { return captures_.load(std::memory_order_relaxed); }
   double capture_ms() const { return capture_ms_.load(std::memory_order_relaxed); }
+  // Workspace reallocations so far (each waits for the device to go idle:
+  // cudaFree synchronises it) and the host milliseconds they took.
+  uint64_t workspace_regrowths() const { return regrowths_.load(std::memory_order_relaxed); }
+  double regrowth_ms() const { return regrowth_ms_.load(std::memory_order_relaxed); }
+  void note_regrowth(double ms) {
+    regrowths_.fetch_add(1, std::memory_order_relaxed);
+    regrowth_ms_.store(regrowth_ms_.load(std::memory_order_relaxed) + ms,
+                       std::memory_order_relaxed);
+  }
 
  private:
+  std::atomic<uint64_t> regrowths_{0};
+  std::atomic<double> regrowth_ms_{0.0};
   std::atomic<uint64_t> captures_{0};
   std::atomic<double> capture_ms_{0.0};
   void record(int k);  // phase event k (a graph node while capturing)

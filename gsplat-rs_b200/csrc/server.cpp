@@ -298,9 +298,11 @@ ServeStats Server::stats() {
   s.device_ms = device_ms_;
   s.launch_ms = launch_ms_;
   s.retire_ms = retire_ms_;
-  uint64_t captures = 0, slabs = 0;
-  double capture_ms = 0, alloc_ms = 0;
-  host_costs(captures, capture_ms, slabs, alloc_ms);
+  uint64_t captures = 0, slabs = 0, regrowths = 0;
+  double capture_ms = 0, alloc_ms = 0, regrowth_ms = 0;
+  host_costs(captures, capture_ms, slabs, alloc_ms, regrowths, regrowth_ms);
+  s.workspace_regrowths = regrowths - base_regrowths_;
+  s.regrowth_ms = regrowth_ms - base_regrowth_ms_;
   s.graph_captures = captures - base_captures_;
   s.capture_ms = capture_ms - base_capture_ms_;
   s.pinned_slabs = slabs - base_slabs_;
@@ -309,12 +311,16 @@ ServeStats Server::stats() {
 }
 
 void Server::host_costs(uint64_t &captures, double &capture_ms, uint64_t &slabs,
-                        double &alloc_ms) {
+                        double &alloc_ms, uint64_t &regrowths, double &regrowth_ms) {
   captures = 0;
   capture_ms = 0;
+  regrowths = 0;
+  regrowth_ms = 0;
   for (auto &ls : lanes_) {
     captures += ls->lane->pipe().graph_captures();
     capture_ms += ls->lane->pipe().capture_ms();
+    regrowths += ls->lane->pipe().workspace_regrowths();
+    regrowth_ms += ls->lane->pipe().regrowth_ms();
   }
   pool_.allocations(slabs, alloc_ms);
 }
@@ -327,7 +333,8 @@ void Server::reset_stats() {
   first_submit_ = -1;
   last_done_ = 0;
   device_ms_ = launch_ms_ = retire_ms_ = 0;
-  host_costs(base_captures_, base_capture_ms_, base_slabs_, base_alloc_ms_);
+  host_costs(base_captures_, base_capture_ms_, base_slabs_, base_alloc_ms_, base_regrowths_,
+             base_regrowth_ms_);
 }
 
 uint64_t Server::view_bytes(const ViewSpec &s, uint64_t pairs) const {

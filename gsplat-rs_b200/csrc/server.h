@@ -62,6 +62,8 @@ struct ServeStats {
   double capture_ms = 0;       // host time in those captures (part of launch_ms)
   double pinned_alloc_ms = 0;  // host time launches waited on pinned allocations (part of
                                // launch_ms; slabs added in the background are not counted)
+  uint64_t workspace_regrowths = 0;  // lane workspace reallocations
+  double regrowth_ms = 0;            // host time in them (part of launch_ms)
 };
 
 // Pinned host buffers recycled by size, carved from slabs of about 64 MB
@@ -165,9 +167,10 @@ class Server {
   std::deque<uint64_t> queue_;
   std::unordered_map<uint64_t, Request> requests_;
   // graph captures and pinned allocations over all lanes, so far
-  void host_costs(uint64_t &captures, double &capture_ms, uint64_t &slabs, double &alloc_ms);
-  uint64_t base_captures_ = 0, base_slabs_ = 0;  // at the last reset
-  double base_capture_ms_ = 0, base_alloc_ms_ = 0;
+  void host_costs(uint64_t &captures, double &capture_ms, uint64_t &slabs, double &alloc_ms,
+                  uint64_t &regrowths, double &regrowth_ms);
+  uint64_t base_captures_ = 0, base_slabs_ = 0, base_regrowths_ = 0;  // at the last reset
+  double base_capture_ms_ = 0, base_alloc_ms_ = 0, base_regrowth_ms_ = 0;
   std::vector<std::unique_ptr<LaneState>> lanes_;
   uint64_t next_id_ = 1;
   bool stop_ = false;

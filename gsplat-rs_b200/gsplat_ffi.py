@@ -139,7 +139,8 @@ class GsplatServeStats(ctypes.Structure):
                 ("device_ms", ctypes.c_double), ("launch_ms", ctypes.c_double),
                 ("retire_ms", ctypes.c_double), ("graph_captures", ctypes.c_uint64),
                 ("pinned_slabs", ctypes.c_uint64), ("capture_ms", ctypes.c_double),
-                ("pinned_alloc_ms", ctypes.c_double)]
+                ("pinned_alloc_ms", ctypes.c_double), ("workspace_regrowths", ctypes.c_uint64),
+                ("regrowth_ms", ctypes.c_double)]
 
 
 REQUEST_QUEUED, REQUEST_RUNNING, REQUEST_DONE, REQUEST_FAILED = 0, 1, 2, 3

@@ -368,7 +368,9 @@ typedef struct GsplatServeStats {
   uint64_t pinned_slabs;     /* pinned result slabs allocated (on demand or in the background) */
   double capture_ms;         /* host time in those captures (part of launch_ms) */
   double pinned_alloc_ms;    /* host time launches waited on allocations (part of launch_ms) */
-} GsplatServeStats;          /* 152 bytes */
+  uint64_t workspace_regrowths; /* lane workspace reallocations (each waits for an idle device) */
+  double regrowth_ms;        /* host time in them (part of launch_ms) */
+} GsplatServeStats;          /* 168 bytes */
 
 int32_t gsplat_server_create(const GsplatServeConfig *config, GsplatServer **out_server);
 /* Finishes the batches in flight, fails queued requests and frees everything. */

@@ -50,7 +50,7 @@ def test_abi_struct_sizes():
     assert ctypes.sizeof(ffi.GsplatServeConfig) == 40
     assert ctypes.sizeof(ffi.GsplatTuneResult) == 32
     assert ctypes.sizeof(ffi.GsplatRequestInfo) == 32
-    assert ctypes.sizeof(ffi.GsplatServeStats) == 152
+    assert ctypes.sizeof(ffi.GsplatServeStats) == 168
 
 
 def test_versions_defaults_and_messages(oracle):
