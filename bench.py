@@ -41,6 +41,15 @@ import gsplat_scenes  # noqa: E402
 METRIC = "1080p frames/s @279k SH3"
 WORKLOAD = "plain SortedAlpha frame: 279,199 synthetic splats, SH degree 3, 1920x1080, 16x16 tiles"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def bench_config(world):
+    """The `config` both arms print, identical so that the two lines compare
+    as one workload; per-arm details go in top-level keys."""
+    return {"workload": WORKLOAD,
+            "l2": "CUDA arm: flushed between frames (256 MiB write); CPU arm: not flushed",
+            "parallelism": f"CUDA arm: one replica per GPU (x{world}), no collective on the "
+                           "data path; CPU arm: host threads on rank 0"}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -240,7 +249,7 @@ def run_reference(args, world, rank, budget_s=150.0):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "parallelism": "host threads"},
+            "config": bench_config(args.gpus),
             "cpu_baseline": {"value": value, "unit": "frames/s", "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0,
@@ -755,9 +764,9 @@ def run_cuda(args, world, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_frame,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "l2": "flushed between frames (256 MiB write)",
-                       "parallelism": f"replicas x{world}", "visible": int(counts.visible),
-                       "tile_pairs": int(counts.tile_keys)},
+            "config": bench_config(world),
+            "frame_counts": {"visible": int(counts.visible), "drawn": int(counts.drawn),
+                             "tile_pairs": int(counts.tile_keys)},
             "e2e": e2e, "gpu_launches": launches_per_frame * args.steps, "clocks": clk,
             "roofline": roofline, "phases": phase_rooflines}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -386,6 +386,7 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
   K1Stage<kPlanes> &st = *reinterpret_cast<K1Stage<kPlanes> *>(k1_dyn);
   __shared__ uint32_t s_block;
   __shared__ uint32_t s_set;
+  __shared__ uint32_t s_lost;  // a stage wait expired twice: copies may still land
   __shared__ uint32_t s_cnt[kMaxSetViews][kK1Warps];  // visible per view and warp
   __shared__ uint32_t s_hist[4][256];
   __shared__ FrameParams s_params[kMaxSetViews];  // the set's per-view uniforms
@@ -393,6 +394,7 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
   if (threadIdx.x == 0) {
     const uint32_t blk = atomicAdd(&b.counters->k1_ticket, 1u);
     s_block = blk;
+    s_lost = 0;
     const uint32_t si = find_view(num_sets, blk, [&](uint32_t v) { return sets[v].block_base; });
     s_set = si;
     const ViewSetDev set0 = sets[si];
@@ -440,12 +442,20 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
   const SceneDev sc = views[set.first_view].sc;
   const uint32_t i = (block - set.block_base) * kK1Threads + threadIdx.x;
   const bool valid = i < sc.n;
+  // Stage waits: a wait that expires sets the error bit (the frame reports an
+  // internal error) and is retried once, bounded, for the copies in flight.
+  // When the retry expires too, this thread reads nothing of that stage (its
+  // splat counts as not visible, or as not drawn), the block never writes
+  // into the stage and does not retire its barriers; the block may then exit
+  // while copies still land in its shared memory, which only a faulting
+  // device can cause.
+  bool ok0 = true, ok1 = true;
   if (sc.hot) {
     // Every thread takes its packed record, the scene constants and its table
     // entries into registers, then the block overwrites the stage with the
-    // decoded planes.
-    if (!mbar_wait(&st.bar[0], 0, &b.counters->error)) mbar_wait(&st.bar[0], 0, &b.counters->error);
-    if (!mbar_wait(&st.bar[1], 0, &b.counters->error)) mbar_wait(&st.bar[1], 0, &b.counters->error);
+    // decoded planes (not at all if any thread's wait expired twice).
+    ok0 = mbar_wait(&st.bar[0], 0, &b.counters->error) || mbar_wait(&st.bar[0], 0, &b.counters->error);
+    ok1 = mbar_wait(&st.bar[1], 0, &b.counters->error) || mbar_wait(&st.bar[1], 0, &b.counters->error);
     const uint32_t *raw = reinterpret_cast<const uint32_t *>(&st);
     PackedIn in;
 #pragma unroll
@@ -462,14 +472,18 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
     in.var[1] = var[(in.w[2] >> 10) & 0x3ffu];
     in.var[2] = var[(in.w[2] >> 20) & 0x3ffu];
     in.ext = table[kPackedHeaderFloats + kPackedVarLut + ((in.w[1] >> 16) & 0xffu)];
+    if (__syncthreads_or(!(ok0 && ok1))) {
+      ok0 = ok1 = false;
+      if (threadIdx.x == 0) s_lost = 1;
+    } else {
+      decode_packed<kPlanes>(sc.planes, in, st);
+    }
     __syncthreads();
-    decode_packed<kPlanes>(sc.planes, in, st);
-    __syncthreads();
+  } else {
+    ok0 = mbar_wait(&st.bar[0], 0, &b.counters->error) || mbar_wait(&st.bar[0], 0, &b.counters->error);
+    if (!ok0) s_lost = 1;
   }
-  // A wait that expires leaves the error bit set (the frame reports an
-  // internal error) after a second bounded wait for the copies in flight.
-  if (!mbar_wait(&st.bar[0], 0, &b.counters->error)) mbar_wait(&st.bar[0], 0, &b.counters->error);
-  const float4 pa = valid ? st.pos[threadIdx.x] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 pa = valid && ok0 ? st.pos[threadIdx.x] : make_float4(0.f, 0.f, 0.f, 0.f);
 
   // Depth test for every view of the set. The block's visible count is
   // known right after it: publish it for the successors' look-back before
@@ -479,7 +493,7 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
     const FrameParams &p = s_params[k];
     const float rx = pa.x - p.cam[0], ry = pa.y - p.cam[1], rz = pa.z - p.cam[2];
     const float depth = p.r2[0] * rx + p.r2[1] * ry + p.r2[2] * rz;
-    const bool vis = valid && depth >= p.near_plane && depth <= p.far_plane;
+    const bool vis = valid && ok0 && depth >= p.near_plane && depth <= p.far_plane;
     const uint32_t ballot = __ballot_sync(0xffffffffu, vis);
     if (lane == 0) s_cnt[k][warp] = __popc(ballot);
     vis_bits |= (vis ? 1u : 0u) << k;
@@ -497,9 +511,13 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
     if (c) atomicAdd(&b.view_counters[set.first_view + threadIdx.x].visible, c);
   }
 
-  if (!mbar_wait(&st.bar[1], 0, &b.counters->error)) mbar_wait(&st.bar[1], 0, &b.counters->error);
-  const float4 ca = st.cov_a[threadIdx.x];
-  const float4 cb = st.cov_b[threadIdx.x];
+  if (!sc.hot) {
+    ok1 = mbar_wait(&st.bar[1], 0, &b.counters->error) || mbar_wait(&st.bar[1], 0, &b.counters->error);
+    if (!ok1) s_lost = 1;
+  }
+  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 ca = ok1 ? st.cov_a[threadIdx.x] : zero4;
+  const float4 cb = ok1 ? st.cov_b[threadIdx.x] : zero4;
   const float4 *col = &st.color[0][threadIdx.x];
   for (uint32_t k = 0; k < set.count; ++k) {
     const uint32_t view = set.first_view + k;
@@ -517,20 +535,22 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
       *dbg = z;
     }
     bool drawn = false;
-    if (vis) {
+    // Digit histograms of the depth keys for every radix pass (every
+    // compacted key is counted).
+    if (vis && !b.reuse_order) {
+      const uint32_t key = ~__float_as_uint(fmaxf(depth, 0.0f));
+#pragma unroll
+      for (int d = 0; d < 4; ++d) atomicAdd(&s_hist[d][(key >> (8 * d)) & 255u], 1u);
+    }
+    if (vis && ok1) {
       Record rec;
       uint2 rect = make_uint2(0u, 0u);
       drawn = project<kPlanes>(p, pa, ca, cb, col, rel, depth, rec, rect, dbg);
       b.rects[gid] = rect;
       if (drawn) b.records[gid] = rec;
-      // Digit histograms of the depth keys for every radix pass.
-      if (!b.reuse_order) {
-        const uint32_t key = ~__float_as_uint(fmaxf(depth, 0.0f));
-#pragma unroll
-        for (int d = 0; d < 4; ++d) atomicAdd(&s_hist[d][(key >> (8 * d)) & 255u], 1u);
-      }
-    } else if (b.reuse_order && valid) {
-      // The reused order may list this splat: it emits no tile this frame.
+    } else if ((b.reuse_order || vis) && valid) {
+      // The reused order may list this splat (or its stage was lost): it
+      // emits no tile this frame.
       b.rects[gid] = make_uint2(0u, 0u);
     }
     const uint32_t dmask = __ballot_sync(0xffffffffu, drawn);
@@ -570,7 +590,7 @@ __global__ void __launch_bounds__(kK1Threads, GSR_K1_MIN_BLOCKS)
     slot += view_total;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {  // every thread has passed both waits
+  if (threadIdx.x == 0 && !s_lost) {  // every thread has passed both waits
     mbar_inval(&st.bar[0]);
     mbar_inval(&st.bar[1]);
   }

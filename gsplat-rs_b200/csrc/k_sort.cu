@@ -20,6 +20,7 @@
 // their input order).
 
 #include <algorithm>
+#include <atomic>
 
 #include "device_common.cuh"
 #include "kernels.h"
@@ -355,19 +356,47 @@ uint64_t sort_work_words(uint32_t capacity, uint32_t passes) {
 }
 
 namespace {
-// Resident pass blocks on the device (the persistent grid).
+constexpr int kMaxDevices = 64;
+int current_device() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    dev = 0;
+  }
+  return dev;
+}
+// Resident pass blocks on the current device (the persistent grid), looked
+// up once per device.
 template <int kIpt>
 uint32_t resident_pass_blocks() {
-  static const uint32_t blocks = [] {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  static std::atomic<uint32_t> cache[kMaxDevices];
+  const int dev = current_device();
+  uint32_t blocks = cache[dev].load(std::memory_order_relaxed);
+  if (blocks == 0) {
+    int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel<kIpt>, kThreads, 0);
-    return (uint32_t)std::max(1, sms * std::max(per_sm, 1));
-  }();
+    blocks = device_sm_count() * (uint32_t)std::max(per_sm, 1);
+    cache[dev].store(blocks, std::memory_order_relaxed);
+  }
   return blocks;
 }
 }  // namespace
+
+uint32_t device_sm_count() {
+  static std::atomic<uint32_t> cache[kMaxDevices];
+  const int dev = current_device();
+  uint32_t sms = cache[dev].load(std::memory_order_relaxed);
+  if (sms == 0) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) {
+      cudaGetLastError();
+      v = 1;
+    }
+    sms = (uint32_t)v;
+    cache[dev].store(sms, std::memory_order_relaxed);
+  }
+  return sms;
+}
 
 void launch_sort(const SortBuffers &b, cudaStream_t stream) {
   const uint32_t tiles = tiles_for(b.capacity);
@@ -385,7 +414,7 @@ void launch_sort(const SortBuffers &b, cudaStream_t stream) {
       hist_kernel<kIptLarge>
           <<<grid, kThreads, 0, stream>>>(b.keys0, b.count, b.begin_bit, b.passes, hist);
   }
-  const uint32_t zero_blocks = std::min<uint32_t>(grid, 296);
+  const uint32_t zero_blocks = std::min<uint32_t>(grid, 2 * device_sm_count());
   plan_kernel<<<zero_blocks, kThreads, 0, stream>>>(b.count, b.hist ? b.hist : hist, b.passes,
                                                     b.plan, status, tiles, kThreads * ipt);
   for (uint32_t p = 0; p < b.passes; ++p) {

@@ -389,7 +389,8 @@ void launch_ranges(const SortPlan *tile_plan, const uint32_t *keys0, const uint3
                    const ViewDev *views, uint32_t num_views, ViewCounters *view_counters,
                    cudaStream_t stream) {
   uint32_t blocks = (capacity + 255) / 256;
-  blocks = blocks < 148 * 8 ? (blocks ? blocks : 1) : 148 * 8;
+  const uint32_t cap = 8 * device_sm_count();
+  blocks = blocks < cap ? (blocks ? blocks : 1) : cap;
   blocks = std::max(blocks, (num_views + 255) / 256);
   ranges_kernel<<<blocks, 256, 0, stream>>>(tile_plan, keys0, keys1, counters, ranges, views,
                                             num_views, view_counters);
@@ -400,14 +401,14 @@ const void *run_init_kernel_entry() { return reinterpret_cast<const void *>(&run
 void launch_run_init(const RunInit &a, cudaStream_t stream) {
   uint64_t words = 0;
   for (int r = 0; r < kRunZeroRegions; ++r) words = std::max(words, a.zero_words[r]);
-  const uint64_t blocks = std::min<uint64_t>(std::max<uint64_t>((words + 255) / 256, 1), 148 * 8);
+  const uint64_t blocks = std::min<uint64_t>(std::max<uint64_t>((words + 255) / 256, 1), 8ull * device_sm_count());
   run_init_kernel<<<(uint32_t)blocks, 256, 0, stream>>>(a);
 }
 
 void launch_fill_u32(uint32_t *dst, uint32_t value, uint64_t count, cudaStream_t stream) {
   if (count == 0) return;
   uint64_t blocks = (count + 255) / 256;
-  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks > 16ull * device_sm_count()) blocks = 16ull * device_sm_count();
   fill_kernel<<<(uint32_t)blocks, 256, 0, stream>>>(dst, value, count);
 }
 

@@ -151,6 +151,9 @@ void launch_run_init(const RunInit &a, cudaStream_t stream);
 const void *run_init_kernel_entry();
 
 // ---- small helpers ----------------------------------------------------------
+// Streaming multiprocessors of the current device (looked up once per
+// device); grid-stride kernels cap their grids at a few blocks per SM.
+uint32_t device_sm_count();
 void launch_fill_u32(uint32_t *dst, uint32_t value, uint64_t count, cudaStream_t stream);
 
 }  // namespace gsr

@@ -95,7 +95,7 @@ void sort_values_by_keys_host(const uint32_t *keys, uint32_t *values, uint64_t n
   GSR_CUDA_S(cudaMemcpyAsync(s.v[0], values, 4 * n, cudaMemcpyHostToDevice, st.s));
   GSR_CUDA_S(cudaMemcpyAsync(s.count, &n32, 4, cudaMemcpyHostToDevice, st.s));
   GSR_CUDA_S(cudaMemsetAsync(s.error, 0, 4, st.s));
-  invert_copy_kernel<<<std::min<uint32_t>((n32 + 255) / 256, 1184), 256, 0, st.s>>>(s.k[1], s.k[0], n32);
+  invert_copy_kernel<<<std::min<uint32_t>((n32 + 255) / 256, 8 * device_sm_count()), 256, 0, st.s>>>(s.k[1], s.k[0], n32);
   int fin = run_sort(s, 0, n32, st.s);
   GSR_CUDA_S(cudaMemcpy(values, s.v[fin], 4 * n, cudaMemcpyDeviceToHost));
 }
@@ -115,7 +115,7 @@ void sort_pairs_host(uint32_t *keys, uint32_t *values, uint64_t n) {
   int a = run_sort(s, 0, n32, st.s);
   // Pass 2: stable order by inverted key, carrying the values.
   int b = 1 - a;
-  const unsigned grid = std::min<uint32_t>((n32 + 255) / 256, 1184);
+  const unsigned grid = std::min<uint32_t>((n32 + 255) / 256, 8 * device_sm_count());
   invert_copy_kernel<<<grid, 256, 0, st.s>>>(s.v[a], s.k[b], n32);
   GSR_CUDA_S(cudaMemcpyAsync(s.v[b], s.k[a], 4 * n, cudaMemcpyDeviceToDevice, st.s));
   int fin = run_sort(s, b, n32, st.s);

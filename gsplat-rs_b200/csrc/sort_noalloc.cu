@@ -18,8 +18,10 @@
 // previous call's contents, so every call zeroes the parts that must start at
 // zero. Two calls running on the GPU at the same time would race on it; this
 // entry point prevents that inside one process by holding a process-wide
-// lock and waiting for its stream before it returns.
+// lock and waiting for its stream before it returns. Because it waits for
+// its stream, it refuses a stream that is being captured.
 
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -92,9 +94,23 @@ Code sort_values_by_keys_noalloc(const uint32_t *keys, uint32_t *values, uint64_
     msg = "keys and values must be device pointers";
     return Code::InvalidArgument;
   }
+  // An error left pending by the caller's earlier work is reported as such
+  // (and cleared), not blamed on the sort's own launches below.
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    msg = std::string("pending CUDA error before the sort: ") + cudaGetErrorString(e);
+    return Code::Internal;
+  }
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(stream, &capture);
+  if (e != cudaSuccess) return fail_code(e, "cudaStreamIsCapturing", msg);
+  if (capture != cudaStreamCaptureStatusNone) {
+    msg = "the stream is being captured: this sort synchronises its stream before returning";
+    return Code::InvalidArgument;
+  }
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
   int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  e = cudaGetDevice(&dev);
   if (e != cudaSuccess) {
     cudaGetLastError();
     msg = std::string("no CUDA device: ") + cudaGetErrorString(e);
@@ -118,14 +134,18 @@ Code sort_values_by_keys_noalloc(const uint32_t *keys, uint32_t *values, uint64_
   uint32_t *count_error = reinterpret_cast<uint32_t *>(base + kOffCount);
   uint32_t *work = reinterpret_cast<uint32_t *>(base + kOffWork);
   const uint32_t n32 = (uint32_t)n;
-  const unsigned grid = (n32 + 255) / 256 < 1184u ? (n32 + 255) / 256 : 1184u;
+  const unsigned grid = std::min<uint32_t>((n32 + 255) / 256, 8 * device_sm_count());
   noalloc_prepare_kernel<<<grid, 256, 0, stream>>>(keys, k0, count_error, n32);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail_code(e, "key preparation launch", msg);
   // launch_sort zeroes the tickets, histograms and look-back words itself.
   SortBuffers b{k0, values, k1, v1, count_error, n32, 0, 4, plan, work, count_error + 1, nullptr};
   launch_sort(b, stream);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail_code(e, "radix sort launch", msg);
   noalloc_finish_kernel<<<grid, 256, 0, stream>>>(plan, v1, values, n32);
   e = cudaGetLastError();
-  if (e != cudaSuccess) return fail_code(e, "kernel launch", msg);
+  if (e != cudaSuccess) return fail_code(e, "result copy launch", msg);
   uint32_t err = 0;
   e = cudaMemcpyAsync(&err, count_error + 1, 4, cudaMemcpyDeviceToHost, stream);
   if (e != cudaSuccess) return fail_code(e, "cudaMemcpyAsync", msg);

@@ -208,9 +208,12 @@ int32_t gsplat_cuda_sort_pairs(uint32_t *keys, uint32_t *values, uint64_t len);
  * that every GPU loading the library holds until exit; len above
  * 1,048,576 (2^20) is rejected with GSPLAT_ERROR_INVALID_ARGUMENT. The first
  * call on a device looks the array's address up (cudaGetSymbolAddress), so
- * make it before any stream capture starts on that device. Calls share the
- * array; overlapping calls would race, so calls are serialised inside the
- * process. Nothing here calls cudaMalloc or cudaFree. */
+ * make it before any stream capture starts on that device. The call waits
+ * for `stream`, so a stream that is being captured is refused with
+ * GSPLAT_ERROR_INVALID_ARGUMENT; a CUDA error left pending by earlier work is
+ * returned (and cleared) as GSPLAT_ERROR_INTERNAL before anything launches.
+ * Calls share the array; overlapping calls would race, so calls are
+ * serialised inside the process. Nothing here calls cudaMalloc or cudaFree. */
 int32_t gsplat_cuda_sort_values_by_keys_noalloc(const uint32_t *keys, uint32_t *values,
                                                 uint64_t len, void *stream);
 

@@ -1,9 +1,9 @@
 """Regenerates the golden fixtures under tests/golden/ from the reference tree.
 
-Run in a checkout that has the reference project mounted (read-only) at
-REFERENCE_ROOT (default /root/reference):
+Run with REFERENCE_ROOT naming a checkout of the reference project (read
+only; the variable is required):
 
-    python tests/golden/make_golden.py
+    REFERENCE_ROOT=/path/to/gsplat-rs python tests/golden/make_golden.py
 
 What it writes (all small, committed):
   minimal_ascii.ply, minimal_binary.ply  byte copies of the reference's
@@ -23,7 +23,10 @@ import os
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("REFERENCE_ROOT", "")
+if not REF or not os.path.isdir(REF):
+    raise SystemExit("REFERENCE_ROOT must name a checkout of the reference project "
+                     "(misotofu0525/gsplat-rs); got " + repr(REF))
 
 
 def ref_text(rel):
