@@ -192,12 +192,33 @@ def algorithmic_bytes(phase, counts, n, planes, width, height, tile_passes):
     return 0
 
 
-def cpu_baseline(scene, cam, w, h, budget_s=15.0, steps=None):
+def image_errors(img, ref):
+    """Per-pixel error of an RGBA8 image against a reference image, in UNORM8
+    steps: max over channels, mean over RGB, fraction of pixels with any RGB
+    channel more than 1/255 (and 3/255) off, and the reference's own image
+    gate (mean |dRGB| <= 1/255 and <= 0.1% of pixels above 3/255,
+    crates/gsplat-render-wgpu/src/lib.rs:3520-3537)."""
+    d = np.abs(img.astype(np.int32) - ref.astype(np.int32))
+    rgb = d[..., :3]
+    over1 = float((rgb > 1).any(axis=-1).mean())
+    over3 = float((rgb > 3).any(axis=-1).mean())
+    mean_rgb = float(rgb.mean()) / 255.0
+    return {"max_abs_steps": int(d.max(initial=0)), "max_abs_rgb": int(rgb.max(initial=0)),
+            "mean_abs_rgb": mean_rgb, "frac_px_over_1_255": over1, "frac_px_over_3_255": over3,
+            "reference_gate": bool(mean_rgb <= 1.0 / 255.0 and over3 <= 0.001)}
+
+
+def cpu_baseline(scene, cam, w, h, budget_s=15.0, steps=None, gpu_images=None):
+    """The reference frame restated on the host (the oracle's C++ port of
+    the CPU depth preprocess, radix sort, vertex stage and UNORM8 blend).
+    gpu_images: {mode: RGBA8 image} rendered on the GPU for the same camera;
+    each is compared with the CPU frame's image (the reference image model)
+    and with the FP64 evaluation of the same frame."""
     import oracle_py
 
     threads = os.cpu_count() or 1
     sv = oracle_py.SceneView(scene)
-    oracle_py.render_reference_frame(sv, cam, w, h, threads)  # warm caches
+    ref_img, _ = oracle_py.render_reference_frame(sv, cam, w, h, threads)  # warm caches
     t0 = time.perf_counter()
     frames = 0
     phases = []
@@ -210,11 +231,19 @@ def cpu_baseline(scene, cam, w, h, budget_s=15.0, steps=None):
             break
     el = time.perf_counter() - t0
     ph = np.mean(np.array(phases), axis=0)
-    return {"value": frames / el, "unit": "frames/s", "cores": threads, "kind": "port",
-            "sample": f"{frames} full frames of the workload; depth preprocess and radix sort on "
-                      f"1 thread, vertex stage and UNORM8 blend on {threads} threads "
-                      f"(mean ms: preprocess {ph[0]:.1f}, sort {ph[1]:.1f}, vertex {ph[2]:.1f}, "
-                      f"raster {ph[3]:.1f})"}
+    out = {"value": frames / el, "unit": "frames/s", "cores": threads, "kind": "port",
+           "sample": f"{frames} full frames of the workload; depth preprocess and radix sort on "
+                     f"1 thread, vertex stage and UNORM8 blend on {threads} threads "
+                     f"(mean ms: preprocess {ph[0]:.1f}, sort {ph[1]:.1f}, vertex {ph[2]:.1f}, "
+                     f"raster {ph[3]:.1f})"}
+    if gpu_images:
+        fr = oracle_py.Frame(sv, cam, w, h)
+        f64, _ = fr.raster_f64(threads)
+        out["gpu_image_errors"] = {
+            mode: {"vs_reference_model": image_errors(img, ref_img),
+                   "vs_fp64": image_errors(img, f64)} for mode, img in gpu_images.items()}
+        out["gpu_image_errors"]["reference_model_vs_fp64"] = image_errors(ref_img, f64)
+    return out
 
 
 def run_reference(args, world, rank, budget_s=150.0):
@@ -705,6 +734,39 @@ def run_cuda(args, world, rank, local):
     replicas.barrier()
     ms_per_frame = device_ms / args.steps
     value = whole_job_rate(world, args.steps, device_ms / 1000.0)
+    img_fp32 = ctx.readback_rgba8().copy()
+
+    # The UNORM8 parity mode (the reference's per-splat UNORM8 rounding,
+    # bit-exact with the oracle's reference image model) on the same frames.
+    ctx.set_blend_mode(1)
+    for _ in range(max(args.warmup, 3)):
+        ctx.render_frame()
+    parity_phase = {}
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(i)
+        ctx.render_frame()
+        for k, v in ctx.phase_times().items():
+            parity_phase[k] = parity_phase.get(k, 0.0) + v
+    replicas.barrier()
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(i + 1)
+            starts[i].record(stream)
+        ctx.render_frame_async()
+        with torch.cuda.stream(stream):
+            ends[i].record(stream)
+    ctx.sync()
+    torch.cuda.synchronize()
+    parity_ms = replicas.max(sum(s.elapsed_time(e) for s, e in zip(starts, ends)))
+    img_unorm8 = ctx.readback_rgba8().copy()
+    ctx.set_blend_mode(0)
+    ctx.render_frame()
+    parity = {"value": whole_job_rate(world, args.steps, parity_ms / 1000.0), "unit": "frames/s",
+              "ms_per_step": parity_ms / args.steps,
+              "phases_ms": {k: v / args.steps for k, v in parity_phase.items()},
+              "blend": "UNORM8 after every splat, back to front (the reference image model)"}
 
     # End to end through the C ABI: camera in, frame, RGBA8 readback to pinned
     # memory every step. Frames are enqueued back to back and each image is
@@ -768,9 +830,10 @@ def run_cuda(args, world, rank, local):
             "frame_counts": {"visible": int(counts.visible), "drawn": int(counts.drawn),
                              "tile_pairs": int(counts.tile_keys)},
             "e2e": e2e, "gpu_launches": launches_per_frame * args.steps, "clocks": clk,
-            "roofline": roofline, "phases": phase_rooflines}
+            "roofline": roofline, "phases": phase_rooflines, "parity_mode": parity}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(scene, cam, w, h, budget_s=args.cpu_budget)
+        line["cpu_baseline"] = cpu_baseline(scene, cam, w, h, budget_s=args.cpu_budget,
+                                            gpu_images={"fp32": img_fp32, "unorm8": img_unorm8})
     ctx.close()
     if not args.no_batched and world == 1:
         line["batched"] = measure_batched(ffi, torch, args.batch_steps, 2)

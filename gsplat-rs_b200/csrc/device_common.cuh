@@ -149,18 +149,23 @@ __device__ __forceinline__ void lookback_publish_inclusive(unsigned long long *s
 // e^x for x in [-4.5, 0]: Cody-Waite reduction to base 2 and the degree-6
 // Taylor polynomial of 2^f (coefficients ln(2)^k / k!), explicit fmaf, so the
 // result is reproducible bit for bit by a C++ restatement. Relative error
-// about 2e-7.
+// about 2e-7. n = rint(t) is taken by adding and subtracting 1.5 * 2^23
+// (for |t| < 2^22 the sum rounds t to the nearest integer, ties to even,
+// exactly as rintf does), and the same sum's bit pattern gives n as an
+// integer: full-rate additions instead of the slower conversion units.
+constexpr float kRoundMagic = 12582912.0f;  // 1.5 * 2^23
 __device__ __forceinline__ float exp_neg(float x) {
-  float t = x * 1.44269504088896341f;
-  float n = rintf(t);
-  float f = t - n;
-  float p = fmaf(1.54035304e-4f, f, 1.33335581e-3f);
-  p = fmaf(p, f, 9.61812911e-3f);
-  p = fmaf(p, f, 5.55041087e-2f);
-  p = fmaf(p, f, 2.40226507e-1f);
-  p = fmaf(p, f, 6.93147181e-1f);
-  p = fmaf(p, f, 1.0f);
-  int e = __float2int_rn(n);
+  const float t = __fmul_rn(x, 1.44269504088896341f);
+  const float big = __fadd_rn(t, kRoundMagic);
+  const float n = __fsub_rn(big, kRoundMagic);
+  const float f = __fsub_rn(t, n);
+  float p = __fmaf_rn(1.54035304e-4f, f, 1.33335581e-3f);
+  p = __fmaf_rn(p, f, 9.61812911e-3f);
+  p = __fmaf_rn(p, f, 5.55041087e-2f);
+  p = __fmaf_rn(p, f, 2.40226507e-1f);
+  p = __fmaf_rn(p, f, 6.93147181e-1f);
+  p = __fmaf_rn(p, f, 1.0f);
+  const int e = __float_as_int(big) - __float_as_int(kRoundMagic);
   return __int_as_float(__float_as_int(p) + e * (1 << 23));
 }
 

@@ -47,77 +47,218 @@ __device__ __forceinline__ void fold_errors(const RasterArgs &a) {
   }
 }
 
-// UNORM8 parity mode: back to front over the tile list, the reference
-// fragment rule with the quad clip, rounding to UNORM8 after every blend.
+// Which 8x4-pixel warp blocks of a kTile x kTile tile the ellipse
+// |local|^2 <= thr reaches (bit band * kTile/8 + column block): for each
+// 4-row band, the x-interval the ellipse spans within the band, plus half a
+// pixel on every side, tested against the 8-column blocks. q(dx, dy) =
+// A dx^2 + 2B dx dy + C dy^2 is |local|^2 in pixel units; (cxl, cyl) is the
+// centre relative to the tile's first pixel. The mask only culls: hardware
+// reciprocal/rsqrt (a few ulp) plus an inflation of the extents far above
+// their error keeps it conservative.
+template <int kTile>
+__device__ __forceinline__ uint32_t ellipse_block_mask(float4 ra, float4 rb, float thr, float cxl,
+                                                       float cyl) {
+  constexpr int kBlocksX = kTile / 8;
+  constexpr int kWarps = kTile * kTile / 32;
+  const float qa = fmaf(ra.z, ra.z, rb.x * rb.x);
+  const float qb = fmaf(ra.z, ra.w, rb.x * rb.y);
+  const float qc = fmaf(ra.w, ra.w, rb.y * rb.y);
+  const float det = fmaf(qa, qc, -qb * qb);
+  const float inv_a = __fdividef(1.0f, qa);
+  const float inv_det = __fdividef(1.0f, det);
+  const float hx2 = thr * qc * inv_det, hy2 = thr * qa * inv_det;
+  const float hx_raw = hx2 * rsqrtf(fmaxf(hx2, 1e-30f));
+  const float hx = fmaf(hx_raw, 1.0001f, 1e-3f);
+  const float hy = fmaf(hy2 * rsqrtf(fmaxf(hy2, 1e-30f)), 1.0001f, 1e-3f);
+  // dy of the leftmost point (rightmost at -dy_left), from the unpadded extent
+  const float dy_left = qb * hx_raw * __fdividef(1.0f, qc);
+  const float s2a = thr * qa;
+  constexpr float kPad = 0.5f + 1.0f / 64.0f;
+  uint32_t mask = 0;
+#pragma unroll
+  for (int band = 0; band < kTile / 4; ++band) {
+    const float lo = fmaxf((float)(4 * band) - 0.5f - cyl, -hy);
+    const float hi = fminf((float)(4 * band) + 3.5f - cyl, hy);
+    if (!(lo <= hi)) continue;
+    const float qlo = fmaxf(s2a - det * lo * lo, 0.0f), qhi = fmaxf(s2a - det * hi * hi, 0.0f);
+    const float r_lo = fmaf(qlo * rsqrtf(fmaxf(qlo, 1e-30f)), 1.0001f, 1e-3f);
+    const float r_hi = fmaf(qhi * rsqrtf(fmaxf(qhi, 1e-30f)), 1.0001f, 1e-3f);
+    float xmin = fminf((-qb * lo - r_lo) * inv_a, (-qb * hi - r_hi) * inv_a);
+    float xmax = fmaxf((-qb * lo + r_lo) * inv_a, (-qb * hi + r_hi) * inv_a);
+    if (dy_left >= lo && dy_left <= hi) xmin = -hx;
+    if (-dy_left >= lo && -dy_left <= hi) xmax = hx;
+    const float bx0f = cxl + xmin - kPad, bx1f = cxl + xmax + kPad;
+#pragma unroll
+    for (int colb = 0; colb < kBlocksX; ++colb)
+      if (bx1f >= (float)(8 * colb) && bx0f <= (float)(8 * colb + 7))
+        mask |= 1u << (band * kBlocksX + colb);
+  }
+  // A degenerate conic (never expected: axes are clamped to an anisotropy of
+  // 64) falls back to every block.
+  if (!(det > 0.0f) || !(hx < 3.0e38f) || !(hy < 3.0e38f)) mask = (1u << kWarps) - 1u;
+  if (!(thr >= 0.0f)) mask = 0;
+  return mask;
+}
+
+// Ordered compaction of the chunk entries whose mask has this warp's bit
+// into list[] (ballots keep the list order); returns their count.
+__device__ __forceinline__ uint32_t compact_warp_entries(const uint8_t *mask, uint32_t n_in,
+                                                        uint32_t warp, uint32_t lane,
+                                                        uint16_t *list) {
+  uint32_t n_w = 0;
+  for (uint32_t k0 = 0; k0 < n_in; k0 += 32) {
+    const uint32_t k = k0 + lane;
+    const bool hit = k < n_in && ((mask[k] >> warp) & 1u);
+    const uint32_t bal = __ballot_sync(0xffffffffu, hit);
+    if (hit) list[n_w + __popc(bal & lanemask_lt())] = (uint16_t)k;
+    n_w += __popc(bal);
+  }
+  __syncwarp();
+  return n_w;
+}
+
+// UNORM8 parity mode: back to front over the tile list (forwards), the
+// reference fragment rule with the quad clip, and the premultiplied OVER
+// blend rounded to UNORM8 after every splat, exactly as the oracle's
+// reference image model evaluates it. The blend has no early exit (a pixel's
+// final value depends on every splat behind it), so the work it saves is
+// culling: threads map to 8x4-pixel warp blocks as in the FP32 mode, one
+// thread per chunk entry forms the entry's premultiplied colour (rgb * alpha,
+// the vertex stage's product) and a conservative mask of the warp blocks the
+// ellipse reaches (r^2 <= s^2, widened by a relative 1e-5 and an absolute
+// 1e-6: alpha e^(-4.5 r^2) > 1/256 holds only below s^2 up to rounding), and
+// each warp walks only the entries whose mask has its bit. A channel keeps
+// its stored value both as the integer t and as f = RN(t / 255), the float
+// the next blend reads.
+template <int kTile>
+struct U8Smem {
+  static constexpr int kWarps = kTile * kTile / 32;
+  static constexpr int kChunk = kTile * kTile;
+  float4 raw[2][3][kChunk];  // (cx, cy, ax, ay), (bx, by, s, alpha), premultiplied rgb
+  uint8_t mask[kChunk];
+  uint16_t list[kWarps][kChunk];
+  uint32_t view;
+};
+
+// RN(t / 255) for integer t in [0, 255] as t * 2^-8 + t * (1/255 - 2^-8)
+// in one fma: exact for every such t (the first product is exact and the
+// second's rounding never moves the sum across a rounding boundary), in two
+// instructions instead of a division.
+constexpr float kInv255Lo = 0x1.010102p-16f;  // RN(1/255 - 2^-8)
+
+// One channel's blend step, dst = to_unorm8(fma(dst / 255, 1 - w, src)):
+// saturate, scale by 255 and round to the nearest integer (ties to even) by
+// the 1.5 * 2^23 addition, then the float the next step reads.
+__device__ __forceinline__ void unorm8_step(float &f, float &t, float om, float src) {
+  const float v = __saturatef(__fmaf_rn(f, om, src));
+  t = __fsub_rn(__fadd_rn(__fmul_rn(v, 255.0f), kRoundMagic), kRoundMagic);
+  f = __fmaf_rn(t, 0x1p-8f, __fmul_rn(t, kInv255Lo));
+}
+
 template <int kTile>
 __global__ void __launch_bounds__(kTile *kTile) raster_unorm8_kernel(RasterArgs a) {
-  constexpr int kN = kTile * kTile;
-  __shared__ float4 s_a[2][kN];
-  __shared__ float4 s_b[2][kN];
-  __shared__ float4 s_c[2][kN];
-  __shared__ uint32_t s_view;
+  using Smem = U8Smem<kTile>;
+  constexpr int kN = Smem::kChunk;
+  constexpr int kBlocksX = kTile / 8;
+  __shared__ Smem sm;
   fold_errors(a);
   const uint32_t tile = blockIdx.x;
   if (threadIdx.x == 0)
-    s_view = find_view(a.num_views, tile, [&](uint32_t v) { return a.views[v].tile_base; });
+    sm.view = find_view(a.num_views, tile, [&](uint32_t v) { return a.views[v].tile_base; });
   __syncthreads();
-  const uint32_t view = s_view;
-  const FrameParams p = a.views[view].p;
+  const uint32_t view = sm.view;
+  const uint32_t width = a.views[view].p.width, height = a.views[view].p.height;
+  const uint32_t tiles_x = a.views[view].p.tiles_x;
   uint32_t *__restrict__ image = a.images + a.views[view].image_base;
   const uint32_t local_tile = tile - a.views[view].tile_base;
-  const uint32_t tx = local_tile % p.tiles_x, ty = local_tile / p.tiles_x;
-  const uint32_t tid = threadIdx.x;
-  const uint32_t px = tx * kTile + (tid % kTile);
-  const uint32_t py = ty * kTile + (tid / kTile);
-  const bool inside = px < p.width && py < p.height;
+  const uint32_t tx = local_tile % tiles_x, ty = local_tile / tiles_x;
+  const uint32_t x0 = tx * kTile, y0 = ty * kTile;
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t px = x0 + (warp % kBlocksX) * 8 + (lane & 7);
+  const uint32_t py = y0 + (warp / kBlocksX) * 4 + (lane >> 3);
+  const bool inside = px < width && py < height;
   const float fpx = (float)px, fpy = (float)py;
+  const float ftx = (float)x0, fty = (float)y0;
   const uint32_t *__restrict__ ids = a.plan->final_buffer == 0 ? a.ids0 : a.ids1;
   const uint2 range = a.ranges[tile];
   const uint32_t count = range.y - range.x;
   const uint32_t chunks = (count + kN - 1) / kN;
   auto issue = [&](uint32_t c, int buf) {
-    uint32_t k = c * kN + tid;
+    const uint32_t k = c * kN + tid;
     if (k < count) {
       const Record *r = &a.records[ids[range.x + k]];
-      cp_async16(&s_a[buf][tid], &r->a);
-      cp_async16(&s_b[buf][tid], &r->b);
-      cp_async16(&s_c[buf][tid], &r->c);
+      cp_async16(&sm.raw[buf][0][tid], &r->a);
+      cp_async16(&sm.raw[buf][1][tid], &r->b);
+      cp_async16(&sm.raw[buf][2][tid], &r->c);
     }
     cp_async_commit();
   };
-  uint32_t d0 = 0, d1 = 0, d2 = 0, d3 = 0;
+  // Coverage and weight of entry j at this pixel (the reference fragment
+  // rule); false when the fragment is discarded.
+  auto weight = [&](int buf, uint32_t j, float &g, float &w) {
+    const float4 d0 = sm.raw[buf][0][j];
+    const float4 d1 = sm.raw[buf][1][j];
+    const float dpx = __fsub_rn(fpx, d0.x), dpy = __fsub_rn(fpy, d0.y);
+    const float lx = __fmaf_rn(d0.z, dpx, __fmul_rn(d0.w, dpy));
+    const float ly = __fmaf_rn(d1.x, dpx, __fmul_rn(d1.y, dpy));
+    if (!(fabsf(lx) <= d1.z && fabsf(ly) <= d1.z)) return false;
+    const float r2 = __fmaf_rn(lx, lx, __fmul_rn(ly, ly));
+    if (!(r2 <= 1.0f)) return false;
+    g = exp_neg(__fmul_rn(-4.5f, r2));
+    w = __fmul_rn(d1.w, g);
+    return w > 1.0f / 256.0f;
+  };
+  float f0 = 0.f, f1 = 0.f, f2 = 0.f, f3 = 0.f;
+  float t0 = 0.f, t1 = 0.f, t2 = 0.f, t3 = 0.f;
+  auto blend = [&](int buf, uint32_t j, float g, float w) {
+    const float4 pc = sm.raw[buf][2][j];
+    const float om = __fsub_rn(1.0f, w);
+    unorm8_step(f0, t0, om, __fmul_rn(pc.x, g));
+    unorm8_step(f1, t1, om, __fmul_rn(pc.y, g));
+    unorm8_step(f2, t2, om, __fmul_rn(pc.z, g));
+    unorm8_step(f3, t3, om, w);
+  };
   if (chunks > 0) issue(0, 0);
   for (uint32_t c = 0; c < chunks; ++c) {
     const int buf = c & 1;
     if (c + 1 < chunks) issue(c + 1, buf ^ 1);
     else cp_async_commit();
     cp_async_wait_1();
-    __syncthreads();
     const uint32_t n_in = min((uint32_t)kN, count - c * kN);
-    if (inside) {
-      for (uint32_t j = 0; j < n_in; ++j) {
-        const float4 ra = s_a[buf][j], rb = s_b[buf][j], col = s_c[buf][j];
-        float dpx = fpx - ra.x, dpy = fpy - ra.y;
-        float lx = fmaf(ra.z, dpx, ra.w * dpy);
-        float ly = fmaf(rb.x, dpx, rb.y * dpy);
-        if (!(fabsf(lx) <= rb.z && fabsf(ly) <= rb.z)) continue;
-        float r2 = fmaf(lx, lx, ly * ly);
-        if (!(r2 <= 1.0f)) continue;
-        float g = exp_neg(-4.5f * r2);
-        float w = rb.w * g;
-        if (!(w > 1.0f / 256.0f)) continue;
-        float om = 1.0f - w;
-        // premultiplied colour: the vertex stage's rgb * alpha
-        d0 = to_unorm8(fmaf((float)d0 / 255.0f, om, (col.x * rb.w) * g));
-        d1 = to_unorm8(fmaf((float)d1 / 255.0f, om, (col.y * rb.w) * g));
-        d2 = to_unorm8(fmaf((float)d2 / 255.0f, om, (col.z * rb.w) * g));
-        d3 = to_unorm8(fmaf((float)d3 / 255.0f, om, w));
-      }
+    if (tid < n_in) {
+      const float4 ra = sm.raw[buf][0][tid], rb = sm.raw[buf][1][tid], rc = sm.raw[buf][2][tid];
+      sm.raw[buf][2][tid] =
+          make_float4(__fmul_rn(rc.x, rb.w), __fmul_rn(rc.y, rb.w), __fmul_rn(rc.z, rb.w), 0.0f);
+      const float thr = __fmaf_rn(__fmul_rn(rb.z, rb.z), 1.00001f, 1e-6f);
+      sm.mask[tid] = (uint8_t)ellipse_block_mask<kTile>(ra, rb, thr, ra.x - ftx, ra.y - fty);
     }
     __syncthreads();
+    const uint32_t n_w = compact_warp_entries(sm.mask, n_in, warp, lane, sm.list[warp]);
+    if (inside) {
+      uint32_t i = 0;
+      // two entries per step: the second's coverage and weight do not wait
+      // for the first's blend
+      for (; i + 1 < n_w; i += 2) {
+        const uint32_t jj = *reinterpret_cast<const uint32_t *>(&sm.list[warp][i]);
+        const uint32_t ja = jj & 0xffffu, jb = jj >> 16;
+        float ga, wa, gb, wb;
+        const bool ca = weight(buf, ja, ga, wa);
+        const bool cb = weight(buf, jb, gb, wb);
+        if (ca) blend(buf, ja, ga, wa);
+        if (cb) blend(buf, jb, gb, wb);
+      }
+      if (i < n_w) {
+        const uint32_t ja = sm.list[warp][i];
+        float ga, wa;
+        if (weight(buf, ja, ga, wa)) blend(buf, ja, ga, wa);
+      }
+    }
+    __syncthreads();  // the next chunk's entries overwrite mask and list
   }
   cp_async_wait_all();
-  if (inside) image[(size_t)py * p.width + px] = d0 | (d1 << 8) | (d2 << 16) | (d3 << 24);
+  if (inside)
+    image[(size_t)py * width + px] =
+        (uint32_t)t0 | ((uint32_t)t1 << 8) | ((uint32_t)t2 << 16) | ((uint32_t)t3 << 24);
 }
 
 // FP32 front-to-back mode. Threads map to 8x4-pixel warp blocks (lane l of
@@ -213,62 +354,11 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
       sm.d0[tid] = make_float4(ra.z, ra.w, ox, thr);
       sm.d1[tid] = make_float4(rb.x, rb.y, oy, rb.w);
       sm.d2[tid] = col;
-      // Which 8x4 warp blocks the ellipse |local|^2 <= thr reaches: for each
-      // 4-row band, the x-interval the ellipse spans within the band (plus
-      // half a pixel on every side), tested against the 8-column blocks.
-      // q(dx, dy) = A dx^2 + 2B dx dy + C dy^2 is |local|^2 in pixel units.
-      const float qa = fmaf(ra.z, ra.z, rb.x * rb.x);
-      const float qb = fmaf(ra.z, ra.w, rb.x * rb.y);
-      const float qc = fmaf(ra.w, ra.w, rb.y * rb.y);
-      const float det = fmaf(qa, qc, -qb * qb);
-      // The mask only culls: hardware reciprocal/rsqrt (a few ulp) plus an
-      // inflation of the extents far above their error keeps it conservative.
-      const float inv_a = __fdividef(1.0f, qa);
-      const float inv_det = __fdividef(1.0f, det);
-      const float hx2 = thr * qc * inv_det, hy2 = thr * qa * inv_det;
-      const float hx_raw = hx2 * rsqrtf(fmaxf(hx2, 1e-30f));
-      const float hx = fmaf(hx_raw, 1.0001f, 1e-3f);
-      const float hy = fmaf(hy2 * rsqrtf(fmaxf(hy2, 1e-30f)), 1.0001f, 1e-3f);
-      // dy of the leftmost point (rightmost at -dy_left), from the unpadded extent
-      const float dy_left = qb * hx_raw * __fdividef(1.0f, qc);
-      const float s2a = thr * qa;
-      constexpr float kPad = 0.5f + 1.0f / 64.0f;
-      uint32_t mask = 0;
-#pragma unroll
-      for (int band = 0; band < kTile / 4; ++band) {
-        const float lo = fmaxf((float)(4 * band) - 0.5f - cyl, -hy);
-        const float hi = fminf((float)(4 * band) + 3.5f - cyl, hy);
-        if (!(lo <= hi)) continue;
-        const float qlo = fmaxf(s2a - det * lo * lo, 0.0f), qhi = fmaxf(s2a - det * hi * hi, 0.0f);
-        const float r_lo = fmaf(qlo * rsqrtf(fmaxf(qlo, 1e-30f)), 1.0001f, 1e-3f);
-        const float r_hi = fmaf(qhi * rsqrtf(fmaxf(qhi, 1e-30f)), 1.0001f, 1e-3f);
-        float xmin = fminf((-qb * lo - r_lo) * inv_a, (-qb * hi - r_hi) * inv_a);
-        float xmax = fmaxf((-qb * lo + r_lo) * inv_a, (-qb * hi + r_hi) * inv_a);
-        if (dy_left >= lo && dy_left <= hi) xmin = -hx;
-        if (-dy_left >= lo && -dy_left <= hi) xmax = hx;
-        const float bx0f = cxl + xmin - kPad, bx1f = cxl + xmax + kPad;
-#pragma unroll
-        for (int colb = 0; colb < kBlocksX; ++colb)
-          if (bx1f >= (float)(8 * colb) && bx0f <= (float)(8 * colb + 7))
-            mask |= 1u << (band * kBlocksX + colb);
-      }
-      // A degenerate conic (never expected: axes are clamped to an
-      // anisotropy of 64) falls back to every block.
-      if (!(det > 0.0f) || !(hx < 3.0e38f) || !(hy < 3.0e38f)) mask = (1u << kWarps) - 1u;
-      if (!(thr >= 0.0f)) mask = 0;
-      sm.mask[tid] = (uint8_t)mask;
+      sm.mask[tid] = (uint8_t)ellipse_block_mask<kTile>(ra, rb, thr, cxl, cyl);
     }
     __syncthreads();
     // Ordered compaction of this warp's entries.
-    uint32_t n_w = 0;
-    for (uint32_t k0 = 0; k0 < n_in; k0 += 32) {
-      uint32_t k = k0 + lane;
-      bool hit = k < n_in && ((sm.mask[k] >> warp) & 1u);
-      uint32_t bal = __ballot_sync(0xffffffffu, hit);
-      if (hit) sm.list[warp][n_w + __popc(bal & lanemask_lt())] = (uint16_t)k;
-      n_w += __popc(bal);
-    }
-    __syncwarp();
+    const uint32_t n_w = compact_warp_entries(sm.mask, n_in, warp, lane, sm.list[warp]);
     // Four list entries per step (one early-out vote, one packed index
     // load); each pixel still takes them strictly in list order.
     // w = alpha e^(-4.5 r2) = 2^(log2 alpha - 4.5 log2(e) r2) (the entry's

@@ -125,6 +125,10 @@ def test_full_config2_parity(oracle):
     assert m["max_vs_f64"] <= 2
     st = ctx.stats()
     assert st.visible_count == fr.visible and st.drawn_count == fr.visible
+    # the UNORM8 parity mode: the reference image model, bit for bit
+    ctx.set_blend_mode(1)
+    ctx.render_frame()
+    assert np.array_equal(ctx.readback_rgba8(), ref8), "unorm8 parity image vs reference model"
     ctx.close()
 
 
