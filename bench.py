@@ -208,36 +208,100 @@ def image_errors(img, ref):
             "reference_gate": bool(mean_rgb <= 1.0 / 255.0 and over3 <= 0.001)}
 
 
-def cpu_baseline(scene, cam, w, h, budget_s=15.0, steps=None, gpu_images=None):
-    """The reference frame restated on the host (the oracle's C++ port of
-    the CPU depth preprocess, radix sort, vertex stage and UNORM8 blend).
-    gpu_images: {mode: RGBA8 image} rendered on the GPU for the same camera;
-    each is compared with the CPU frame's image (the reference image model)
-    and with the FP64 evaluation of the same frame."""
+def nearest_rank(values, q):
+    """Nearest-rank percentile (the reference bench-runner's definition,
+    tools/bench-runner/src/main.rs:1051-1072)."""
+    v = sorted(values)
+    return float(v[max(0, int(math.ceil(q * len(v))) - 1)])
+
+
+def _dist(values):
+    return {"median": nearest_rank(values, 0.5), "p95": nearest_rank(values, 0.95),
+            "mean": float(np.mean(values))}
+
+
+def host_cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def lcg_keys(seed, n):
+    """The reference sort tests' key generator (x = x * 1664525 + 1013904223,
+    crates/gsplat-sort/src/lib.rs:597-612)."""
+    out = np.empty(n, np.uint32)
+    x = seed & 0xFFFFFFFF
+    for i in range(n):
+        x = (x * 1664525 + 1013904223) & 0xFFFFFFFF
+        out[i] = x
+    return out
+
+
+def cpu_baseline(scene, cam, w, h, warmup=5, iters=30, gpu_images=None):
+    """The reference frame restated on the host (the oracle's C++ port of the
+    CPU depth preprocess and radix sort on one thread, the vertex stage and
+    UNORM8 blend on every host thread), per phase as median and p95 over
+    `iters` frames after `warmup`, at the 16,384-splat SH0 256x256 workload
+    and at the headline 279,199-splat SH3 1080p one; and the CPU radix sort
+    on its own, on the reference's 200k-key microbenchmark input
+    (crates/gsplat-sort/src/lib.rs:649-676) and on the 1080p frame's depth
+    keys. gpu_images: {mode: RGBA8 image} rendered on the GPU for the headline
+    camera; each is compared with the CPU frame's image (the reference image
+    model) and with the FP64 evaluation of the same frame."""
     import oracle_py
 
     threads = os.cpu_count() or 1
-    sv = oracle_py.SceneView(scene)
-    ref_img, _ = oracle_py.render_reference_frame(sv, cam, w, h, threads)  # warm caches
-    t0 = time.perf_counter()
-    frames = 0
-    phases = []
-    while True:
-        _, t = oracle_py.render_reference_frame(sv, cam, w, h, threads)
-        phases.append((t.preprocess_ms, t.sort_ms, t.project_ms, t.raster_ms))
-        frames += 1
+    per_config = {}
+    ref_img = None
+    sv2 = None
+    c1 = gsplat_scenes.config1(seed=0)
+    for name, (sc, cm, ww, hh) in (("config1_16k_sh0_256", c1),
+                                   ("config2_279k_sh3_1080p", (scene, cam, w, h))):
+        sv = oracle_py.SceneView(sc)
+        for _ in range(warmup):
+            img, _ = oracle_py.render_reference_frame(sv, cm, ww, hh, threads)
+        rows = {k: [] for k in ("preprocess", "sort", "vertex", "raster", "total")}
+        t0 = time.perf_counter()
+        for _ in range(iters):
+            img, t = oracle_py.render_reference_frame(sv, cm, ww, hh, threads)
+            rows["preprocess"].append(t.preprocess_ms)
+            rows["sort"].append(t.sort_ms)
+            rows["vertex"].append(t.project_ms)
+            rows["raster"].append(t.raster_ms)
+            rows["total"].append(t.total_ms)
         el = time.perf_counter() - t0
-        if (steps is not None and frames >= steps) or (steps is None and el >= budget_s):
-            break
-    el = time.perf_counter() - t0
-    ph = np.mean(np.array(phases), axis=0)
-    out = {"value": frames / el, "unit": "frames/s", "cores": threads, "kind": "port",
-           "sample": f"{frames} full frames of the workload; depth preprocess and radix sort on "
-                     f"1 thread, vertex stage and UNORM8 blend on {threads} threads "
-                     f"(mean ms: preprocess {ph[0]:.1f}, sort {ph[1]:.1f}, vertex {ph[2]:.1f}, "
-                     f"raster {ph[3]:.1f})"}
+        per_config[name] = {"frames_per_s": iters / el, "visible": int(t.visible),
+                            "phases_ms": {k: _dist(v) for k, v in rows.items()}}
+        if sc is scene:
+            ref_img, sv2 = img, sv
+    # the CPU radix sort alone (one thread)
+    sort_alone = {}
+    keys2, ids2 = oracle_py.preprocess_visible(sv2.pos.reshape(-1, 3), cam)
+    for name, keys in (("reference_microbench_200k_lcg99", lcg_keys(99, 200_000)),
+                       ("config2_depth_keys", keys2)):
+        vals0 = np.arange(len(keys), dtype=np.uint32)
+        for _ in range(warmup):
+            oracle_py.sort_values_by_keys(keys, vals0)
+        ms = []
+        for _ in range(iters):
+            t0 = time.perf_counter()
+            oracle_py.sort_values_by_keys(keys, vals0)
+            ms.append((time.perf_counter() - t0) * 1e3)
+        sort_alone[name] = {"n": int(len(keys)), "ms": _dist(ms)}
+    head = per_config["config2_279k_sh3_1080p"]
+    out = {"value": head["frames_per_s"], "unit": "frames/s", "cores": threads, "kind": "port",
+           "host_cpu": host_cpu_model(),
+           "sample": f"{iters} full frames of each workload after {warmup} warm-up frames; depth "
+                     f"preprocess and radix sort on 1 thread, vertex stage and UNORM8 blend on "
+                     f"{threads} threads; value = frames/s of the 279,199-splat SH3 1080p frame",
+           "per_config": per_config, "sort_alone": sort_alone}
     if gpu_images:
-        fr = oracle_py.Frame(sv, cam, w, h)
+        fr = oracle_py.Frame(sv2, cam, w, h)
         f64, _ = fr.raster_f64(threads)
         out["gpu_image_errors"] = {
             mode: {"vs_reference_model": image_errors(img, ref_img),
@@ -832,7 +896,7 @@ def run_cuda(args, world, rank, local):
             "e2e": e2e, "gpu_launches": launches_per_frame * args.steps, "clocks": clk,
             "roofline": roofline, "phases": phase_rooflines, "parity_mode": parity}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(scene, cam, w, h, budget_s=args.cpu_budget,
+        line["cpu_baseline"] = cpu_baseline(scene, cam, w, h, iters=args.cpu_iters,
                                             gpu_images={"fp32": img_fp32, "unorm8": img_unorm8})
     ctx.close()
     if not args.no_batched and world == 1:
@@ -855,7 +919,8 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
-    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--cpu-iters", type=int, default=30,
+                    help="timed CPU-baseline frames per workload (after 5 warm-up frames)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=3)
