@@ -1,3 +1,4 @@
+#include <cmath>
 // Plain frames: one view of the frame pipeline (no device code in this file).
 
 #include <cstring>
@@ -76,8 +77,7 @@ void Renderer::load_scene(const HostScene &s) {
   GSR_CUDA(cudaStreamSynchronize(stream_));
   scene_.reset();
   scene_ = upload_scene(s, stream_);
-  has_frame_ = false;
-  force_sort_ = true;
+  scene_changed();
 }
 
 void Renderer::load_scene_packed(const HostScene &s) {
@@ -87,8 +87,7 @@ void Renderer::load_scene_packed(const HostScene &s) {
   GSR_CUDA(cudaStreamSynchronize(stream_));
   std::unique_ptr<DeviceScene> sc = upload_scene_packed(s, stream_);
   scene_ = std::move(sc);
-  has_frame_ = false;
-  force_sort_ = true;
+  scene_changed();
 }
 
 void Renderer::load_scene_path(const std::string &path) {
@@ -97,8 +96,7 @@ void Renderer::load_scene_path(const std::string &path) {
   // The current scene stays loaded until the new one is complete.
   std::unique_ptr<DeviceScene> sc = load_scene_file(path, stream_, {});
   scene_ = std::move(sc);
-  has_frame_ = false;
-  force_sort_ = true;
+  scene_changed();
 }
 
 void Renderer::ensure_image() {
@@ -154,15 +152,52 @@ std::vector<ViewSpec> Renderer::one_view(const GsplatCamera &cam) {
 
 void Renderer::set_sort_interval(uint32_t interval) { sort_interval_ = interval; }
 
+void Renderer::scene_changed() {
+  has_frame_ = false;
+  force_sort_ = true;
+  // The stale-order translation bound: 2% of the scene's bounding-box
+  // diagonal, at least 1e-4 (surface_session.rs:660-674, f32 as there).
+  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  const std::vector<float> &pos = scene_->positions;
+  for (size_t i = 0; i + 2 < pos.size(); i += 3)
+    for (int a = 0; a < 3; ++a) {
+      mn[a] = std::fmin(mn[a], pos[i + a]);
+      mx[a] = std::fmax(mx[a], pos[i + a]);
+    }
+  const float dx = mx[0] - mn[0], dy = mx[1] - mn[1], dz = mx[2] - mn[2];
+  const float diagonal = std::sqrt(dx * dx + dy * dy + dz * dz);
+  order_translation_limit_ = pos.empty() ? 1e-4f : std::fmax(diagonal * 0.02f, 1e-4f);
+}
+
+// The reference's async_order_pose_compatible (surface_session.rs:1255-1272):
+// an order sorted for camera `a` may be drawn for camera `b` while b's
+// position is within `limit` of a's and the rotation between them is at
+// most 0.01 rad.
+bool order_pose_compatible(const GsplatCamera &a, const GsplatCamera &b, float limit) {
+  const float dx = b.position[0] - a.position[0];
+  const float dy = b.position[1] - a.position[1];
+  const float dz = b.position[2] - a.position[2];
+  if (dx * dx + dy * dy + dz * dz > limit * limit) return false;
+  const float *qa = a.rotation_xyzw, *qb = b.rotation_xyzw;
+  const float dot =
+      std::fmin(std::fmax(std::fabs(qa[0] * qb[0] + qa[1] * qb[1] + qa[2] * qb[2] + qa[3] * qb[3]),
+                          0.0f),
+                1.0f);
+  return 2.0f * std::acos(dot) <= 0.01f;
+}
+
 // Interval 0 sorts every frame, as the reference's Renderer::render_frame
 // does. Otherwise the reference's SurfaceFrameState::plan
 // (surface_session.rs:536-596): sort when forced, when there is no order
-// yet, or when the camera has changed `interval` times since the last sort.
+// yet, or when the camera has changed `interval` times since the last sort;
+// and, as for the reference's reused orders (surface_session.rs:1149-1153),
+// when the camera has left the pose bound of the order's own camera.
 void Renderer::plan_order(const GsplatCamera &cam) {
   const bool changed = !has_last_camera_ || std::memcmp(&cam, &last_camera_, sizeof cam) != 0;
   if (changed) ++changes_since_sort_;
   const bool refresh = sort_interval_ == 0 || force_sort_ ||
-                       (changed && changes_since_sort_ >= sort_interval_);
+                       (changed && changes_since_sort_ >= sort_interval_) ||
+                       !order_pose_compatible(sorted_camera_, cam, order_translation_limit_);
   pipe_->set_reuse_order(!refresh);
   last_camera_ = cam;
   has_last_camera_ = true;
@@ -172,6 +207,7 @@ void Renderer::finish_order() {
   if (!pipe_->last_reused_order()) {
     changes_since_sort_ = 0;
     force_sort_ = false;
+    sorted_camera_ = last_camera_;
   }
 }
 

@@ -15,6 +15,10 @@ namespace gsr {
 
 using FrameResult = RunResult;
 
+// True when an order sorted for camera `a` may still be drawn for camera `b`
+// (the reference's stale-order pose bound; `limit` is the translation bound).
+bool order_pose_compatible(const GsplatCamera &a, const GsplatCamera &b, float limit);
+
 // Checks for a usable sm_100 device and returns its ordinal; throws
 // Error(Unsupported) otherwise.
 int require_b200();
@@ -39,7 +43,11 @@ class Renderer {
   // reference's context does. k >= 1: the reference's surface sort interval —
   // the order is re-sorted when the camera has changed k times since the
   // last sort; other frames reuse the last sorted visible order with the new
-  // camera's projection.
+  // camera's projection, but only while the camera stays within the
+  // reference's stale-order pose bound of the camera that order was sorted
+  // for (translation at most 2% of the scene's bounding-box diagonal, at
+  // least 1e-4; rotation at most 0.01 rad; surface_session.rs:23-24,
+  // 670-674, 1255-1272): a larger move re-sorts at once.
   void set_sort_interval(uint32_t interval);
   uint32_t sort_interval() const { return sort_interval_; }
 
@@ -85,6 +93,7 @@ class Renderer {
   void ensure_image();
   void plan_order(const GsplatCamera &cam);  // sets the pipeline's order reuse
   void finish_order();
+  void scene_changed();  // forces a sort and takes the scene's translation bound
 
   int device_ = 0;
   cudaStream_t stream_ = nullptr;
@@ -93,6 +102,8 @@ class Renderer {
   uint32_t sort_interval_ = 0, changes_since_sort_ = 0;
   bool force_sort_ = true, has_last_camera_ = false;
   GsplatCamera last_camera_{};
+  GsplatCamera sorted_camera_{};      // the camera the current order was sorted for
+  float order_translation_limit_ = 1e-4f;
   std::unique_ptr<Pipeline> pipe_;
   std::unique_ptr<DeviceScene> scene_;
   FrameResult last_;

@@ -85,6 +85,12 @@ typedef struct OrcFrameParams {
 
 /* ---- gsplat-core ---- */
 int32_t orc_camera_validate(const OrcCamera *camera);
+/* Automatic framing of gsplat_context_set_auto_camera
+ * (crates/gsplat-ffi-c/src/lib.rs:1593-1779); 1 for an empty scene. */
+int32_t orc_auto_camera(const float *positions, uint64_t n, uint32_t width, uint32_t height,
+                        OrcCamera *out);
+/* camera_rotation_looking_at (crates/gsplat-ffi-c/src/lib.rs:1679-1733). */
+void orc_camera_look_at(const float position[3], const float target[3], float q[4]);
 int32_t orc_config_validate(uint32_t width, uint32_t height);
 int32_t orc_scene_validate(const OrcScene *scene, uint64_t sh_rest_len);
 

@@ -393,3 +393,104 @@ void orc_pack_pairs(const uint32_t *keys, const uint32_t *values, uint64_t n, in
 }
 
 }  // extern "C"
+
+// ---- automatic framing (crates/gsplat-ffi-c/src/lib.rs:1593-1779) --------
+// The reference's context camera for gsplat_context_set_auto_camera: the
+// scene's bounding box (scene_bounds, :1764-1779), a distance that frames it
+// at the default camera's field of view (auto_surface_camera_control,
+// :1601-1637), and the camera placed at yaw = pitch = 0 looking at the box
+// centre (surface_camera_from_control, :1652-1677) with the rotation of
+// camera_rotation_looking_at / quat_from_camera_basis (:1679-1733). Every
+// step is one f32 operation in the reference's order.
+namespace {
+struct V3 {
+  float x, y, z;
+};
+V3 v3_sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+V3 v3_cross(V3 a, V3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+bool v3_normalize(V3 v, V3 &out) {
+  const float len = std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
+  if (!std::isfinite(len) || len <= 1.0e-6f) return false;
+  const float inv = 1.0f / len;
+  out = {v.x * inv, v.y * inv, v.z * inv};
+  return true;
+}
+void look_at_rotation(V3 position, V3 target, float q[4]) {
+  V3 forward;
+  if (!v3_normalize(v3_sub(target, position), forward)) forward = {0.0f, 0.0f, 1.0f};
+  const V3 world_up = std::fabs(forward.y) > 0.98f ? V3{0.0f, 0.0f, 1.0f} : V3{0.0f, 1.0f, 0.0f};
+  V3 right;
+  if (!v3_normalize(v3_cross(world_up, forward), right)) right = {1.0f, 0.0f, 0.0f};
+  const V3 up = v3_cross(forward, right);
+  // rotation matrix with columns right, up, forward -> quaternion
+  const float m00 = right.x, m01 = up.x, m02 = forward.x;
+  const float m10 = right.y, m11 = up.y, m12 = forward.y;
+  const float m20 = right.z, m21 = up.z, m22 = forward.z;
+  const float trace = m00 + m11 + m22;
+  float x, y, z, w;
+  if (trace > 0.0f) {
+    const float s = std::sqrt(trace + 1.0f) * 2.0f;
+    x = (m21 - m12) / s; y = (m02 - m20) / s; z = (m10 - m01) / s; w = 0.25f * s;
+  } else if (m00 > m11 && m00 > m22) {
+    const float s = std::sqrt(1.0f + m00 - m11 - m22) * 2.0f;
+    x = 0.25f * s; y = (m01 + m10) / s; z = (m02 + m20) / s; w = (m21 - m12) / s;
+  } else if (m11 > m22) {
+    const float s = std::sqrt(1.0f + m11 - m00 - m22) * 2.0f;
+    x = (m01 + m10) / s; y = 0.25f * s; z = (m12 + m21) / s; w = (m02 - m20) / s;
+  } else {
+    const float s = std::sqrt(1.0f + m22 - m00 - m11) * 2.0f;
+    x = (m02 + m20) / s; y = (m12 + m21) / s; z = 0.25f * s; w = (m10 - m01) / s;
+  }
+  const float norm = std::fmax(std::sqrt(x * x + y * y + z * z + w * w), 1.0e-6f);
+  q[0] = x / norm; q[1] = y / norm; q[2] = z / norm; q[3] = w / norm;
+}
+// f32::to_radians: the value times (PI / 180) formed in f32.
+float to_radians_f32(float deg) { return deg * (3.14159265358979323846f / 180.0f); }
+}  // namespace
+
+extern "C" void orc_camera_look_at(const float position[3], const float target[3], float q[4]) {
+  look_at_rotation({position[0], position[1], position[2]}, {target[0], target[1], target[2]}, q);
+}
+
+extern "C" int32_t orc_auto_camera(const float *positions, uint64_t n, uint32_t width,
+                                   uint32_t height, OrcCamera *out) {
+  if (n == 0) return 1;  // the reference's InvalidArgument for an empty scene
+  V3 mn{INFINITY, INFINITY, INFINITY}, mx{-INFINITY, -INFINITY, -INFINITY};
+  for (uint64_t i = 0; i < n; ++i) {
+    const float *p = positions + 3 * i;
+    mn.x = std::fmin(mn.x, p[0]); mn.y = std::fmin(mn.y, p[1]); mn.z = std::fmin(mn.z, p[2]);
+    mx.x = std::fmax(mx.x, p[0]); mx.y = std::fmax(mx.y, p[1]); mx.z = std::fmax(mx.z, p[2]);
+  }
+  const V3 center{(mn.x + mx.x) * 0.5f, (mn.y + mx.y) * 0.5f, (mn.z + mx.z) * 0.5f};
+  const V3 extent{mx.x - mn.x, mx.y - mn.y, mx.z - mn.z};
+  const float half_x = std::fmax(extent.x * 0.5f, 1e-3f);
+  const float half_y = std::fmax(extent.y * 0.5f, 1e-3f);
+  const float half_z = std::fmax(extent.z * 0.5f, 1e-3f);
+  const float aspect = (float)width / (float)height;
+  const float default_fov = to_radians_f32(60.0f);  // Camera::default()
+  const float vfov = std::fmax(default_fov, 1e-3f);
+  const float hfov = 2.0f * std::atan(std::tan(vfov * 0.5f) * aspect);
+  const float dist_y = half_y / std::tan(vfov * 0.5f);
+  const float dist_x = half_x / std::tan(hfov * 0.5f);
+  const float distance = (std::fmax(dist_y, dist_x) + half_z) * 1.2f;
+  const float radius = std::fmax(std::fmax(half_x, half_y), half_z);
+  // surface_camera_from_control with yaw = pitch = 0 (pitch clamped to +-1.45)
+  const float yaw = 0.0f, pitch = 0.0f;
+  const float cos_pitch = std::cos(pitch);
+  const V3 offset{std::sin(yaw) * cos_pitch * distance, std::sin(pitch) * distance,
+                  -std::cos(yaw) * cos_pitch * distance};
+  const V3 pos{center.x + offset.x, center.y + offset.y, center.z + offset.z};
+  OrcCamera c;
+  c.position[0] = pos.x; c.position[1] = pos.y; c.position[2] = pos.z;
+  look_at_rotation(pos, center, c.rotation_xyzw);
+  c.vertical_fov_radians = default_fov;
+  const float r = std::fmax(radius, 1.0e-3f);
+  c.near_plane = std::fmax(distance - r * 2.0f, 0.01f);
+  c.far_plane = std::fmax(distance + r * 8.0f, 100.0f);
+  const float asp = std::fmax((float)width / (float)std::max<uint32_t>(height, 1u), 1.0e-3f);
+  if (asp < 0.6f) c.vertical_fov_radians = to_radians_f32(65.0f);
+  *out = c;
+  return 0;
+}

@@ -77,6 +77,11 @@ def lib():
         L.orc_scene_validate.argtypes = [ctypes.POINTER(OrcScene), ctypes.c_uint64]
         L.orc_scene_validate.restype = ctypes.c_int32
         L.orc_view_rotation.argtypes = [_f32p, _f32p]
+        L.orc_auto_camera.argtypes = [_f32p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
+                                      ctypes.POINTER(OrcCamera)]
+        L.orc_auto_camera.restype = ctypes.c_int32
+        L.orc_camera_look_at.argtypes = [_f32p, _f32p, _f32p]
+        L.orc_camera_look_at.restype = None
         L.orc_quat_inverse.argtypes = [_f32p, _f32p]
         L.orc_frame_params.argtypes = [ctypes.POINTER(OrcCamera), ctypes.c_uint32, ctypes.c_uint32,
                                        ctypes.c_uint32, ctypes.c_uint32,
@@ -214,6 +219,26 @@ class PackedSceneView(SceneView):
 
 def camera_validate(cam):
     return lib().orc_camera_validate(ctypes.byref(camera(cam)))
+
+
+def auto_camera(positions, width, height):
+    """gsplat_context_set_auto_camera's camera for a scene (dict of floats)."""
+    pos = np.ascontiguousarray(positions, np.float32).reshape(-1)
+    c = OrcCamera()
+    rc = lib().orc_auto_camera(_p(pos, _f32p), pos.size // 3, width, height, ctypes.byref(c))
+    if rc != 0:
+        raise ValueError("empty scene")
+    return {"position": list(c.position), "rotation_xyzw": list(c.rotation_xyzw),
+            "vertical_fov_radians": c.vertical_fov_radians, "near_plane": c.near_plane,
+            "far_plane": c.far_plane}
+
+
+def camera_look_at(position, target):
+    p = np.ascontiguousarray(position, np.float32)
+    t = np.ascontiguousarray(target, np.float32)
+    q = np.zeros(4, np.float32)
+    lib().orc_camera_look_at(_p(p, _f32p), _p(t, _f32p), _p(q, _f32p))
+    return q
 
 
 def view_rotation(q):

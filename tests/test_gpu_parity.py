@@ -393,10 +393,11 @@ def test_sort_interval_reuses_the_last_order(oracle):
     """The reference's surface sort cadence: with interval 3 the depth order
     is re-sorted on the 3rd camera change; frames in between draw the last
     sorted order with their own projection, equal to the oracle given that
-    stale order."""
+    stale order. The orbit steps (0.0015 rad, 7.5 mm) stay inside the
+    reference's stale-order pose bound."""
     scene, _, w, h = gsplat_scenes.config1(seed=21)
     sv = oracle.SceneView(scene)
-    cams = [gsplat_scenes.camera((5.0 * math.sin(0.05 * k), 0.3, -5.0 * math.cos(0.05 * k)),
+    cams = [gsplat_scenes.camera((5.0 * math.sin(0.0015 * k), 0.3, -5.0 * math.cos(0.0015 * k)),
                                  (0, 0, 0), 50.0) for k in range(6)]
     ctx = _ctx(w, h)
     ctx.set_debug_taps(True)
@@ -434,6 +435,85 @@ def test_sort_interval_reuses_the_last_order(oracle):
     ctx.render_frame()
     assert ctx.frame_counts().sort_refreshed == 1
     assert np.array_equal(ctx.readback_rgba8(), img)
+
+
+def test_auto_camera_matches_the_oracle(oracle):
+    """gsplat_context_set_auto_camera frames the scene exactly as the
+    reference's context does (crates/gsplat-ffi-c/src/lib.rs:1593-1779): the
+    camera read back equals the oracle's restatement bit for bit, for the
+    reference's minimal_ascii.ply, the 16k and 279k synthetic scenes, and a
+    portrait image (aspect below 0.6 takes the 65 degree field of view)."""
+    import json
+
+    import gsplat_scenes as gs
+    with open(os.path.join(GOLDEN, "minimal_ascii_scene.json")) as f:
+        minimal = gs.scene_from_json(json.load(f))
+    scenes = [("minimal_ascii", minimal, 64, 64), ("config1", gs.config1(seed=0)[0], 256, 256),
+              ("config2", gs.config2()[0], 1920, 1080), ("portrait", gs.config1(seed=4)[0], 200, 400)]
+    for name, scene, w, h in scenes:
+        ctx = _ctx(w, h)
+        ctx.load_scene(scene)
+        ctx.set_auto_camera()
+        got = ctx.camera().to_dict()
+        want = oracle.auto_camera(scene["positions"], w, h)
+        for k in ("position", "rotation_xyzw", "vertical_fov_radians", "near_plane", "far_plane"):
+            a = np.asarray(got[k], np.float32).view(np.uint32)
+            b = np.asarray(want[k], np.float32).view(np.uint32)
+            assert np.array_equal(a, b), (name, k, got[k], want[k])
+        ctx.render_frame()
+        assert ctx.stats().visible_count > 0, name
+        ctx.close()
+    # the PLY path keeps the host positions the framing reads
+    ctx = _ctx(64, 64)
+    ctx.load_scene_path(os.path.join(GOLDEN, "minimal_ascii.ply"))
+    ctx.set_auto_camera()
+    want = oracle.auto_camera(minimal["positions"], 64, 64)
+    assert np.array_equal(np.asarray(ctx.camera().to_dict()["position"], np.float32),
+                          np.asarray(want["position"], np.float32))
+    ctx.close()
+
+
+def test_sort_interval_pose_bound(oracle):
+    """A reused order is dropped, and the frame sorted, as soon as the camera
+    leaves the reference's stale-order pose bound of the camera the order was
+    sorted for (surface_session.rs:23-24, 1255-1272): rotation above 0.01 rad,
+    or translation above 2% of the scene's bounding-box diagonal."""
+    scene, _, w, h = gsplat_scenes.config1(seed=22)
+    sv = oracle.SceneView(scene)
+    pos = scene["positions"].astype(np.float32)
+    ext = pos.max(axis=0) - pos.min(axis=0)
+    diag = float(np.sqrt(np.float32((ext * ext).sum())))
+    base = (0.0, 0.3, -5.0)
+    ctx = _ctx(w, h)
+    ctx.set_debug_taps(True)
+    ctx.load_scene(scene)
+    ctx.set_sort_interval(8)
+
+    def frame(cam, expect_sorted):
+        ctx.set_camera(cam)
+        ctx.render_frame()
+        assert bool(ctx.frame_counts().sort_refreshed) == expect_sorted, cam
+        return ctx.debug_order()
+
+    frame(gsplat_scenes.camera(base, (0, 0, 0), 50.0), True)  # first frame sorts
+    # inside the bound: 0.006 rad of yaw, translation well under 2% of the diagonal
+    yaw = 0.003
+    small = gsplat_scenes.camera((5.0 * math.sin(yaw), 0.3, -5.0 * math.cos(yaw)), (0, 0, 0), 50.0)
+    frame(small, False)
+    # rotation beyond 0.01 rad from the sorted camera (the look-at turns ~0.02 rad)
+    yaw = 0.02
+    turned = gsplat_scenes.camera((5.0 * math.sin(yaw), 0.3, -5.0 * math.cos(yaw)), (0, 0, 0), 50.0)
+    order = frame(turned, True)
+    assert np.array_equal(order, oracle.Frame(sv, turned, w, h).order)
+    # translation beyond 2% of the diagonal with the same rotation
+    shifted = dict(turned, position=[turned["position"][0], turned["position"][1] + 0.03 * diag,
+                                     turned["position"][2]])
+    order = frame(shifted, True)
+    assert np.array_equal(order, oracle.Frame(sv, shifted, w, h).order)
+    # a move of 1% of the diagonal stays inside the bound: the order is reused
+    near = dict(shifted, position=[shifted["position"][0] + 0.01 * diag, shifted["position"][1],
+                                   shifted["position"][2]])
+    assert np.array_equal(frame(near, False), order)
 
 
 def test_benchmark_artifact_from_rendered_frames(tmp_path):

@@ -213,3 +213,28 @@ def test_fp32_tile_raster_vs_reference_models(oracle):
     rgb = d8[..., :3] / 255.0
     assert rgb.mean() <= 1.0 / 255.0
     assert (rgb > 3.0 / 255.0).any(axis=-1).mean() <= 0.001
+
+
+def _f32_bits(values):
+    return np.asarray(values, np.float32).view(np.uint32)
+
+
+def test_look_at_rotation_matches_the_oracle(oracle):
+    """The product's camera_rotation_looking_at (host code, no GPU) equals the
+    oracle's restatement of crates/gsplat-ffi-c/src/lib.rs:1679-1733 bit for
+    bit, including forward vectors near +-Y (the alternative up vector) and
+    a target on the camera (the +Z fallback)."""
+    import gsplat_ffi as ffi
+
+    rng = np.random.default_rng(31)
+    cases = [((0.0, 0.0, -5.0), (0.0, 0.0, 0.0)), ((0.0, 5.0, 0.0), (0.0, 0.0, 0.0)),
+             ((0.0, -5.0, 0.01), (0.0, 0.0, 0.0)), ((1.0, 2.0, 3.0), (1.0, 2.0, 3.0)),
+             ((3.0, 0.0, 0.0), (-3.0, 0.0, 0.0))]
+    for _ in range(500):
+        cases.append((tuple(rng.normal(0, 5, 3)), tuple(rng.normal(0, 1, 3))))
+    for pos, tgt in cases:
+        pos32 = np.float32(pos)
+        tgt32 = np.float32(tgt)
+        want = oracle.camera_look_at(pos32, tgt32)
+        got = ffi.camera_look_at([float(v) for v in pos32], [float(v) for v in tgt32], 1.0)
+        assert np.array_equal(_f32_bits(list(got.rotation_xyzw)), _f32_bits(want)), (pos, tgt)
