@@ -51,6 +51,12 @@ def bench_config(world):
             "parallelism": f"CUDA arm: one replica per GPU (x{world}), no collective on the "
                            "data path; CPU arm: host threads on rank 0"}
 FALLBACK_HBM_GBS = 6650.0
+# Per-launch counters of the 1080p raster (raster_fp32_kernel<16, 256>) from
+# one ncu capture of this workload (profiles/frame_279k_sh3_1080p.md gives
+# the command): DRAM bytes read + written, warp instructions issued, and
+# executed FP32 thread operations (2 x FFMA + FADD + FMUL). None until
+# captured for the current kernel.
+NCU_RASTER = None
 
 
 def dist_setup():
@@ -730,6 +736,67 @@ def measure_packed(ffi, torch, frames=60):
     return out
 
 
+NOMINAL_HBM_GBS = 8000.0  # B200 HBM3e data-sheet bandwidth, for context beside the measured peak
+
+
+def measure_config3(ffi, torch, frames=20):
+    """The sort/raster stress frame: 3,000,000 SH3 splats (uniform 10^3 box
+    plus a dense core), camera inside the volume, 3840x2160, 16x16 tiles.
+    Per-phase device time (median over `frames`, L2 flushed between frames),
+    achieved GB/s of each phase's algorithmic bytes against the measured HBM
+    copy peak and the nominal 8 TB/s, in both blend modes."""
+    scene, cam, w, h = gsplat_scenes.config3()
+    peaks = {}
+    if os.path.exists(PEAKS_FILE):
+        with open(PEAKS_FILE) as f:
+            peaks = json.load(f)
+    hbm = peaks.get("hbm_gbs") or FALLBACK_HBM_GBS
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
+    n = scene["positions"].shape[0]
+    tiles = ((w + 15) // 16) * ((h + 15) // 16)
+    tile_passes = 1
+    while (1 << (8 * tile_passes)) < tiles:
+        tile_passes += 1
+    out = {"workload": "3,000,000 synthetic splats, SH degree 3, uniform 10^3 box + dense core, "
+                       "camera inside the volume, 3840x2160, 16x16 tiles",
+           "hbm_peak_gbs": hbm, "hbm_peak_source": "measured" if peaks.get("hbm_gbs") else "fallback",
+           "nominal_hbm_gbs": NOMINAL_HBM_GBS}
+    with ffi.Context(w, h) as ctx:
+        ctx.load_scene(scene)
+        ctx.set_camera(cam)
+        for blend, name in ((0, "fp32"), (1, "unorm8")):
+            ctx.set_blend_mode(blend)
+            for _ in range(3):
+                ctx.render_frame()
+            counts = ctx.frame_counts()
+            stream = torch.cuda.ExternalStream(ctx.stream())
+            acc = {}
+            for i in range(frames):
+                with torch.cuda.stream(stream):
+                    flush.fill_(i)
+                ctx.render_frame()
+                for k, v in ctx.phase_times().items():
+                    acc.setdefault(k, []).append(v)
+            ph = {k: float(np.median(v)) for k, v in acc.items()}
+            phases = {}
+            for k, ms in ph.items():
+                b = algorithmic_bytes(k, counts, n, 12, w, h, tile_passes)
+                gbs = b / (ms * 1e-3) / 1e9 if ms > 0 else None
+                phases[k] = {"ms": ms, "bytes": b, "gbs": gbs,
+                             "frac_measured": gbs / hbm if gbs else None,
+                             "frac_nominal": gbs / NOMINAL_HBM_GBS if gbs else None}
+            ps = ["preprocess", "depth_sort", "emit", "tile_sort"]
+            ps_bytes = sum(phases[k]["bytes"] for k in ps)
+            ps_ms = sum(phases[k]["ms"] for k in ps)
+            out[name] = {"frame_ms": sum(ph.values()), "frames_per_s": 1000.0 / sum(ph.values()),
+                         "visible": int(counts.visible), "drawn": int(counts.drawn),
+                         "tile_pairs": int(counts.tile_keys), "phases": phases,
+                         "preprocess_emit_sort_gbs": ps_bytes / (ps_ms * 1e-3) / 1e9,
+                         "preprocess_emit_sort_frac_measured":
+                             ps_bytes / (ps_ms * 1e-3) / 1e9 / hbm}
+    return out
+
+
 def run_sections_only(args, ffi, torch):
     """The batched and/or served sections alone (no plain-frame line), for
     profiling those workloads by themselves."""
@@ -744,6 +811,8 @@ def run_sections_only(args, ffi, torch):
         out["ingest"] = measure_ingest(ffi, args.ingest_splats)
     if "packed" in args.only:
         out["packed"] = measure_packed(ffi, torch)
+    if "config3" in args.only:
+        out["config3"] = measure_config3(ffi, torch)
     print(json.dumps(out), flush=True)
 
 
@@ -877,6 +946,25 @@ def run_cuda(args, world, rank, local):
                 "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                 "peak_source": "measured" if hbm else "fallback",
                 "algorithmic_bytes": bytes_dom}
+    if dominant == "raster":
+        # The raster's limiter is FP32 issue, not HBM: its records and ids
+        # stay in L2. Issue rate = warp instructions per launch (ncu) over the
+        # live launch time, against 4 schedulers x SMs x the live SM clock;
+        # FP32 rate = executed FP32 operations (ncu) over the live launch
+        # time, against this device's measured FMA throughput.
+        raster_s = phases["raster"] * 1e-3
+        sms = ffi.device_info()["sm_count"]
+        fp32_peak, _ = ffi.measure_fp32_peak()
+        roofline["limiter"] = "fp32_issue"
+        roofline["fp32_peak_tflops"] = fp32_peak
+        roofline["fp32_peak_source"] = "measured (FMA-only kernel, gsplat_cuda_measure_fp32_peak)"
+        if NCU_RASTER:
+            roofline["traffic"] = NCU_RASTER["dram_bytes"]
+            roofline["issue_inst_per_launch"] = NCU_RASTER["warp_inst"]
+            roofline["fp32_flop_per_launch"] = NCU_RASTER["thread_flop"]
+            roofline["fp32_tflops"] = NCU_RASTER["thread_flop"] / raster_s / 1e12
+            roofline["fp32_frac"] = roofline["fp32_tflops"] / fp32_peak
+            roofline["counters_source"] = NCU_RASTER["source"]
     phase_rooflines = {}
     for k, ms in phases.items():
         b = algorithmic_bytes(k, counts, scene["positions"].shape[0], planes, w, h, tile_passes)
@@ -895,6 +983,10 @@ def run_cuda(args, world, rank, local):
                              "tile_pairs": int(counts.tile_keys)},
             "e2e": e2e, "gpu_launches": launches_per_frame * args.steps, "clocks": clk,
             "roofline": roofline, "phases": phase_rooflines, "parity_mode": parity}
+    if roofline.get("issue_inst_per_launch") and clk.get("sm_mhz"):
+        issue_peak = ffi.device_info()["sm_count"] * 4 * clk["sm_mhz"] * 1e6
+        roofline["issue_frac"] = (roofline["issue_inst_per_launch"] /
+                                  (phases["raster"] * 1e-3) / issue_peak)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(scene, cam, w, h, iters=args.cpu_iters,
                                             gpu_images={"fp32": img_fp32, "unorm8": img_unorm8})
@@ -908,6 +1000,8 @@ def run_cuda(args, world, rank, local):
         line["ingest"] = measure_ingest(ffi, args.ingest_splats)
     if not args.no_packed and world == 1:
         line["packed"] = measure_packed(ffi, torch)
+    if not args.no_config3 and world == 1:
+        line["config3"] = measure_config3(ffi, torch)
     replicas.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -933,10 +1027,12 @@ def main():
                     help="also write the plain frames as a v1 benchmark artifact into this folder")
     ap.add_argument("--no-ingest", action="store_true")
     ap.add_argument("--no-packed", action="store_true")
+    ap.add_argument("--no-config3", action="store_true")
     ap.add_argument("--ingest-splats", type=int, default=279_199,
                     help="splats of the PLY ingestion workload")
     ap.add_argument("--only", default="",
-                    help="comma list of batched,served,ingest,packed: run just those sections")
+                    help="comma list of batched,served,ingest,packed,config3: run just those "
+                         "sections")
     args = ap.parse_args()
     args.only = [x for x in args.only.split(",") if x]
     world, rank, local = dist_setup()

@@ -662,6 +662,14 @@ int32_t gsplat_cuda_device_info(char *name, uint64_t name_capacity, int32_t *sm_
   });
 }
 
+int32_t gsplat_cuda_measure_fp32_peak(double *out_tflops, double *out_ms) {
+  return guarded("gsplat_cuda_measure_fp32_peak", [&]() -> int32_t {
+    if (!out_tflops) return fail(Code::InvalidArgument, "gsplat_cuda_measure_fp32_peak: out is null");
+    gsr::measure_fp32_peak(out_tflops, out_ms);
+    return ok();
+  });
+}
+
 // ---- batched frames (gsplat_cuda.h) ----------------------------------------
 
 int32_t gsplat_batch_create(GsplatBatch **out_batch) {

@@ -26,14 +26,6 @@ namespace {
 constexpr uint64_t kMaxItems = (1u << 30) - 1;
 inline uint64_t align256(uint64_t v) { return (v + 255) & ~uint64_t(255); }
 
-void require_device() {
-  int count = 0;
-  cudaError_t e = cudaGetDeviceCount(&count);
-  if (e != cudaSuccess || count == 0) {
-    cudaGetLastError();
-    throw Error(Code::Unsupported, "no CUDA device");
-  }
-}
 
 __global__ void invert_copy_kernel(const uint32_t *src, uint32_t *dst, uint32_t n) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -83,6 +75,15 @@ struct Stream {
 };
 
 }  // namespace
+
+void require_device() {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    throw Error(Code::Unsupported, "no CUDA device");
+  }
+}
 
 void sort_values_by_keys_host(const uint32_t *keys, uint32_t *values, uint64_t n) {
   if (n <= 1) return;

@@ -20,6 +20,11 @@ void sort_pairs_host(uint32_t *keys, uint32_t *values, uint64_t n);
 
 void device_info(char *name, uint64_t name_capacity, int32_t *sm_count, int32_t *cc_major,
                  int32_t *cc_minor);
+// Throws Error(Unsupported) when no CUDA device is present.
+void require_device();
+// FP32 FMA throughput of the current device (probe.cu): the best of five
+// timed launches of an FMA-only kernel, in TFLOP/s, and that launch's time.
+void measure_fp32_peak(double *tflops, double *best_ms);
 
 // The same sort on caller-owned device buffers, with all scratch in a static
 // device array (sort_noalloc.cu); never allocates. Returns Ok or an error code

@@ -293,6 +293,8 @@ _SIGS = [
     ("gsplat_cuda_device_info", ctypes.c_int32,
      [ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32),
       ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
+    ("gsplat_cuda_measure_fp32_peak", ctypes.c_int32,
+     [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
 ]
 
 _lib = None
@@ -766,6 +768,13 @@ def camera_look_at(position, target, fov, near=0.01, far=1000.0):
     c = GsplatCamera()
     check(lib().gsplat_camera_look_at(p, t, fov, near, far, ctypes.byref(c)))
     return c
+
+
+def measure_fp32_peak():
+    """The device's measured FP32 FMA throughput: (TFLOP/s, best launch ms)."""
+    t, ms = ctypes.c_double(), ctypes.c_double()
+    check(lib().gsplat_cuda_measure_fp32_peak(ctypes.byref(t), ctypes.byref(ms)))
+    return t.value, ms.value
 
 
 def device_info():

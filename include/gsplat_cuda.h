@@ -410,6 +410,12 @@ int32_t gsplat_camera_look_at(const float position[3], const float target[3],
                               float vertical_fov_radians, float near_plane, float far_plane,
                               GsplatCamera *out_camera);
 
+/* No counterpart in the reference: the FP32 FMA throughput of the current
+ * device, measured by an FMA-only kernel (best of five launches after a
+ * warm-up; about 20 ms), in TFLOP/s, and the best launch's time in ms
+ * (out_ms may be NULL). The benchmark uses it as the FP32 roofline. */
+int32_t gsplat_cuda_measure_fp32_peak(double *out_tflops, double *out_ms);
+
 /* Name, SM count and compute capability of the current CUDA device. */
 int32_t gsplat_cuda_device_info(char *name, uint64_t name_capacity, int32_t *sm_count,
                                 int32_t *cc_major, int32_t *cc_minor);

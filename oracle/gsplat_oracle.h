@@ -154,6 +154,18 @@ void orc_sort_u64_pairs_stable(uint64_t *keys, uint32_t *values, uint64_t n);
 
 /* ---- compositing ---- */
 float orc_exp_neg(float x);
+/* Row ranges [y0, y1) of the compositors below (other rows zero). */
+void orc_raster_unorm8_rows(const OrcRecord *records, const OrcProjected *proj,
+                            const uint32_t *order, uint64_t v, uint32_t width, uint32_t height,
+                            uint8_t *rgba, int32_t threads, uint32_t y0, uint32_t y1);
+void orc_raster_f64_rows(const OrcRecord *records, const OrcProjected *proj,
+                         const uint32_t *order, uint64_t v, uint32_t width, uint32_t height,
+                         uint8_t *rgba, double *rgba_f64, int32_t threads, uint32_t y0,
+                         uint32_t y1);
+void orc_raster_tiles_fp32_rows(const OrcRecord *records, const uint32_t *ranges,
+                                const uint32_t *sorted_ids, uint32_t width, uint32_t height,
+                                uint32_t tile, uint32_t tiles_x, uint8_t *rgba, int32_t threads,
+                                uint32_t y0, uint32_t y1);
 void orc_raster_unorm8(const OrcRecord *records, const OrcProjected *proj,
                        const uint32_t *order, uint64_t v, uint32_t width, uint32_t height,
                        uint8_t *rgba, int32_t threads);

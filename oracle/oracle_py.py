@@ -123,6 +123,17 @@ def lib():
                                         ctypes.c_uint32, ctypes.c_uint32, _u8p, ctypes.c_int32]
         L.orc_raster_f64.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _u32p, ctypes.c_uint64,
                                      ctypes.c_uint32, ctypes.c_uint32, _u8p, _f64p, ctypes.c_int32]
+        L.orc_raster_unorm8_rows.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _u32p,
+                                             ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
+                                             _u8p, ctypes.c_int32, ctypes.c_uint32,
+                                             ctypes.c_uint32]
+        L.orc_raster_f64_rows.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _u32p, ctypes.c_uint64,
+                                          ctypes.c_uint32, ctypes.c_uint32, _u8p, _f64p,
+                                          ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32]
+        L.orc_raster_tiles_fp32_rows.argtypes = [ctypes.c_void_p, _u32p, _u32p, ctypes.c_uint32,
+                                                 ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                                 _u8p, ctypes.c_int32, ctypes.c_uint32,
+                                                 ctypes.c_uint32]
         L.orc_raster_tiles_fp32.argtypes = [ctypes.c_void_p, _u32p, _u32p, ctypes.c_uint32,
                                             ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                             _u8p, ctypes.c_int32]
@@ -346,28 +357,34 @@ class Frame:
     def drawn(self):
         return int(np.count_nonzero(self.proj["flags"] & 2))
 
-    def raster_unorm8(self, threads=8):
+    # rows=(y0, y1): only those rows are composited (the others stay zero)
+
+    def raster_unorm8(self, threads=8, rows=None):
         out = np.zeros(self.width * self.height * 4, np.uint8)
-        lib().orc_raster_unorm8(self.rec.ctypes.data, self.proj.ctypes.data,
-                                _p(self._order_c, _u32p), self.visible, self.width, self.height,
-                                _p(out, _u8p), threads)
+        y0, y1 = rows if rows else (0, self.height)
+        lib().orc_raster_unorm8_rows(self.rec.ctypes.data, self.proj.ctypes.data,
+                                     _p(self._order_c, _u32p), self.visible, self.width,
+                                     self.height, _p(out, _u8p), threads, y0, y1)
         return out.reshape(self.height, self.width, 4)
 
-    def raster_f64(self, threads=8):
+    def raster_f64(self, threads=8, rows=None):
         out = np.zeros(self.width * self.height * 4, np.uint8)
         acc = np.zeros(self.width * self.height * 4, np.float64)
-        lib().orc_raster_f64(self.rec.ctypes.data, self.proj.ctypes.data,
-                             _p(self._order_c, _u32p), self.visible, self.width, self.height,
-                             _p(out, _u8p), _p(acc, _f64p), threads)
+        y0, y1 = rows if rows else (0, self.height)
+        lib().orc_raster_f64_rows(self.rec.ctypes.data, self.proj.ctypes.data,
+                                  _p(self._order_c, _u32p), self.visible, self.width, self.height,
+                                  _p(out, _u8p), _p(acc, _f64p), threads, y0, y1)
         return out.reshape(self.height, self.width, 4), acc.reshape(self.height, self.width, 4)
 
-    def raster_tiles_fp32(self, threads=8):
+    def raster_tiles_fp32(self, threads=8, rows=None):
         out = np.zeros(self.width * self.height * 4, np.uint8)
         ids = self.tile_ids if len(self.tile_ids) else np.zeros(1, np.uint32)
-        lib().orc_raster_tiles_fp32(self.rec.ctypes.data,
-                                    _p(np.ascontiguousarray(self.ranges.reshape(-1)), _u32p),
-                                    _p(np.ascontiguousarray(ids), _u32p), self.width, self.height,
-                                    self.tile, self.tiles_x, _p(out, _u8p), threads)
+        y0, y1 = rows if rows else (0, self.height)
+        lib().orc_raster_tiles_fp32_rows(self.rec.ctypes.data,
+                                         _p(np.ascontiguousarray(self.ranges.reshape(-1)), _u32p),
+                                         _p(np.ascontiguousarray(ids), _u32p), self.width,
+                                         self.height, self.tile, self.tiles_x, _p(out, _u8p),
+                                         threads, y0, y1)
         return out.reshape(self.height, self.width, 4)
 
 

@@ -584,13 +584,35 @@ void orc_raster_unorm8(const OrcRecord *records, const OrcProjected *proj,
   });
 }
 
+// Rows [y0, y1) of the reference image model; the other rows stay zero. A
+// band of a large frame (the 3M-splat 4K stress frame) finishes in seconds.
+void orc_raster_unorm8_rows(const OrcRecord *records, const OrcProjected *proj,
+                            const uint32_t *order, uint64_t v, uint32_t width, uint32_t height,
+                            uint8_t *rgba, int32_t threads, uint32_t y0, uint32_t y1) {
+  std::memset(rgba, 0, (size_t)width * height * 4);
+  y1 = std::min(y1, height);
+  if (y0 >= y1) return;
+  parallel_rows(y1 - y0, threads, [&](uint32_t ya, uint32_t yb) {
+    unorm8_band(records, proj, order, v, width, height, rgba, y0 + ya, y0 + yb);
+  });
+}
+
 // FP64 evaluation of the same image: local coordinates, coverage, weights and
 // blending in double precision, one rounding to UNORM8 at the end.
 void orc_raster_f64(const OrcRecord *records, const OrcProjected *proj, const uint32_t *order,
                     uint64_t v, uint32_t width, uint32_t height, uint8_t *rgba,
                     double *rgba_f64, int32_t threads) {
+  orc_raster_f64_rows(records, proj, order, v, width, height, rgba, rgba_f64, threads, 0, height);
+}
+
+void orc_raster_f64_rows(const OrcRecord *records, const OrcProjected *proj,
+                         const uint32_t *order, uint64_t v, uint32_t width, uint32_t height,
+                         uint8_t *rgba, double *rgba_f64, int32_t threads, uint32_t row0,
+                         uint32_t row1) {
   std::vector<double> acc((size_t)width * height * 4, 0.0);
-  parallel_rows(height, threads, [&](uint32_t ya, uint32_t yb) {
+  row1 = std::min(row1, height);
+  parallel_rows(row1 > row0 ? row1 - row0 : 0, threads, [&](uint32_t ra, uint32_t rb) {
+    const uint32_t ya = row0 + ra, yb = row0 + rb;
     for (uint64_t j = 0; j < v; ++j) {
       uint32_t s = order[j];
       const OrcProjected &p = proj[s];
@@ -635,6 +657,18 @@ void orc_raster_tiles_fp32(const OrcRecord *records, const uint32_t *ranges,
                            uint32_t tile, uint32_t tiles_x, uint8_t *rgba, int32_t threads) {
   parallel_rows(height, threads, [&](uint32_t ya, uint32_t yb) {
     tiles_fp32_band(records, ranges, sorted_ids, width, tile, tiles_x, rgba, ya, yb);
+  });
+}
+
+void orc_raster_tiles_fp32_rows(const OrcRecord *records, const uint32_t *ranges,
+                                const uint32_t *sorted_ids, uint32_t width, uint32_t height,
+                                uint32_t tile, uint32_t tiles_x, uint8_t *rgba, int32_t threads,
+                                uint32_t y0, uint32_t y1) {
+  std::memset(rgba, 0, (size_t)width * height * 4);
+  y1 = std::min(y1, height);
+  if (y0 >= y1) return;
+  parallel_rows(y1 - y0, threads, [&](uint32_t ya, uint32_t yb) {
+    tiles_fp32_band(records, ranges, sorted_ids, width, tile, tiles_x, rgba, y0 + ya, y0 + yb);
   });
 }
 
