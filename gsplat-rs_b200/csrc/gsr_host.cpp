@@ -167,7 +167,12 @@ GsplatCamera auto_camera(const float *p, uint64_t n, uint32_t width, uint32_t he
   }
   GsplatCamera cam = camera_default();
   float aspect = (float)width / (float)height;
-  float vfov = std::fmax(cam.vertical_fov_radians, 1e-3f);
+  // Read through a volatile: tan/atan of the default fov must come from the
+  // C library at run time, as the reference's f32 methods do, never from
+  // the compiler folding a constant (correctly rounded, which can differ in
+  // the last bit).
+  volatile float fov_v = cam.vertical_fov_radians;
+  float vfov = std::fmax((float)fov_v, 1e-3f);
   float hfov = 2.0f * std::atan(std::tan(vfov * 0.5f) * aspect);
   float dist_y = half[1] / std::tan(vfov * 0.5f);
   float dist_x = half[0] / std::tan(hfov * 0.5f);

@@ -469,7 +469,11 @@ extern "C" int32_t orc_auto_camera(const float *positions, uint64_t n, uint32_t 
   const float half_y = std::fmax(extent.y * 0.5f, 1e-3f);
   const float half_z = std::fmax(extent.z * 0.5f, 1e-3f);
   const float aspect = (float)width / (float)height;
-  const float default_fov = to_radians_f32(60.0f);  // Camera::default()
+  // Camera::default(). Read through a volatile so that the compiler cannot
+  // fold tan/atan of a constant at build time (correctly rounded) where the
+  // reference calls the platform's f32 libm at run time.
+  volatile float default_fov_v = to_radians_f32(60.0f);
+  const float default_fov = default_fov_v;
   const float vfov = std::fmax(default_fov, 1e-3f);
   const float hfov = 2.0f * std::atan(std::tan(vfov * 0.5f) * aspect);
   const float dist_y = half_y / std::tan(vfov * 0.5f);
