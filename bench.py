@@ -970,11 +970,10 @@ def run_cuda(args, world, rank, local):
         b = algorithmic_bytes(k, counts, scene["positions"].shape[0], planes, w, h, tile_passes)
         phase_rooflines[k] = {"ms": ms, "bytes": b, "gbs": b / (ms * 1e-3) / 1e9 if ms > 0 else None}
 
-    # scratch zeroing; preprocess; depth sort: one cluster launch up to
-    # 294,912 splats (else plan + 4 passes, histograms from K1); emit; tile
-    # sort: plan + passes (histograms from K2); ranges; raster
-    depth_sort_launches = 1 if scene["positions"].shape[0] <= 294_912 else 1 + 4  # cluster sort
-    launches_per_frame = 1 + 1 + depth_sort_launches + 1 + (1 + tile_passes) + 1 + 1
+    # scratch zeroing; preprocess; depth sort: plan + 4 passes (histograms
+    # from K1); emit; tile sort: plan + passes (histograms from K2); ranges;
+    # raster
+    launches_per_frame = 1 + 1 + (1 + 4) + 1 + (1 + tile_passes) + 1 + 1
     line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_frame,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",

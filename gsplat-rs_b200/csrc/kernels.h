@@ -67,16 +67,6 @@ uint64_t sort_work_words(uint32_t capacity, uint32_t passes);
 // plan and pass kernels on `stream`.
 void launch_sort(const SortBuffers &b, cudaStream_t stream);
 
-// ---- K3a for small frames: the depth sort in one 16-CTA cluster ------------
-// Same order as launch_sort over 4 passes (stable ascending, 32-bit keys),
-// for at most kClusterSortMaxItems items: one launch, all passes in
-// distributed shared memory (k_cluster_sort.cu). The result is in
-// (keys1, vals1); plan->final_buffer = 1 and plan->n = *count.
-constexpr uint32_t kClusterSortMaxItems = 16u * 1024u * 18u;  // 294,912
-bool cluster_sort_available();  // the current device can co-schedule the cluster
-void launch_cluster_sort(const uint32_t *count, const uint32_t *keys0, const uint32_t *vals0,
-                         uint32_t *keys1, uint32_t *vals1, SortPlan *plan, cudaStream_t stream);
-
 // ---- K2: tile-pair emission over the depth-sorted visible ids ------------
 struct EmitBuffers {
   const SortPlan *depth_plan;      // selects the buffer holding the sorted ids; n = their count

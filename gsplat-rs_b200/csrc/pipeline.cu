@@ -373,15 +373,6 @@ RunInit Pipeline::make_run_init(const Layout &l) const {
   return init;
 }
 
-// Runs whose splats (an upper bound of the visible count) fit one cluster
-// sort it there: one launch instead of the plan kernel and four passes.
-#ifndef GSR_CLUSTER_SORT
-#define GSR_CLUSTER_SORT 1
-#endif
-bool Pipeline::use_cluster_depth_sort(const Layout &l) const {
-  return GSR_CLUSTER_SORT && l.total_splats <= kClusterSortMaxItems && cluster_sort_available();
-}
-
 void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &sinks,
                           bool reuse, const ViewDev *views_dev, const ViewSetDev *sets_dev) {
   const uint32_t n = std::max<uint32_t>(l.total_splats, 1);
@@ -396,14 +387,9 @@ void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &si
   record(1);
 
   if (!reuse) {  // a reused order keeps the last sort's ids and plan
-    if (use_cluster_depth_sort(l)) {
-      launch_cluster_sort(&counters_->visible, vis_keys0_, vis_vals0_, vis_keys1_, vis_vals1_,
-                          depth_plan_, stream_);
-    } else {
-      SortBuffers ds{vis_keys0_, vis_vals0_, vis_keys1_, vis_vals1_, &counters_->visible, n, 0,
-                     4, depth_plan_, depth_sort_work_, &counters_->error, key_hist_, true};
-      launch_sort(ds, stream_);
-    }
+    SortBuffers ds{vis_keys0_, vis_vals0_, vis_keys1_, vis_vals1_, &counters_->visible, n, 0, 4,
+                   depth_plan_, depth_sort_work_, &counters_->error, key_hist_, true};
+    launch_sort(ds, stream_);
   }
   record(2);
 

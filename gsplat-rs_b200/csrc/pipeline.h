@@ -169,7 +169,6 @@ class Pipeline {
   Layout plan_views(const ViewSpec *views, uint32_t count, const uint64_t *image_bases);
   void ensure_workspace(const Layout &l);
   void ensure_key_workspace(uint64_t capacity);
-  bool use_cluster_depth_sort(const Layout &l) const;
   void launch_all(const Layout &l, uint32_t *images, const HostSinks &sinks, bool reuse,
                   const ViewDev *views_dev, const ViewSetDev *sets_dev);
   void fetch_counters();  // device-resident counters of the last run -> host (stream synchronised)
