@@ -248,7 +248,7 @@ def lcg_keys(seed, n):
     return out
 
 
-def cpu_baseline(scene, cam, w, h, warmup=5, iters=30, gpu_images=None):
+def cpu_baseline(scene, cam, w, h, warmup=5, iters=30, gpu_images=None, gpu_projected=None):
     """The reference frame restated on the host (the oracle's C++ port of the
     CPU depth preprocess and radix sort on one thread, the vertex stage and
     UNORM8 blend on every host thread), per phase as median and p95 over
@@ -258,7 +258,9 @@ def cpu_baseline(scene, cam, w, h, warmup=5, iters=30, gpu_images=None):
     (crates/gsplat-sort/src/lib.rs:649-676) and on the 1080p frame's depth
     keys. gpu_images: {mode: RGBA8 image} rendered on the GPU for the headline
     camera; each is compared with the CPU frame's image (the reference image
-    model) and with the FP64 evaluation of the same frame."""
+    model) and with the FP64 evaluation of the same frame. gpu_projected: the
+    GPU's per-splat vertex outputs for that camera (the debug tap), compared
+    with a float64 evaluation of the reference's vertex stage."""
     import oracle_py
 
     threads = os.cpu_count() or 1
@@ -313,6 +315,11 @@ def cpu_baseline(scene, cam, w, h, warmup=5, iters=30, gpu_images=None):
             mode: {"vs_reference_model": image_errors(img, ref_img),
                    "vs_fp64": image_errors(img, f64)} for mode, img in gpu_images.items()}
         out["gpu_image_errors"]["reference_model_vs_fp64"] = image_errors(ref_img, f64)
+    if gpu_projected is not None:
+        import oracle_f64
+
+        out["gpu_vertex_errors_vs_fp64"] = oracle_f64.output_errors(
+            gpu_projected, oracle_f64.project(scene, cam, w, h))
     return out
 
 
@@ -988,8 +995,17 @@ def run_cuda(args, world, rank, local):
         roofline["issue_frac"] = (roofline["issue_inst_per_launch"] /
                                   (phases["raster"] * 1e-3) / issue_peak)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the GPU's per-splat outputs of the same frame, from a context with
+        # the debug tap on (outside every timed region)
+        with ffi.Context(w, h) as dbg:
+            dbg.set_debug_taps(True)
+            dbg.load_scene(scene)
+            dbg.set_camera(cam)
+            dbg.render_frame()
+            projected = dbg.debug_projected()
         line["cpu_baseline"] = cpu_baseline(scene, cam, w, h, iters=args.cpu_iters,
-                                            gpu_images={"fp32": img_fp32, "unorm8": img_unorm8})
+                                            gpu_images={"fp32": img_fp32, "unorm8": img_unorm8},
+                                            gpu_projected=projected)
     ctx.close()
     if not args.no_batched and world == 1:
         line["batched"] = measure_batched(ffi, torch, args.batch_steps, 2)

@@ -109,11 +109,19 @@ def test_frame_parity_stages_and_images(oracle, cfg):
 def test_full_config2_parity(oracle):
     """279,199 splats, SH3, 1920x1080: every stage bit-exact at full size (the
     FP32 image within its tolerance)."""
+    import oracle_f64
+
     scene, cam, w, h = gsplat_scenes.config2()
     sv = oracle.SceneView(scene)
     fr = oracle.Frame(sv, cam, w, h)
     ctx = _render(scene, cam, w, h)
     _compare_stages(ctx, fr, sv)
+    # the GPU's per-splat outputs against the float64 evaluation
+    e = oracle_f64.output_errors(ctx.debug_projected(), oracle_f64.project(scene, cam, w, h))
+    print("config2 vertex outputs vs fp64", e)
+    assert e["drawn_disagree"] <= max(2, 1e-4 * e["drawn_both"])
+    assert e["center_ndc"]["max_abs"] <= 2e-6 and e["color"]["max_abs"] <= 1e-6
+    assert e["conic"]["mean_rel"] <= 2e-6 and e["conic"]["p999_rel"] <= 1e-4
     img = ctx.readback_rgba8()
     assert_fp32_image(img, fr.raster_tiles_fp32())
     ref8 = fr.raster_unorm8()

@@ -238,3 +238,26 @@ def test_look_at_rotation_matches_the_oracle(oracle):
         want = oracle.camera_look_at(pos32, tgt32)
         got = ffi.camera_look_at([float(v) for v in pos32], [float(v) for v in tgt32], 1.0)
         assert np.array_equal(_f32_bits(list(got.rotation_xyzw)), _f32_bits(want)), (pos, tgt)
+
+
+def test_vertex_outputs_against_fp64(oracle):
+    """The float32 vertex stage (the oracle's, which the CUDA kernel equals bit
+    for bit, tests/test_gpu_parity.py) against a float64 evaluation of the
+    same reference math (oracle/oracle_f64.py), per output: means2d (NDC
+    centres, absolute), the premultiplied colour (absolute) and the conic of
+    the clamped axes (relative). Both draw the same splats."""
+    import gsplat_scenes
+    import oracle_f64
+
+    for scene, cam, w, h in (gsplat_scenes.config1(seed=0),
+                             gsplat_scenes.config2(seed=11, n=40000)[:2] + (960, 540)):
+        sv = oracle.SceneView(scene)
+        fr = oracle.Frame(sv, cam, w, h)
+        ref = oracle_f64.project(scene, cam, w, h)
+        e = oracle_f64.output_errors(fr.proj, ref)
+        print(e)
+        assert e["drawn_both"] > 0
+        assert e["drawn_disagree"] <= max(2, 1e-4 * e["drawn_both"])
+        assert e["center_ndc"]["max_abs"] <= 2e-6
+        assert e["color"]["max_abs"] <= 1e-6
+        assert e["conic"]["mean_rel"] <= 2e-6 and e["conic"]["p999_rel"] <= 1e-4
