@@ -56,7 +56,9 @@ FALLBACK_HBM_GBS = 6650.0
 # the command): DRAM bytes read + written, warp instructions issued, and
 # executed FP32 thread operations (2 x FFMA + FADD + FMUL). None until
 # captured for the current kernel.
-NCU_RASTER = None
+NCU_RASTER = {"dram_bytes": 18_304_256, "warp_inst": 148_805_815,
+              "thread_flop": 2 * 922_818_785 + 128_638_205 + 270_554_805,
+              "source": "profiles/frame_279k_sh3_1080p.md (ncu --set full, one launch)"}
 
 
 def dist_setup():
