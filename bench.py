@@ -912,31 +912,45 @@ def run_cuda(args, world, rank, local):
 
     # End to end through the C ABI: camera in, frame, RGBA8 readback to pinned
     # memory every step. Frames are enqueued back to back and each image is
-    # read back asynchronously while the next frame renders (two device images
-    # alternate), into two pinned host buffers in turn.
-    pinned = [torch.empty(w * h * 4, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
-    outs = [p.numpy() for p in pinned]
+    # read back asynchronously while later frames render. With frame lanes
+    # (gsplat_context_set_frame_lanes) consecutive frames also overlap on the
+    # device, each on its own stream and workspace; one lane is measured too.
     cams = []
-    rng = np.random.default_rng(5)
     for i in range(args.steps):
         yaw = 0.7 + 0.002 * i
         cams.append(ffi.GsplatCamera.from_dict(gsplat_scenes.camera(
             (4.0 * math.sin(yaw), 0.5, -4.0 * math.cos(yaw)), (0, 0, 0), 45.0)))
-    replicas.barrier()
-    t0 = time.perf_counter()
-    for i in range(args.steps):
-        ctx.set_camera(cams[i])
-        ctx.render_frame_async()
-        ctx.readback_rgba8_async(outs[i % 2])
-    ctx.sync()
-    e2e_s = time.perf_counter() - t0
-    out = outs[(args.steps - 1) % 2]
-    e2e_s = replicas.max(e2e_s)
+
+    def e2e_run(lanes):
+        ctx.set_frame_lanes(lanes)
+        pinned = [torch.empty(w * h * 4, dtype=torch.uint8, pin_memory=True)
+                  for _ in range(max(2, lanes))]
+        outs = [p.numpy() for p in pinned]
+        for i in range(max(args.warmup, 3) * lanes):  # every lane captures its graph
+            ctx.set_camera(cams[i % len(cams)])
+            ctx.render_frame_async()
+            ctx.readback_rgba8_async(outs[i % len(outs)])
+        ctx.sync()
+        replicas.barrier()
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            ctx.set_camera(cams[i])
+            ctx.render_frame_async()
+            ctx.readback_rgba8_async(outs[i % len(outs)])
+        ctx.sync()
+        el = replicas.max(time.perf_counter() - t0)
+        return el, outs[(args.steps - 1) % len(outs)]
+
+    e2e_single_s, _ = e2e_run(1)
+    e2e_s, out = e2e_run(args.frame_lanes)
+    ctx.set_frame_lanes(1)
     if args.artifact and rank == 0:
         write_plain_artifact(args, ffi, ctx, scene, cams, out, w, h)
     clk = clocks.stop()
     e2e = {"value": whole_job_rate(world, args.steps, e2e_s), "unit": "frames/s",
-           "h2d_bytes_per_step": 40, "d2h_bytes_per_step": w * h * 4 + 64}
+           "h2d_bytes_per_step": 40, "d2h_bytes_per_step": w * h * 4 + 64,
+           "frame_lanes": args.frame_lanes,
+           "single_lane_value": whole_job_rate(world, args.steps, e2e_single_s)}
 
     tiles = ((w + 15) // 16) * ((h + 15) // 16)
     tile_passes = 2 if tiles > 256 else 1
@@ -1046,6 +1060,8 @@ def main():
     ap.add_argument("--no-ingest", action="store_true")
     ap.add_argument("--no-packed", action="store_true")
     ap.add_argument("--no-config3", action="store_true")
+    ap.add_argument("--frame-lanes", type=int, default=3,
+                    help="frame lanes of the e2e loop (gsplat_context_set_frame_lanes)")
     ap.add_argument("--ingest-splats", type=int, default=279_199,
                     help="splats of the PLY ingestion workload")
     ap.add_argument("--only", default="",

@@ -381,6 +381,14 @@ int32_t gsplat_context_set_sort_interval(GsplatContext *ctx, uint32_t interval) 
   });
 }
 
+int32_t gsplat_context_set_frame_lanes(GsplatContext *ctx, uint32_t lanes) {
+  return guarded("gsplat_context_set_frame_lanes", [&]() -> int32_t {
+    if (!ctx) return fail(Code::InvalidArgument, "gsplat_context_set_frame_lanes: ctx is null");
+    ctx->renderer->set_frame_lanes(lanes);
+    return ok();
+  });
+}
+
 int32_t gsplat_context_load_scene_buffers(GsplatContext *ctx, const GsplatSceneDesc *scene) {
   return guarded("gsplat_context_load_scene_buffers", [&]() -> int32_t {
     if (!ctx || !scene)

@@ -110,6 +110,7 @@ class Pipeline {
   void set_debug(bool on) { debug_ = on; }
   bool debug() const { return debug_; }
   void set_use_graph(bool on) { use_graph_ = on; }
+  bool use_graph() const { return use_graph_; }
   // Asks the next runs to reuse the last sorted visible order instead of
   // sorting (honoured only for a layout identical to the one last sorted):
   // splats are projected with the new camera, but only those in the reused

@@ -1,7 +1,9 @@
+#include <algorithm>
 #include <cmath>
 // Plain frames: one view of the frame pipeline (no device code in this file).
 
 #include <cstring>
+#include <exception>
 #include <string>
 
 #include "cuda_check.h"
@@ -30,29 +32,78 @@ Renderer::Renderer(uint32_t width, uint32_t height) : width_(width), height_(hei
   device_ = require_b200();
   if (width > kMaxImageDimension || height > kMaxImageDimension)
     throw Error(Code::Unsupported, "requested dimensions exceed the maximum of 16384");
-  GSR_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  lanes_.reserve(kMaxLanes);
+  lanes_.emplace_back();
+  GSR_CUDA(cudaStreamCreateWithFlags(&lanes_[0].stream, cudaStreamNonBlocking));
   GSR_CUDA(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
-  for (int k = 0; k < 2; ++k) {
+  for (uint32_t k = 0; k < kMaxLanes; ++k) {
     GSR_CUDA(cudaEventCreateWithFlags(&rendered_[k], cudaEventDisableTiming));
     GSR_CUDA(cudaEventCreateWithFlags(&copied_[k], cudaEventDisableTiming));
   }
-  pipe_ = std::make_unique<Pipeline>(device_, stream_);
+  lanes_[0].pipe = std::make_unique<Pipeline>(device_, lanes_[0].stream);
 }
 
 Renderer::~Renderer() {
   cudaSetDevice(device_);
-  if (stream_) cudaStreamSynchronize(stream_);
+  for (auto &lane : lanes_)
+    if (lane.stream) cudaStreamSynchronize(lane.stream);
   if (copy_stream_) cudaStreamSynchronize(copy_stream_);
-  pipe_.reset();
+  for (auto &lane : lanes_) lane.pipe.reset();
   scene_.reset();
-  image_[0].reset(0);
-  image_[1].reset(0);
-  for (int k = 0; k < 2; ++k) {
+  for (uint32_t k = 0; k < kMaxLanes; ++k) {
+    image_[k].reset(0);
     if (rendered_[k]) cudaEventDestroy(rendered_[k]);
     if (copied_[k]) cudaEventDestroy(copied_[k]);
   }
   if (copy_stream_) cudaStreamDestroy(copy_stream_);
-  if (stream_) cudaStreamDestroy(stream_);
+  for (auto &lane : lanes_)
+    if (lane.stream) cudaStreamDestroy(lane.stream);
+}
+
+void Renderer::sync_all_lanes() {
+  for (auto &lane : lanes_) GSR_CUDA(cudaStreamSynchronize(lane.stream));
+}
+
+// New lanes copy the first lane's settings and its tile-pair capacity (an
+// enqueued frame keeps the capacity it finds, so a fresh lane must not start
+// smaller than the frames it will take over).
+void Renderer::set_frame_lanes(uint32_t lanes) {
+  if (lanes < 1 || lanes > kMaxLanes)
+    throw Error(Code::InvalidArgument, "frame lanes must be 1 to 4");
+  GSR_CUDA(cudaSetDevice(device_));
+  if (deferred_.pending) issue_copy(false);
+  sync_all_lanes();
+  GSR_CUDA(cudaStreamSynchronize(copy_stream_));
+  const Pipeline &first = *lanes_[0].pipe;
+  while (lanes_.size() < lanes) {
+    Lane lane;
+    GSR_CUDA(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking));
+    lane.pipe = std::make_unique<Pipeline>(device_, lane.stream);
+    lane.pipe->set_tile(first.tile());
+    lane.pipe->set_blend_mode(first.blend_mode());
+    lane.pipe->set_debug(first.debug());
+    lane.pipe->set_use_graph(first.use_graph());
+    lane.pipe->set_raster_config(first.raster_config());
+    lanes_.push_back(std::move(lane));
+  }
+  for (auto &lane : lanes_) pair_capacity_ = std::max(pair_capacity_, lane.pipe->key_capacity());
+  for (uint32_t k = 0; k < lanes; ++k)
+    if (pair_capacity_) lanes_[k].pipe->reserve_pairs(pair_capacity_);
+  lane_count_ = lanes;
+  ensure_image();
+}
+
+void Renderer::set_blend_mode(uint32_t mode) {
+  for (auto &lane : lanes_) lane.pipe->set_blend_mode(mode);
+}
+void Renderer::set_debug(bool on) {
+  for (auto &lane : lanes_) lane.pipe->set_debug(on);
+}
+void Renderer::set_use_graph(bool on) {
+  for (auto &lane : lanes_) lane.pipe->set_use_graph(on);
+}
+void Renderer::set_raster_config(const RasterConfig &c) {
+  for (auto &lane : lanes_) lane.pipe->set_raster_config(c);
 }
 
 void Renderer::set_size(uint32_t width, uint32_t height) {
@@ -67,16 +118,16 @@ void Renderer::set_size(uint32_t width, uint32_t height) {
 
 void Renderer::set_tile(uint32_t tile) {
   if (tile != 8 && tile != 16) throw Error(Code::InvalidArgument, "tile size must be 8 or 16");
-  pipe_->set_tile(tile);
+  for (auto &lane : lanes_) lane.pipe->set_tile(tile);
 }
 
 void Renderer::load_scene(const HostScene &s) {
   Code c = scene_validate(s);
   if (c != Code::Ok) throw Error(Code::InvalidArgument, "invalid scene buffers");
   GSR_CUDA(cudaSetDevice(device_));
-  GSR_CUDA(cudaStreamSynchronize(stream_));
+  sync_all_lanes();
   scene_.reset();
-  scene_ = upload_scene(s, stream_);
+  scene_ = upload_scene(s, lanes_[0].stream);
   scene_changed();
 }
 
@@ -84,57 +135,69 @@ void Renderer::load_scene_packed(const HostScene &s) {
   Code c = scene_validate(s);
   if (c != Code::Ok) throw Error(Code::InvalidArgument, "invalid scene buffers");
   GSR_CUDA(cudaSetDevice(device_));
-  GSR_CUDA(cudaStreamSynchronize(stream_));
-  std::unique_ptr<DeviceScene> sc = upload_scene_packed(s, stream_);
+  sync_all_lanes();
+  std::unique_ptr<DeviceScene> sc = upload_scene_packed(s, lanes_[0].stream);
   scene_ = std::move(sc);
   scene_changed();
 }
 
 void Renderer::load_scene_path(const std::string &path) {
   GSR_CUDA(cudaSetDevice(device_));
-  GSR_CUDA(cudaStreamSynchronize(stream_));
+  sync_all_lanes();
   // The current scene stays loaded until the new one is complete.
-  std::unique_ptr<DeviceScene> sc = load_scene_file(path, stream_, {});
+  std::unique_ptr<DeviceScene> sc = load_scene_file(path, lanes_[0].stream, {});
   scene_ = std::move(sc);
   scene_changed();
 }
 
 void Renderer::ensure_image() {
   const uint64_t need = 4ull * width_ * height_;
-  if (image_[0].size() < need || image_[0].size() > 2 * need) {
+  const uint32_t slots = image_slots();
+  bool ok = true;
+  for (uint32_t k = 0; k < slots; ++k)
+    ok = ok && image_[k].size() >= need && image_[k].size() <= 2 * need;
+  if (!ok) {
     if (deferred_.pending) issue_copy(false);
-    GSR_CUDA(cudaStreamSynchronize(stream_));
+    sync_all_lanes();
     GSR_CUDA(cudaStreamSynchronize(copy_stream_));
-    image_[0].reset(need);
-    image_[1].reset(need);
-    copy_pending_[0] = copy_pending_[1] = false;
+    for (uint32_t k = 0; k < kMaxLanes; ++k) {
+      image_[k].reset(k < slots ? need : 0);
+      copy_pending_[k] = false;
+    }
   }
 }
 
-uint32_t *Renderer::next_image() {
-  const int k = front_ ^ 1;
+void Renderer::next_frame(uint32_t &lane, uint32_t &slot) {
+  lane = (uint32_t)(frame_seq_ % lanes_in_use());
+  slot = (uint32_t)(frame_seq_ % image_slots());
+  ++frame_seq_;
+  const cudaStream_t st = lanes_[lane].stream;
   // a requested readback of this buffer has to be issued before it is reused
-  if (deferred_.pending && deferred_.image == k) issue_copy(false);
-  // the buffer's last readback must land before the frame overwrites it
-  if (copy_pending_[k]) {
-    GSR_CUDA(cudaStreamWaitEvent(stream_, copied_[k], 0));
-    copy_pending_[k] = false;
+  if (deferred_.pending && deferred_.image == (int)slot) issue_copy(false);
+  // the buffer's last frame (another lane's, after a change of lanes) and
+  // its last readback must complete before this frame overwrites it
+  GSR_CUDA(cudaStreamWaitEvent(st, rendered_[slot], 0));
+  if (copy_pending_[slot]) {
+    GSR_CUDA(cudaStreamWaitEvent(st, copied_[slot], 0));
+    copy_pending_[slot] = false;
   }
-  return image_[k].as<uint32_t>();
 }
 
-void Renderer::frame_enqueued() {
-  front_ ^= 1;
-  GSR_CUDA(cudaEventRecord(rendered_[front_], stream_));
+void Renderer::frame_enqueued(uint32_t lane, uint32_t slot) {
+  front_ = slot;
+  front_lane_ = lane;
+  GSR_CUDA(cudaEventRecord(rendered_[slot], lanes_[lane].stream));
   if (deferred_.pending) issue_copy(true);
 }
 
 void Renderer::issue_copy(bool after_next_raster) {
   const int k = deferred_.image;
   // The image is complete once its frame is; with a frame enqueued after it,
-  // that frame's raster start is later still.
-  GSR_CUDA(cudaStreamWaitEvent(copy_stream_,
-                               after_next_raster ? pipe_->raster_start_event() : rendered_[k], 0));
+  // the copy also waits for that frame's raster to start (one long kernel,
+  // so the copy's PCIe traffic does not delay that frame's other launches).
+  GSR_CUDA(cudaStreamWaitEvent(copy_stream_, rendered_[k], 0));
+  if (after_next_raster)
+    GSR_CUDA(cudaStreamWaitEvent(copy_stream_, front_pipe().raster_start_event(), 0));
   GSR_CUDA(cudaMemcpyAsync(deferred_.out, image_[k].get(), deferred_.bytes, cudaMemcpyDeviceToHost,
                            copy_stream_));
   GSR_CUDA(cudaEventRecord(copied_[k], copy_stream_));
@@ -192,19 +255,19 @@ bool order_pose_compatible(const GsplatCamera &a, const GsplatCamera &b, float l
 // yet, or when the camera has changed `interval` times since the last sort;
 // and, as for the reference's reused orders (surface_session.rs:1149-1153),
 // when the camera has left the pose bound of the order's own camera.
-void Renderer::plan_order(const GsplatCamera &cam) {
+void Renderer::plan_order(Pipeline &pipe, const GsplatCamera &cam) {
   const bool changed = !has_last_camera_ || std::memcmp(&cam, &last_camera_, sizeof cam) != 0;
   if (changed) ++changes_since_sort_;
   const bool refresh = sort_interval_ == 0 || force_sort_ ||
                        (changed && changes_since_sort_ >= sort_interval_) ||
                        !order_pose_compatible(sorted_camera_, cam, order_translation_limit_);
-  pipe_->set_reuse_order(!refresh);
+  pipe.set_reuse_order(!refresh);
   last_camera_ = cam;
   has_last_camera_ = true;
 }
 
-void Renderer::finish_order() {
-  if (!pipe_->last_reused_order()) {
+void Renderer::finish_order(const Pipeline &pipe) {
+  if (!pipe.last_reused_order()) {
     changes_since_sort_ = 0;
     force_sort_ = false;
     sorted_camera_ = last_camera_;
@@ -213,32 +276,53 @@ void Renderer::finish_order() {
 
 FrameResult Renderer::render(const GsplatCamera &cam) {
   auto views = one_view(cam);
-  plan_order(cam);
-  last_ = pipe_->run(views, next_image(), image_base_);
-  frame_enqueued();
-  finish_order();
+  uint32_t lane, slot;
+  next_frame(lane, slot);
+  Pipeline &pipe = *lanes_[lane].pipe;
+  plan_order(pipe, cam);
+  last_ = pipe.run(views, image_[slot].as<uint32_t>(), image_base_);
+  pair_capacity_ = std::max(pair_capacity_, pipe.key_capacity());
+  frame_enqueued(lane, slot);
+  finish_order(pipe);
   has_frame_ = true;
   return last_;
 }
 
 void Renderer::render_async(const GsplatCamera &cam) {
   auto views = one_view(cam);
-  plan_order(cam);
-  pipe_->enqueue(views, next_image(), image_base_);
-  frame_enqueued();
-  finish_order();
+  uint32_t lane, slot;
+  next_frame(lane, slot);
+  Pipeline &pipe = *lanes_[lane].pipe;
+  // an enqueued frame keeps the pair capacity it finds: every lane gets the
+  // largest a synchronous frame has needed
+  if (pipe.key_capacity() < pair_capacity_) pipe.reserve_pairs(pair_capacity_);
+  plan_order(pipe, cam);
+  pipe.enqueue(views, image_[slot].as<uint32_t>(), image_base_);
+  frame_enqueued(lane, slot);
+  finish_order(pipe);
   has_frame_ = true;
 }
 
 void Renderer::sync() {
   if (deferred_.pending) issue_copy(false);
-  try {
-    last_ = pipe_->sync();
-  } catch (const Error &e) {
-    if (e.code == Code::Internal) has_frame_ = false;
-    throw;
+  // Every lane is waited for; the first error is reported after all of
+  // them, and the result is the last frame's.
+  std::exception_ptr first;
+  bool internal = false;
+  for (uint32_t k = 0; k < lanes_.size(); ++k) {
+    try {
+      FrameResult r = lanes_[k].pipe->sync();
+      if (k == front_lane_) last_ = r;
+    } catch (const Error &e) {
+      if (!first) first = std::current_exception();
+      internal = internal || e.code == Code::Internal;
+    }
   }
   GSR_CUDA(cudaStreamSynchronize(copy_stream_));
+  if (first) {
+    if (internal) has_frame_ = false;
+    std::rethrow_exception(first);
+  }
 }
 
 void Renderer::readback_rgba8(uint8_t *out, uint64_t len) {
@@ -247,8 +331,9 @@ void Renderer::readback_rgba8(uint8_t *out, uint64_t len) {
   if (len < need) throw Error(Code::InvalidArgument, "output buffer too small for the RGBA8 image");
   GSR_CUDA(cudaSetDevice(device_));
   if (deferred_.pending) issue_copy(false);
-  GSR_CUDA(cudaMemcpyAsync(out, image_[front_].get(), need, cudaMemcpyDeviceToHost, stream_));
-  GSR_CUDA(cudaStreamSynchronize(stream_));
+  const cudaStream_t st = lanes_[front_lane_].stream;
+  GSR_CUDA(cudaMemcpyAsync(out, image_[front_].get(), need, cudaMemcpyDeviceToHost, st));
+  GSR_CUDA(cudaStreamSynchronize(st));
 }
 
 void Renderer::readback_rgba8_async(uint8_t *out, uint64_t len) {
@@ -257,29 +342,29 @@ void Renderer::readback_rgba8_async(uint8_t *out, uint64_t len) {
   if (len < need) throw Error(Code::InvalidArgument, "output buffer too small for the RGBA8 image");
   GSR_CUDA(cudaSetDevice(device_));
   if (deferred_.pending) issue_copy(false);
-  deferred_ = DeferredCopy{true, front_, out, need};
+  deferred_ = DeferredCopy{true, (int)front_, out, need};
 }
 
 std::vector<uint32_t> Renderer::debug_order() {
   if (!has_frame_) throw Error(Code::InvalidArgument, "no rendered frame");
-  return pipe_->debug_order();
+  return front_pipe().debug_order();
 }
 
 std::vector<ProjectedDev> Renderer::debug_projected() {
   if (!has_frame_) throw Error(Code::InvalidArgument, "debug taps were not enabled for the last frame");
-  return pipe_->debug_projected(scene_->n);
+  return front_pipe().debug_projected(scene_->n);
 }
 
 void Renderer::debug_tile_pairs(std::vector<uint32_t> &tiles, std::vector<uint32_t> &ids) {
   if (!has_frame_) throw Error(Code::InvalidArgument, "debug taps were not enabled for the last frame");
-  pipe_->debug_tile_pairs(tiles, ids);
+  front_pipe().debug_tile_pairs(tiles, ids);
 }
 
 void Renderer::debug_tile_ranges(std::vector<uint32_t> &ranges, std::vector<uint32_t> &ids) {
   if (!has_frame_) throw Error(Code::InvalidArgument, "no rendered frame");
-  const uint32_t t = pipe_->tile();
+  const uint32_t t = front_pipe().tile();
   const uint32_t tiles = ((width_ + t - 1) / t) * ((height_ + t - 1) / t);
-  pipe_->debug_tile_ranges(tiles, ranges, ids);
+  front_pipe().debug_tile_ranges(tiles, ranges, ids);
 }
 
 }  // namespace gsr

@@ -33,12 +33,22 @@ class Renderer {
   uint32_t width() const { return width_; }
   uint32_t height() const { return height_; }
   void set_tile(uint32_t tile);
-  uint32_t tile() const { return pipe_->tile(); }
-  void set_blend_mode(uint32_t mode) { pipe_->set_blend_mode(mode); }
-  uint32_t blend_mode() const { return pipe_->blend_mode(); }
-  void set_debug(bool on) { pipe_->set_debug(on); }
-  void set_use_graph(bool on) { pipe_->set_use_graph(on); }
-  void set_raster_config(const RasterConfig &c) { pipe_->set_raster_config(c); }
+  uint32_t tile() const { return lanes_[0].pipe->tile(); }
+  void set_blend_mode(uint32_t mode);
+  uint32_t blend_mode() const { return lanes_[0].pipe->blend_mode(); }
+  void set_debug(bool on);
+  void set_use_graph(bool on);
+  void set_raster_config(const RasterConfig &c);
+  // Frame lanes: enqueued frames rotate over `lanes` pipelines, each on its
+  // own stream with its own workspace and image, so consecutive frames
+  // overlap on the device (one frame's latency-bound sorts beside another's
+  // raster). 1 (the default) runs every frame on one stream. Frames stay
+  // independent and each image is exactly the single-lane image. A sort
+  // interval other than 0 runs on one lane (its reused order lives in that
+  // lane's workspace).
+  static constexpr uint32_t kMaxLanes = 4;
+  void set_frame_lanes(uint32_t lanes);
+  uint32_t frame_lanes() const { return lane_count_; }
   // Depth-order refresh cadence. 0 (the default): every frame sorts, as the
   // reference's context does. k >= 1: the reference's surface sort interval —
   // the order is re-sorted when the camera has changed k times since the
@@ -70,7 +80,7 @@ class Renderer {
   // overflowed its pair buffers or hit a device wait limit.
   void sync();
   const FrameResult &last() const { return last_; }
-  uint64_t key_capacity() const { return pipe_->key_capacity(); }
+  uint64_t key_capacity() const { return front_pipe().key_capacity(); }
   bool has_frame() const { return has_frame_; }
 
   void readback_rgba8(uint8_t *out, uint64_t len);
@@ -86,17 +96,34 @@ class Renderer {
   void debug_tile_ranges(std::vector<uint32_t> &ranges, std::vector<uint32_t> &ids);
 
   int device() const { return device_; }
-  cudaStream_t stream() const { return stream_; }
+  // The first lane's stream (the only one while frame lanes are 1).
+  cudaStream_t stream() const { return lanes_[0].stream; }
 
  private:
+  struct Lane {
+    cudaStream_t stream = nullptr;
+    std::unique_ptr<Pipeline> pipe;
+  };
   std::vector<ViewSpec> one_view(const GsplatCamera &cam);
   void ensure_image();
-  void plan_order(const GsplatCamera &cam);  // sets the pipeline's order reuse
-  void finish_order();
+  void plan_order(Pipeline &pipe, const GsplatCamera &cam);  // sets the lane's order reuse
+  void finish_order(const Pipeline &pipe);
   void scene_changed();  // forces a sort and takes the scene's translation bound
+  void sync_all_lanes();  // waits for every lane's stream (no error checks)
+  uint32_t lanes_in_use() const { return sort_interval_ == 0 ? lane_count_ : 1u; }
+  uint32_t image_slots() const { return lanes_in_use() < 2 ? 2u : lanes_in_use(); }
+  Pipeline &front_pipe() const { return *lanes_[front_lane_].pipe; }
+  // The lane and image slot of the next frame; makes the lane wait for
+  // whatever still reads or writes that slot.
+  void next_frame(uint32_t &lane, uint32_t &slot);
+  void frame_enqueued(uint32_t lane, uint32_t slot);  // the slot now holds the last frame
 
   int device_ = 0;
-  cudaStream_t stream_ = nullptr;
+  std::vector<Lane> lanes_;  // lanes_[0] always exists
+  uint32_t lane_count_ = 1;
+  uint64_t frame_seq_ = 0;   // frames enqueued: selects the lane and the image slot
+  uint32_t front_lane_ = 0;  // lane of the last frame
+  uint64_t pair_capacity_ = 0;  // largest tile-pair capacity a synchronous frame needed
   uint32_t width_, height_;
   bool has_frame_ = false;
   uint32_t sort_interval_ = 0, changes_since_sort_ = 0;
@@ -104,16 +131,16 @@ class Renderer {
   GsplatCamera last_camera_{};
   GsplatCamera sorted_camera_{};      // the camera the current order was sorted for
   float order_translation_limit_ = 1e-4f;
-  std::unique_ptr<Pipeline> pipe_;
   std::unique_ptr<DeviceScene> scene_;
   FrameResult last_;
-  // Two image buffers: frames alternate between them (front_ = last frame's).
-  DeviceBuffer image_[2];
-  int front_ = 1;
+  // Image slots: frames rotate over max(2, lanes in use) buffers (front_ =
+  // the last frame's), so a frame's readback overlaps the next frames.
+  DeviceBuffer image_[kMaxLanes];
+  uint32_t front_ = 0;
   cudaStream_t copy_stream_ = nullptr;
-  cudaEvent_t rendered_[2] = {nullptr, nullptr};  // frame into image_[k] complete
-  cudaEvent_t copied_[2] = {nullptr, nullptr};    // async readback of image_[k] complete
-  bool copy_pending_[2] = {false, false};
+  cudaEvent_t rendered_[kMaxLanes] = {};  // the frame into image_[k] is complete
+  cudaEvent_t copied_[kMaxLanes] = {};    // the async readback of image_[k] is complete
+  bool copy_pending_[kMaxLanes] = {};
   // A readback requested but not yet issued: it starts with the next frame's
   // raster (one long kernel, so the copy's PCIe traffic does not delay that
   // frame's other launches), or at sync().
@@ -124,8 +151,6 @@ class Renderer {
     uint64_t bytes = 0;
   } deferred_;
   void issue_copy(bool after_next_raster);
-  uint32_t *next_image();  // the buffer the next frame renders into (waits for its readback)
-  void frame_enqueued();   // marks that buffer as the last frame's
   const std::vector<uint64_t> image_base_{0};
 };
 

@@ -207,6 +207,7 @@ _SIGS = [
     ("gsplat_context_set_raster_config", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]),
     ("gsplat_context_set_sort_interval", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
+    ("gsplat_context_set_frame_lanes", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
     ("gsplat_context_load_scene_buffers", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.POINTER(GsplatSceneDesc)]),
     ("gsplat_context_readback_rgba8", ctypes.c_int32, [ctypes.c_void_p, _u8p, ctypes.c_uint64]),
@@ -413,6 +414,9 @@ class Context:
 
     def set_sort_interval(self, interval):
         check(lib().gsplat_context_set_sort_interval(self.ptr, interval))
+
+    def set_frame_lanes(self, lanes):
+        check(lib().gsplat_context_set_frame_lanes(self.ptr, lanes))
 
     def load_scene_path(self, path):
         check(lib().gsplat_context_load_scene_path(self.ptr, os.fsencode(path)))

@@ -111,6 +111,15 @@ int32_t gsplat_context_set_raster_config(GsplatContext *ctx, uint32_t chunk, uin
  * order, in that order (stale-order frames, as in the reference). */
 int32_t gsplat_context_set_sort_interval(GsplatContext *ctx, uint32_t interval);
 
+/* No counterpart in the reference: frame lanes (1 to 4, default 1).
+ * Frames enqueued with gsplat_context_render_frame_async rotate over `lanes`
+ * independent pipelines, each on its own CUDA stream with its own workspace
+ * and image, so consecutive frames overlap on the device (one frame's sorts
+ * run beside another's raster). Every image is the one a single lane gives;
+ * readbacks, stats and debug taps refer to the last frame. Waits for the
+ * frames in flight. A sort interval other than 0 runs frames on one lane. */
+int32_t gsplat_context_set_frame_lanes(GsplatContext *ctx, uint32_t lanes);
+
 /* Load a scene from host memory (validated like SceneBuffers::validate,
  * crates/gsplat-core/src/lib.rs:224-276). Replaces any loaded scene. */
 int32_t gsplat_context_load_scene_buffers(GsplatContext *ctx, const GsplatSceneDesc *scene);

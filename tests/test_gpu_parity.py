@@ -615,3 +615,58 @@ def test_async_readback_pipeline_equals_synchronous_frames():
         ctx.sync()
         ctx.render_frame()
         assert np.array_equal(ctx.readback_rgba8().reshape(-1), big)
+
+
+@pytest.mark.parametrize("lanes", [2, 3, 4])
+def test_frame_lanes_equal_single_lane_frames(lanes):
+    """Frames that overlap on the device over `lanes` pipelines (one stream,
+    workspace and image each) give, frame by frame, the single-lane images:
+    async frames with async readbacks, a synchronous frame among them (its
+    counters and debug order are the last frame's), a larger scene that
+    overflows a lane's pair buffers on a synchronous frame, and a return to
+    one lane."""
+    scene, _, w, h = gsplat_scenes.config1(seed=17)
+    rng = np.random.default_rng(lanes)
+    cams = [gsplat_scenes.orbit_camera(rng, (4.0, 6.0)) for _ in range(11)]
+    ref, orders = [], []
+    with ffi.Context(w, h) as ctx:
+        ctx.set_debug_taps(True)
+        ctx.load_scene(scene)
+        for c in cams:
+            ctx.set_camera(c)
+            ctx.render_frame()
+            ref.append(ctx.readback_rgba8().copy())
+            orders.append(ctx.debug_order().copy())
+    with ffi.Context(w, h) as ctx:
+        ctx.set_debug_taps(True)
+        ctx.load_scene(scene)
+        ctx.set_frame_lanes(lanes)
+        outs = [np.zeros(w * h * 4, np.uint8) for _ in cams]
+        for rep in range(2):
+            for k, (c, out) in enumerate(zip(cams, outs)):
+                ctx.set_camera(c)
+                if k == 5:
+                    ctx.render_frame()
+                    assert np.array_equal(ctx.debug_order(), orders[k])
+                    assert ctx.stats().visible_count == len(orders[k])
+                else:
+                    ctx.render_frame_async()
+                ctx.readback_rgba8_async(out)
+            ctx.sync()
+            assert np.array_equal(ctx.debug_order(), orders[-1])
+            for k, out in enumerate(outs):
+                assert np.array_equal(out.reshape(h, w, 4), ref[k]), (rep, k)
+        big, bcam, bw, bh = gsplat_scenes.config2(seed=5, n=60000)
+        ctx.load_scene(big)
+        ctx.set_size(bw // 2, bh // 2)
+        ctx.set_camera(bcam)
+        ctx.render_frame()
+        want = ctx.readback_rgba8().copy()
+        for _ in range(2 * lanes):
+            ctx.render_frame_async()
+        ctx.sync()
+        assert np.array_equal(ctx.readback_rgba8(), want)
+        ctx.set_frame_lanes(1)
+        ctx.render_frame_async()
+        ctx.sync()
+        assert np.array_equal(ctx.readback_rgba8(), want)
