@@ -102,15 +102,17 @@ __device__ __forceinline__ uint32_t ellipse_block_mask(float4 ra, float4 rb, flo
 
 // Ordered compaction of the chunk entries whose mask has this warp's bit
 // into list[] (ballots keep the list order); returns their count.
+// Entries are stored as k << shift (shift 4: the byte offset of a float4
+// array element).
 __device__ __forceinline__ uint32_t compact_warp_entries(const uint8_t *mask, uint32_t n_in,
                                                         uint32_t warp, uint32_t lane,
-                                                        uint16_t *list) {
+                                                        uint16_t *list, uint32_t shift = 0) {
   uint32_t n_w = 0;
   for (uint32_t k0 = 0; k0 < n_in; k0 += 32) {
     const uint32_t k = k0 + lane;
     const bool hit = k < n_in && ((mask[k] >> warp) & 1u);
     const uint32_t bal = __ballot_sync(0xffffffffu, hit);
-    if (hit) list[n_w + __popc(bal & lanemask_lt())] = (uint16_t)k;
+    if (hit) list[n_w + __popc(bal & lanemask_lt())] = (uint16_t)(k << shift);
     n_w += __popc(bal);
   }
   __syncwarp();
@@ -195,9 +197,13 @@ __global__ void __launch_bounds__(kTile *kTile) raster_unorm8_kernel(RasterArgs 
   };
   // Coverage and weight of entry j at this pixel (the reference fragment
   // rule); false when the fragment is discarded.
+  // j is the entry's byte offset into a float4 array of the chunk
+  auto at = [&](const float4 *arr, uint32_t j) {
+    return *reinterpret_cast<const float4 *>(reinterpret_cast<const char *>(arr) + j);
+  };
   auto weight = [&](int buf, uint32_t j, float &g, float &w) {
-    const float4 d0 = sm.raw[buf][0][j];
-    const float4 d1 = sm.raw[buf][1][j];
+    const float4 d0 = at(sm.raw[buf][0], j);
+    const float4 d1 = at(sm.raw[buf][1], j);
     const float dpx = __fsub_rn(fpx, d0.x), dpy = __fsub_rn(fpy, d0.y);
     const float lx = __fmaf_rn(d0.z, dpx, __fmul_rn(d0.w, dpy));
     const float ly = __fmaf_rn(d1.x, dpx, __fmul_rn(d1.y, dpy));
@@ -211,7 +217,7 @@ __global__ void __launch_bounds__(kTile *kTile) raster_unorm8_kernel(RasterArgs 
   float f0 = 0.f, f1 = 0.f, f2 = 0.f, f3 = 0.f;
   float t0 = 0.f, t1 = 0.f, t2 = 0.f, t3 = 0.f;
   auto blend = [&](int buf, uint32_t j, float g, float w) {
-    const float4 pc = sm.raw[buf][2][j];
+    const float4 pc = at(sm.raw[buf][2], j);
     const float om = __fsub_rn(1.0f, w);
     unorm8_step(f0, t0, om, __fmul_rn(pc.x, g));
     unorm8_step(f1, t1, om, __fmul_rn(pc.y, g));
@@ -233,7 +239,7 @@ __global__ void __launch_bounds__(kTile *kTile) raster_unorm8_kernel(RasterArgs 
       sm.mask[tid] = (uint8_t)ellipse_block_mask<kTile>(ra, rb, thr, ra.x - ftx, ra.y - fty);
     }
     __syncthreads();
-    const uint32_t n_w = compact_warp_entries(sm.mask, n_in, warp, lane, sm.list[warp]);
+    const uint32_t n_w = compact_warp_entries(sm.mask, n_in, warp, lane, sm.list[warp], 4);
     if (inside) {
       uint32_t i = 0;
       // two entries per step: the second's coverage and weight do not wait
@@ -357,16 +363,20 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
       sm.mask[tid] = (uint8_t)ellipse_block_mask<kTile>(ra, rb, thr, cxl, cyl);
     }
     __syncthreads();
-    // Ordered compaction of this warp's entries.
-    const uint32_t n_w = compact_warp_entries(sm.mask, n_in, warp, lane, sm.list[warp]);
+    // Ordered compaction of this warp's entries (as byte offsets).
+    const uint32_t n_w = compact_warp_entries(sm.mask, n_in, warp, lane, sm.list[warp], 4);
     // Four list entries per step (one early-out vote, one packed index
     // load); each pixel still takes them strictly in list order.
     // w = alpha e^(-4.5 r2) = 2^(log2 alpha - 4.5 log2(e) r2) (the entry's
     // log2 alpha in its colour's w), so the colour takes rgb * (w T) and the
     // transmittance loses w T.
+    // j is the entry's byte offset into the float4 arrays
+    auto at = [&](const float4 *arr, uint32_t j) {
+      return *reinterpret_cast<const float4 *>(reinterpret_cast<const char *>(arr) + j);
+    };
     auto blend = [&](uint32_t j, float r2, float thr) {
       if (done || !(r2 <= thr)) return;
-      const float4 col = sm.d2[j];
+      const float4 col = at(sm.d2, j);
       const float w = blend_weight(r2, col.w);
       const float wT = w * T;
       c0 = fmaf(col.x, wT, c0);
@@ -376,8 +386,8 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
       if (T < 1e-4f) done = true;
     };
     auto local_r2 = [&](uint32_t j, float &s2) {
-      const float4 d0 = sm.d0[j];
-      const float4 d1 = sm.d1[j];
+      const float4 d0 = at(sm.d0, j);
+      const float4 d1 = at(sm.d1, j);
       const float lx = fmaf(d0.x, fx, fmaf(d0.y, fy, d0.z));
       const float ly = fmaf(d1.x, fx, fmaf(d1.y, fy, d1.z));
       s2 = d0.w;
