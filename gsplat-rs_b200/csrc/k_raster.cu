@@ -201,28 +201,33 @@ __global__ void __launch_bounds__(kTile *kTile) raster_unorm8_kernel(RasterArgs 
   auto at = [&](const float4 *arr, uint32_t j) {
     return *reinterpret_cast<const float4 *>(reinterpret_cast<const char *>(arr) + j);
   };
-  auto weight = [&](int buf, uint32_t j, float &g, float &w) {
+  // Coverage and weight of entry j at this pixel (the reference fragment
+  // rule), branch-free: a discarded fragment gets g = 0, om = 1 and alpha 0,
+  // a step that leaves the stored value bit for bit as it is (sat(f) = f,
+  // rint(f * 255) = t and RN(t / 255) = f for every stored t).
+  auto weight = [&](int buf, uint32_t j, float &g, float &om, float &wa) {
     const float4 d0 = at(sm.raw[buf][0], j);
     const float4 d1 = at(sm.raw[buf][1], j);
     const float dpx = __fsub_rn(fpx, d0.x), dpy = __fsub_rn(fpy, d0.y);
     const float lx = __fmaf_rn(d0.z, dpx, __fmul_rn(d0.w, dpy));
     const float ly = __fmaf_rn(d1.x, dpx, __fmul_rn(d1.y, dpy));
-    if (!(fabsf(lx) <= d1.z && fabsf(ly) <= d1.z)) return false;
     const float r2 = __fmaf_rn(lx, lx, __fmul_rn(ly, ly));
-    if (!(r2 <= 1.0f)) return false;
-    g = exp_neg(__fmul_rn(-4.5f, r2));
-    w = __fmul_rn(d1.w, g);
-    return w > 1.0f / 256.0f;
+    // the exponential's argument stays in its domain [-4.5, 0]
+    const float gg = exp_neg(__fmul_rn(-4.5f, fminf(r2, 1.0f)));
+    const float w = __fmul_rn(d1.w, gg);
+    const bool cov = fabsf(lx) <= d1.z && fabsf(ly) <= d1.z && r2 <= 1.0f && w > 1.0f / 256.0f;
+    g = cov ? gg : 0.0f;
+    om = cov ? __fsub_rn(1.0f, w) : 1.0f;
+    wa = cov ? w : 0.0f;
   };
   float f0 = 0.f, f1 = 0.f, f2 = 0.f, f3 = 0.f;
   float t0 = 0.f, t1 = 0.f, t2 = 0.f, t3 = 0.f;
-  auto blend = [&](int buf, uint32_t j, float g, float w) {
+  auto blend = [&](int buf, uint32_t j, float g, float om, float wa) {
     const float4 pc = at(sm.raw[buf][2], j);
-    const float om = __fsub_rn(1.0f, w);
     unorm8_step(f0, t0, om, __fmul_rn(pc.x, g));
     unorm8_step(f1, t1, om, __fmul_rn(pc.y, g));
     unorm8_step(f2, t2, om, __fmul_rn(pc.z, g));
-    unorm8_step(f3, t3, om, w);
+    unorm8_step(f3, t3, om, wa);
   };
   if (chunks > 0) issue(0, 0);
   for (uint32_t c = 0; c < chunks; ++c) {
@@ -247,16 +252,17 @@ __global__ void __launch_bounds__(kTile *kTile) raster_unorm8_kernel(RasterArgs 
       for (; i + 1 < n_w; i += 2) {
         const uint32_t jj = *reinterpret_cast<const uint32_t *>(&sm.list[warp][i]);
         const uint32_t ja = jj & 0xffffu, jb = jj >> 16;
-        float ga, wa, gb, wb;
-        const bool ca = weight(buf, ja, ga, wa);
-        const bool cb = weight(buf, jb, gb, wb);
-        if (ca) blend(buf, ja, ga, wa);
-        if (cb) blend(buf, jb, gb, wb);
+        float ga, oa, wa, gb, ob, wb;
+        weight(buf, ja, ga, oa, wa);
+        weight(buf, jb, gb, ob, wb);
+        blend(buf, ja, ga, oa, wa);
+        blend(buf, jb, gb, ob, wb);
       }
       if (i < n_w) {
         const uint32_t ja = sm.list[warp][i];
-        float ga, wa;
-        if (weight(buf, ja, ga, wa)) blend(buf, ja, ga, wa);
+        float ga, oa, wa;
+        weight(buf, ja, ga, oa, wa);
+        blend(buf, ja, ga, oa, wa);
       }
     }
     __syncthreads();  // the next chunk's entries overwrite mask and list
@@ -374,16 +380,19 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
     auto at = [&](const float4 *arr, uint32_t j) {
       return *reinterpret_cast<const float4 *>(reinterpret_cast<const char *>(arr) + j);
     };
+    // Branch-free: a lane that does not take the entry (finished, or not
+    // covered) blends with wT = 0, which leaves C and T bit for bit as they
+    // are (fma(x, 0, c) = c and T - 0 = T for finite x).
     auto blend = [&](uint32_t j, float r2, float thr) {
-      if (done || !(r2 <= thr)) return;
+      const bool take = !done && r2 <= thr;
       const float4 col = at(sm.d2, j);
       const float w = blend_weight(r2, col.w);
-      const float wT = w * T;
+      const float wT = take ? w * T : 0.0f;
       c0 = fmaf(col.x, wT, c0);
       c1 = fmaf(col.y, wT, c1);
       c2 = fmaf(col.z, wT, c2);
       T = T - wT;
-      if (T < 1e-4f) done = true;
+      done = done || T < 1e-4f;
     };
     auto local_r2 = [&](uint32_t j, float &s2) {
       const float4 d0 = at(sm.d0, j);
