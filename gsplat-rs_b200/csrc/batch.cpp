@@ -168,7 +168,8 @@ Lane::~Lane() {
 }
 
 void Lane::enqueue(const std::vector<ViewSpec> &views, const std::vector<uint64_t> &bases,
-                   uint64_t total_pixels, const std::vector<ViewGroup> &groups, uint64_t reserve) {
+                   uint64_t total_pixels, const std::vector<ViewGroup> &groups, uint64_t reserve,
+                   bool one_graph) {
   GSR_CUDA(cudaSetDevice(device_));
   const uint64_t need = 4 * std::max<uint64_t>(total_pixels, 1);
   if (images_.size() < need) {
@@ -187,11 +188,20 @@ void Lane::enqueue(const std::vector<ViewSpec> &views, const std::vector<uint64_
   }
   pipe_->reserve_pairs(std::min<uint64_t>(std::max<uint64_t>(reserve, 1u << 20), kMaxPairs));
   GSR_CUDA(cudaEventRecord(start_, stream_));
-  for (size_t g = 0; g < groups.size(); ++g) {
-    const ViewGroup &gr = groups[g];
-    HostSinks sinks{group_counters_.get() + g, view_counters_.get() + gr.first};
-    pipe_->enqueue(views.data() + gr.first, gr.count, images_.as<uint32_t>(),
-                   bases.data() + gr.first, sinks);
+  if (one_graph) {
+    std::vector<Pipeline::GroupRun> runs(groups.size());
+    for (size_t g = 0; g < groups.size(); ++g)
+      runs[g] = Pipeline::GroupRun{groups[g].first, groups[g].count,
+                                   HostSinks{group_counters_.get() + g,
+                                             view_counters_.get() + groups[g].first}};
+    pipe_->enqueue_groups(views.data(), images_.as<uint32_t>(), bases.data(), runs);
+  } else {
+    for (size_t g = 0; g < groups.size(); ++g) {
+      const ViewGroup &gr = groups[g];
+      HostSinks sinks{group_counters_.get() + g, view_counters_.get() + gr.first};
+      pipe_->enqueue(views.data() + gr.first, gr.count, images_.as<uint32_t>(),
+                     bases.data() + gr.first, sinks);
+    }
   }
   GSR_CUDA(cudaEventRecord(end_, stream_));
 }
@@ -294,12 +304,15 @@ BatchResult Batch::render(const std::vector<BatchView> &in) {
   groups_ = plan_groups(specs_, predicted, tile_, limits_);
   uint64_t reserve = 0;
   for (const auto &g : groups_) reserve = std::max(reserve, g.predicted_pairs);
-  lane_->enqueue(specs_, bases_, pixels, groups_, reserve);
+  // the whole batch, every launch group, as one CUDA graph
+  const uint64_t graphs_before = lane_->pipe().batch_graph_launches();
+  lane_->enqueue(specs_, bases_, pixels, groups_, reserve, true);
   BatchResult r;
   r.reruns = lane_->finish(specs_, bases_, groups_);
   r.device_ms = lane_->device_ms();
   r.groups = (uint32_t)groups_.size();
   r.launches = r.groups * lane_->pipe().launches_per_run();
+  r.graph_launches = (uint32_t)(lane_->pipe().batch_graph_launches() - graphs_before);
   stats_.assign(lane_->view_counters(), lane_->view_counters() + n);
   for (uint32_t v = 0; v < n; ++v) {
     predictor_.observe(views[v].scene, specs_[v].scene->n, views[v].width, views[v].height, tile_,

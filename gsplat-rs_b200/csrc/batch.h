@@ -88,6 +88,7 @@ struct BatchResult {
   float device_ms = 0;     // CUDA-event time of all groups on the batch stream
   float wall_ms = 0;       // host time of the call
   uint32_t groups = 0, reruns = 0, launches = 0;
+  uint32_t graph_launches = 0;  // whole-batch graph launches of the first pass (0 or 1)
   uint64_t pairs = 0;      // tile pairs over all views
 };
 
@@ -119,9 +120,12 @@ class Lane {
   cudaStream_t stream() const { return stream_; }
   // Enqueues `groups` of `views` (image offsets in `bases`, pixels) without
   // waiting; per-view counters land in view_counters(), per-group counters
-  // in group_counters() once the stream reaches them.
+  // in group_counters() once the stream reaches them. one_graph: every group
+  // in one CUDA graph (Pipeline::enqueue_groups; for repeated batches), else
+  // one graph per group layout (served batches, which rarely repeat whole).
   void enqueue(const std::vector<ViewSpec> &views, const std::vector<uint64_t> &bases,
-               uint64_t total_pixels, const std::vector<ViewGroup> &groups, uint64_t reserve);
+               uint64_t total_pixels, const std::vector<ViewGroup> &groups, uint64_t reserve,
+               bool one_graph = false);
   // Waits, re-runs groups that overflowed their pair buffers and throws on
   // device errors. Returns the reruns.
   uint32_t finish(const std::vector<ViewSpec> &views, const std::vector<uint64_t> &bases,

@@ -825,7 +825,7 @@ int32_t gsplat_batch_get_times(const GsplatBatch *batch, GsplatBatchTimes *out_t
     GSR_BATCH_CHECK("gsplat_batch_get_times");
     if (!out_times) return fail(Code::InvalidArgument, "gsplat_batch_get_times: out_times is null");
     const gsr::BatchResult &r = batch->batch->last();
-    *out_times = GsplatBatchTimes{r.device_ms, r.wall_ms, r.groups, r.reruns, r.launches, 0, r.pairs};
+    *out_times = GsplatBatchTimes{r.device_ms, r.wall_ms, r.groups, r.reruns, r.launches, r.graph_launches, r.pairs};
     return ok();
   });
 }

@@ -136,9 +136,12 @@ Pipeline::~Pipeline() {
   if (counters_host_) cudaFreeHost(counters_host_);
   if (view_counters_pinned_) cudaFreeHost(view_counters_pinned_);
   if (table_pinned_) cudaFreeHost(table_pinned_);
+  if (batch_stage_) cudaFreeHost(batch_stage_);
+  if (batch_ev_) cudaEventDestroy(batch_ev_);
 }
 
 void Pipeline::record(int k) {
+  if (batch_mode_) return;  // a batch of groups is timed by its caller
   if (capturing_)
     GSR_CUDA(cudaEventRecordWithFlags(ev_[k], stream_, cudaEventRecordExternal));
   else
@@ -165,6 +168,16 @@ void Pipeline::drop_graph() {
   }
   graphs_.clear();
   seen_keys_.clear();
+  drop_batch_graphs();
+}
+
+void Pipeline::drop_batch_graphs() {
+  for (auto &g : batch_graphs_) {
+    cudaGraphExecDestroy(g.exec);
+    cudaGraphDestroy(g.graph);
+  }
+  batch_graphs_.clear();
+  batch_seen_.clear();
 }
 
 Pipeline::Layout Pipeline::plan_views(const ViewSpec *views, uint32_t count,
@@ -362,7 +375,7 @@ RunInit Pipeline::make_run_init(const Layout &l) const {
   init.zero_words[3] = kSortScratchHeadWords;
   init.zero[4] = tile_sort_work_;
   init.zero_words[4] = kSortScratchHeadWords;
-  if (l.views <= kRunInlineViews) {
+  if (l.views <= kRunInlineViews && !batch_mode_) {
     init.inline_views = l.views;
     init.inline_sets = l.sets;
     init.sets_dst = sets_dev_;
@@ -570,6 +583,130 @@ void Pipeline::enqueue(const ViewSpec *views, uint32_t count, uint32_t *images,
     sorted_scenes_.clear();
     for (uint32_t v = 0; v < count; ++v) sorted_scenes_.push_back(views[v].scene);
   }
+}
+
+void Pipeline::enqueue_groups(const ViewSpec *views, uint32_t *images,
+                              const uint64_t *image_bases, const std::vector<GroupRun> &groups) {
+  GSR_CUDA(cudaSetDevice(device_));
+  if (!use_graph_ || groups.empty()) {
+    for (const GroupRun &g : groups)
+      enqueue(views + g.first, g.count, images, image_bases + g.first, g.sinks);
+    return;
+  }
+  // Size the workspace for every group first (growing it drops the graphs),
+  // then stage every group's view table in the pinned area.
+  std::vector<Layout> layouts;
+  layouts.reserve(groups.size());
+  for (const GroupRun &g : groups) {
+    layouts.push_back(plan_views(views + g.first, g.count, image_bases + g.first));
+    ensure_workspace(layouts.back());
+  }
+  std::vector<uint64_t> offs(groups.size());
+  uint64_t total = 0;
+  for (size_t k = 0; k < groups.size(); ++k) {
+    offs[k] = total;
+    total += (table_sets_bytes_ + sizeof(ViewDev) * layouts[k].views + 255) & ~uint64_t(255);
+  }
+  // the previous batch launch must have read the staging area
+  if (batch_ev_) GSR_CUDA(cudaEventSynchronize(batch_ev_));
+  else GSR_CUDA(cudaEventCreateWithFlags(&batch_ev_, cudaEventDisableTiming));
+  if (total > batch_stage_bytes_) {
+    drop_batch_graphs();  // the captured copies read the old area
+    if (batch_stage_) cudaFreeHost(batch_stage_);
+    batch_stage_ = nullptr;
+    batch_stage_bytes_ = 0;
+    GSR_CUDA(cudaMallocHost((void **)&batch_stage_, total + total / 4));
+    batch_stage_bytes_ = total + total / 4;
+  }
+  for (size_t k = 0; k < groups.size(); ++k) {
+    plan_views(views + groups[k].first, groups[k].count, image_bases + groups[k].first);
+    std::memcpy(batch_stage_ + offs[k], sets_host_.data(), sizeof(ViewSetDev) * layouts[k].sets);
+    std::memcpy(batch_stage_ + offs[k] + table_sets_bytes_, views_host_.data(),
+                sizeof(ViewDev) * layouts[k].views);
+  }
+  BatchKey key{layouts, {}, {}, images, key_cap_, tile_, blend_mode_, debug_, raster_cfg_};
+  for (const GroupRun &g : groups) {
+    key.counters.push_back(g.sinks.counters);
+    key.views.push_back(g.sinks.views);
+  }
+  // The groups in stream order: each copies its table into the device table
+  // (no inline tables) and runs the frame pipeline over it.
+  auto launch_groups = [&]() {
+    for (size_t k = 0; k < groups.size(); ++k) {
+      GSR_CUDA(cudaMemcpyAsync(sets_dev_, batch_stage_ + offs[k],
+                               table_sets_bytes_ + sizeof(ViewDev) * layouts[k].views,
+                               cudaMemcpyHostToDevice, stream_));
+      launch_all(layouts[k], images, groups[k].sinks, false, views_dev_, sets_dev_);
+    }
+  };
+  BatchGraph *hit = nullptr;
+  for (auto &g : batch_graphs_)
+    if (g.key == key) hit = &g;
+  const bool seen = std::find(batch_seen_.begin(), batch_seen_.end(), key) != batch_seen_.end();
+  batch_mode_ = true;
+  try {
+    if (!hit && !seen) {
+      // first sighting: direct launches (a one-off batch pays no capture)
+      if (batch_seen_.size() >= kBatchGraphCacheSize) batch_seen_.erase(batch_seen_.begin());
+      batch_seen_.push_back(key);
+      launch_groups();
+    } else {
+      if (!hit) {
+        if (batch_graphs_.size() >= kBatchGraphCacheSize) {
+          auto lru = std::min_element(
+              batch_graphs_.begin(), batch_graphs_.end(),
+              [](const BatchGraph &a, const BatchGraph &b) { return a.last_use < b.last_use; });
+          cudaGraphExecDestroy(lru->exec);
+          cudaGraphDestroy(lru->graph);
+          batch_graphs_.erase(lru);
+        }
+        const auto t_capture = std::chrono::steady_clock::now();
+        cudaGraph_t g = nullptr;
+        GSR_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        capturing_ = true;
+        try {
+          launch_groups();
+        } catch (...) {
+          capturing_ = false;
+          cudaStreamEndCapture(stream_, &g);
+          if (g) cudaGraphDestroy(g);
+          cudaGetLastError();
+          throw;
+        }
+        capturing_ = false;
+        GSR_CUDA(cudaStreamEndCapture(stream_, &g));
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+        if (e != cudaSuccess) {
+          cudaGraphDestroy(g);
+          throw Error(Code::Internal, std::string("CUDA graph instantiation failed: ") +
+                                          cudaGetErrorString(e));
+        }
+        batch_graphs_.push_back(BatchGraph{key, g, exec, 0});
+        hit = &batch_graphs_.back();
+        captures_.fetch_add(1, std::memory_order_relaxed);
+        const double ms = std::chrono::duration<double, std::milli>(
+                              std::chrono::steady_clock::now() - t_capture).count();
+        capture_ms_.store(capture_ms_.load(std::memory_order_relaxed) + ms,
+                          std::memory_order_relaxed);
+      }
+      hit->last_use = ++graph_clock_;
+      GSR_CUDA(cudaGraphLaunch(hit->exec, stream_));
+      ++batch_graph_launches_;
+    }
+  } catch (...) {
+    batch_mode_ = false;
+    throw;
+  }
+  batch_mode_ = false;
+  GSR_CUDA(cudaEventRecord(batch_ev_, stream_));
+  GSR_CUDA(cudaGetLastError());
+  last_layout_ = layouts.back();
+  last_sinks_ = groups.back().sinks;
+  last_device_sinks_ = false;
+  has_run_ = true;
+  last_reused_ = false;
+  sorted_valid_ = false;  // a batch never hands its order to a later frame
 }
 
 void Pipeline::fetch_counters() {

@@ -139,6 +139,20 @@ class Pipeline {
     enqueue(views.data(), (uint32_t)views.size(), images, image_bases.data(), sinks);
   }
   RunResult sync();
+  // One batch of launch groups: group g renders views [first, first + count)
+  // into `images` with host sinks `sinks`. With graphs on, the whole
+  // sequence becomes one CUDA graph from the second time the same group
+  // layouts are seen: every group's view table is a captured copy from a
+  // pinned staging area that the host refills before each launch (the
+  // previous launch having read it). Otherwise the groups are enqueued one
+  // by one, as by enqueue().
+  struct GroupRun {
+    uint32_t first, count;
+    HostSinks sinks;
+  };
+  void enqueue_groups(const ViewSpec *views, uint32_t *images, const uint64_t *image_bases,
+                      const std::vector<GroupRun> &groups);
+  uint64_t batch_graph_launches() const { return batch_graph_launches_; }
   // Grows the pair buffers to hold at least `pairs` tile pairs.
   void reserve_pairs(uint64_t pairs) { ensure_key_workspace(pairs); }
 
@@ -294,6 +308,37 @@ class Pipeline {
   static constexpr size_t kGraphCacheSize = 64;
   std::vector<GraphEntry> graphs_;
   std::vector<GraphKey> seen_keys_;  // layouts launched once without a graph
+  // Whole-batch graphs (enqueue_groups).
+  struct BatchKey {
+    std::vector<Layout> layouts;
+    std::vector<FrameCounters *> counters;
+    std::vector<ViewCounters *> views;
+    uint32_t *images;
+    uint64_t key_cap;
+    uint32_t tile, blend;
+    bool debug;
+    RasterConfig raster;
+    bool operator==(const BatchKey &o) const {
+      return layouts == o.layouts && counters == o.counters && views == o.views &&
+             images == o.images && key_cap == o.key_cap && tile == o.tile && blend == o.blend &&
+             debug == o.debug && raster == o.raster;
+    }
+  };
+  struct BatchGraph {
+    BatchKey key;
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    uint64_t last_use;
+  };
+  static constexpr size_t kBatchGraphCacheSize = 8;
+  std::vector<BatchGraph> batch_graphs_;
+  std::vector<BatchKey> batch_seen_;
+  unsigned char *batch_stage_ = nullptr;  // pinned: every group's view table, back to back
+  uint64_t batch_stage_bytes_ = 0;
+  cudaEvent_t batch_ev_ = nullptr;        // the last batch launch has read the staging area
+  bool batch_mode_ = false;               // launch_all: table copied, no phase events
+  uint64_t batch_graph_launches_ = 0;
+  void drop_batch_graphs();
   uint64_t graph_clock_ = 0;
 };
 

@@ -104,7 +104,7 @@ class GsplatBatchViewStats(ctypes.Structure):
 class GsplatBatchTimes(ctypes.Structure):
     _fields_ = [("device_ms", ctypes.c_float), ("wall_ms", ctypes.c_float),
                 ("groups", ctypes.c_uint32), ("reruns", ctypes.c_uint32),
-                ("kernel_launches", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("kernel_launches", ctypes.c_uint32), ("graph_launches", ctypes.c_uint32),
                 ("tile_pairs", ctypes.c_uint64)]
 
 

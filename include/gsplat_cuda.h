@@ -258,7 +258,8 @@ typedef struct GsplatBatchTimes {
   uint32_t groups;       /* launch groups */
   uint32_t reruns;       /* groups re-run after outgrowing their pair buffers */
   uint32_t kernel_launches;
-  uint32_t reserved;
+  uint32_t graph_launches; /* CUDA graph launches of the first pass: 1 once the same batch layout
+                              repeats (every group captured in one graph), 0 the first time */
   uint64_t tile_pairs;   /* over all views */
 } GsplatBatchTimes;
 
