@@ -643,6 +643,18 @@ void Pipeline::enqueue_groups(const ViewSpec *views, uint32_t *images,
   for (auto &g : batch_graphs_)
     if (g.key == key) hit = &g;
   const bool seen = std::find(batch_seen_.begin(), batch_seen_.end(), key) != batch_seen_.end();
+#ifdef GSR_BATCH_DEBUG
+  fprintf(stderr, "batch: groups %zu hit %d seen %d graphs %zu seen_list %zu key_cap %llu images %p\n",
+          groups.size(), hit != nullptr, (int)seen, batch_graphs_.size(), batch_seen_.size(),
+          (unsigned long long)key_cap_, (void *)images);
+  if (!batch_seen_.empty()) {
+    const BatchKey &o = batch_seen_.back();
+    fprintf(stderr, "  vs last seen: layouts %d counters %d views %d images %d cap %d tile %d blend %d dbg %d raster %d\n",
+            o.layouts == key.layouts, o.counters == key.counters, o.views == key.views,
+            o.images == key.images, o.key_cap == key.key_cap, o.tile == key.tile, o.blend == key.blend,
+            o.debug == key.debug, o.raster == key.raster);
+  }
+#endif
   batch_mode_ = true;
   try {
     if (!hit && !seen) {
