@@ -875,6 +875,9 @@ int32_t gsplat_batch_get_stream(const GsplatBatch *batch, void **out_stream) {
 
 // ---- served rendering (gsplat_cuda.h) ----------------------------------------
 
+static_assert(sizeof(GsplatServeConfig) == 48, "GsplatServeConfig layout");
+static_assert(sizeof(GsplatServeStats) == 176, "GsplatServeStats layout");
+
 int32_t gsplat_server_create(const GsplatServeConfig *config, GsplatServer **out_server) {
   return guarded("gsplat_server_create", [&]() -> int32_t {
     if (!out_server) return fail(Code::InvalidArgument, "gsplat_server_create: out_server is null");
@@ -882,6 +885,7 @@ int32_t gsplat_server_create(const GsplatServeConfig *config, GsplatServer **out
     gsr::ServeConfig c;
     if (config) {
       c.result_pool_mib = config->result_pool_mib;
+      c.max_queue_ms = config->max_queue_ms;
       if (config->scene_budget_bytes) c.scene_budget = config->scene_budget_bytes;
       if (config->work_budget_bytes) c.work_budget = config->work_budget_bytes;
       if (config->lanes) c.lanes = config->lanes;
@@ -1008,7 +1012,7 @@ int32_t gsplat_server_get_stats(GsplatServer *server, GsplatServeStats *out_stat
                                   s.peak_admitted_bytes, s.p50_ms, s.p99_ms, s.mean_ms, s.max_ms,
                                   s.views_per_s, s.mean_batch_views, s.device_ms, s.launch_ms,
                                   s.retire_ms, s.graph_captures, s.pinned_slabs, s.capture_ms,
-                                  s.pinned_alloc_ms, s.workspace_regrowths, s.regrowth_ms};
+                                  s.pinned_alloc_ms, s.workspace_regrowths, s.regrowth_ms, s.shed};
     return ok();
   });
 }

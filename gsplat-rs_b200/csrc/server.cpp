@@ -274,6 +274,7 @@ ServeStats Server::stats() {
   s.submitted = submitted_;
   s.completed = latencies_.size();
   s.failed = failed_;
+  s.shed = shed_;
   s.batches = batches_;
   s.reruns = reruns_;
   s.peak_admitted_bytes = peak_admitted_;
@@ -328,7 +329,7 @@ void Server::host_costs(uint64_t &captures, double &capture_ms, uint64_t &slabs,
 void Server::reset_stats() {
   std::lock_guard<std::mutex> g(mu_);
   latencies_.clear();
-  submitted_ = failed_ = batches_ = batch_views_ = reruns_ = 0;
+  submitted_ = failed_ = batches_ = batch_views_ = reruns_ = shed_ = 0;
   peak_admitted_ = 0;
   first_submit_ = -1;
   last_done_ = 0;
@@ -354,6 +355,26 @@ void Server::on_lane_done(void *arg) {
 }
 
 bool Server::launch(LaneState &ls, std::unique_lock<std::mutex> &lk) {
+  // Shed the requests that have waited longer than the queueing bound (the
+  // queue is in arrival order, so they are at its front).
+  if (cfg_.max_queue_ms) {
+    const double now = now_ms();
+    bool shed = false;
+    while (!queue_.empty()) {
+      Request &r = requests_.at(queue_.front());
+      if (now - r.t_submit <= (double)cfg_.max_queue_ms) break;
+      queue_.pop_front();
+      r.info.status = RequestStatus::Failed;
+      r.info.error_code = (int32_t)Code::Unsupported;
+      r.info.error = "request shed: queued longer than the server's max_queue_ms (" +
+                     std::to_string(cfg_.max_queue_ms) + " ms)";
+      r.info.queue_ms = (float)(now - r.t_submit);
+      ++failed_;
+      ++shed_;
+      shed = true;
+    }
+    if (shed) done_cv_.notify_all();
+  }
   if (queue_.empty()) return false;
   const uint64_t lane_budget = cfg_.work_budget / cfg_.lanes;
   ls.ids.clear();

@@ -34,6 +34,10 @@ struct ServeConfig {
   uint32_t tile = 16;
   RasterConfig raster;  // chunk 0 = full tile
   uint32_t result_pool_mib = 0;  // pinned result memory reserved at creation
+  // A request still queued this long after its submit is shed (fails with
+  // Unsupported) when a lane next admits work, so that under overload the
+  // requests that do run keep a bounded queueing delay; 0 = never shed.
+  uint32_t max_queue_ms = 0;
 };
 
 enum class RequestStatus : uint32_t { Queued = 0, Running = 1, Done = 2, Failed = 3 };
@@ -64,6 +68,7 @@ struct ServeStats {
                                // launch_ms; slabs added in the background are not counted)
   uint64_t workspace_regrowths = 0;  // lane workspace reallocations
   double regrowth_ms = 0;            // host time in them (part of launch_ms)
+  uint64_t shed = 0;                 // requests shed after max_queue_ms in the queue (in failed)
 };
 
 // Pinned host buffers recycled by size, carved from slabs of about 64 MB
@@ -176,7 +181,7 @@ class Server {
   bool stop_ = false;
   // statistics since the last reset
   std::vector<double> latencies_;
-  uint64_t submitted_ = 0, failed_ = 0, batches_ = 0, batch_views_ = 0, reruns_ = 0;
+  uint64_t submitted_ = 0, failed_ = 0, batches_ = 0, batch_views_ = 0, reruns_ = 0, shed_ = 0;
   uint64_t peak_admitted_ = 0;
   double first_submit_ = -1, last_done_ = 0;
   double device_ms_ = 0, launch_ms_ = 0, retire_ms_ = 0;

@@ -112,7 +112,8 @@ class GsplatServeConfig(ctypes.Structure):
     _fields_ = [("scene_budget_bytes", ctypes.c_uint64), ("work_budget_bytes", ctypes.c_uint64),
                 ("lanes", ctypes.c_uint32), ("max_views_per_batch", ctypes.c_uint32),
                 ("tile_size", ctypes.c_uint32), ("raster_chunk", ctypes.c_uint32),
-                ("raster_blocks_per_sm", ctypes.c_uint32), ("result_pool_mib", ctypes.c_uint32)]
+                ("raster_blocks_per_sm", ctypes.c_uint32), ("result_pool_mib", ctypes.c_uint32),
+                ("max_queue_ms", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class GsplatTuneResult(ctypes.Structure):
@@ -140,7 +141,7 @@ class GsplatServeStats(ctypes.Structure):
                 ("retire_ms", ctypes.c_double), ("graph_captures", ctypes.c_uint64),
                 ("pinned_slabs", ctypes.c_uint64), ("capture_ms", ctypes.c_double),
                 ("pinned_alloc_ms", ctypes.c_double), ("workspace_regrowths", ctypes.c_uint64),
-                ("regrowth_ms", ctypes.c_double)]
+                ("regrowth_ms", ctypes.c_double), ("shed", ctypes.c_uint64)]
 
 
 REQUEST_QUEUED, REQUEST_RUNNING, REQUEST_DONE, REQUEST_FAILED = 0, 1, 2, 3
@@ -647,9 +648,9 @@ class Server:
     """One GsplatServer: resident scenes and a continuous-batching request loop."""
 
     def __init__(self, lanes=0, max_views=0, tile=0, scene_budget=0, work_budget=0,
-                 raster_chunk=0, raster_blocks_per_sm=0, result_pool_mib=0):
+                 raster_chunk=0, raster_blocks_per_sm=0, result_pool_mib=0, max_queue_ms=0):
         cfg = GsplatServeConfig(scene_budget, work_budget, lanes, max_views, tile, raster_chunk,
-                                raster_blocks_per_sm, result_pool_mib)
+                                raster_blocks_per_sm, result_pool_mib, max_queue_ms, 0)
         self.ptr = ctypes.c_void_p()
         check(lib().gsplat_server_create(ctypes.byref(cfg), ctypes.byref(self.ptr)))
         self.sizes = {}

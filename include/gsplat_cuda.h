@@ -348,7 +348,12 @@ typedef struct GsplatServeConfig {
                                    (pinning on demand stalls the request loop for tens of ms
                                    per 64 MiB, so a server that must keep its latency under
                                    load reserves what its outstanding results will hold) */
-} GsplatServeConfig;            /* 40 bytes */
+  uint32_t max_queue_ms;        /* a request still queued this long after submit is shed:
+                                   it fails with GSPLAT_ERROR_UNSUPPORTED ("request shed") when a
+                                   lane next takes work, so under overload the requests that run
+                                   keep a bounded queueing delay; 0 = never shed */
+  uint32_t reserved;
+} GsplatServeConfig;            /* 48 bytes */
 
 typedef enum GsplatRequestStatus {
   GSPLAT_REQUEST_QUEUED = 0,
@@ -383,7 +388,8 @@ typedef struct GsplatServeStats {
   double pinned_alloc_ms;    /* host time launches waited on allocations (part of launch_ms) */
   uint64_t workspace_regrowths; /* lane workspace reallocations (each waits for an idle device) */
   double regrowth_ms;        /* host time in them (part of launch_ms) */
-} GsplatServeStats;          /* 168 bytes */
+  uint64_t shed;             /* requests shed after max_queue_ms in the queue (counted in failed) */
+} GsplatServeStats;          /* 176 bytes */
 
 int32_t gsplat_server_create(const GsplatServeConfig *config, GsplatServer **out_server);
 /* Finishes the batches in flight, fails queued requests and frees everything. */

@@ -47,10 +47,10 @@ def test_abi_struct_sizes():
     assert ctypes.sizeof(ffi.GsplatBatchView) == 56
     assert ctypes.sizeof(ffi.GsplatBatchViewStats) == 16
     assert ctypes.sizeof(ffi.GsplatBatchTimes) == 32
-    assert ctypes.sizeof(ffi.GsplatServeConfig) == 40
+    assert ctypes.sizeof(ffi.GsplatServeConfig) == 48
     assert ctypes.sizeof(ffi.GsplatTuneResult) == 32
     assert ctypes.sizeof(ffi.GsplatRequestInfo) == 32
-    assert ctypes.sizeof(ffi.GsplatServeStats) == 168
+    assert ctypes.sizeof(ffi.GsplatServeStats) == 176
 
 
 def test_versions_defaults_and_messages(oracle):
@@ -126,7 +126,7 @@ def test_server_null_and_no_gpu_errors():
     rid = ctypes.c_uint64()
     assert L.gsplat_server_submit(None, None, ctypes.byref(rid)) == 1
     assert "server is null" in ffi.last_error()
-    cfg = ffi.GsplatServeConfig(0, 0, 9, 0, 0, 0, 0, 0)  # lanes must be 1..8
+    cfg = ffi.GsplatServeConfig(0, 0, 9, 0, 0, 0, 0, 0, 0, 0)  # lanes must be 1..8
     out = ctypes.c_void_p(1)
     assert L.gsplat_server_create(ctypes.byref(cfg), ctypes.byref(out)) == 1
     assert not out.value

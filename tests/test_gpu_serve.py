@@ -189,3 +189,33 @@ def test_reserved_result_pool_serves_without_pinning_on_demand():
         for k, rid in enumerate(ids):
             assert np.array_equal(srv.read_rgba8(rid), plain[k][0]), f"request {k}"
             srv.release(rid)
+
+
+def test_served_overload_sheds_requests_queued_past_the_bound():
+    """Overload with a queueing bound: one lane, one request per batch, a
+    burst far above the rate the lane serves. Requests still queued 5 ms after
+    their submit are shed (FAILED, UNSUPPORTED) when the lane next takes work;
+    every request that runs was admitted within the bound, and its image is
+    still the plain render's."""
+    scenes = _scenes()
+    reqs = _requests(31, 120, len(scenes))
+    plain = _plain_images(scenes, reqs)
+    with ffi.Server(lanes=1, max_views=1, max_queue_ms=5) as srv:
+        for s in scenes:
+            srv.add_scene(s)
+        ids = [srv.submit(*r) for r in reqs]
+        shed = 0
+        for k, rid in enumerate(ids):
+            info = srv.wait(rid)
+            if info.status == ffi.REQUEST_FAILED:
+                assert info.error_code == ffi.UNSUPPORTED
+                assert info.queue_ms > 5.0
+                shed += 1
+            else:
+                assert info.status == ffi.REQUEST_DONE
+                assert info.queue_ms <= 5.0 + 1.0, info.queue_ms
+                assert np.array_equal(srv.read_rgba8(rid), plain[k][0]), k
+            srv.release(rid)
+        st = srv.stats()
+        assert shed > 0 and st.shed == shed and st.failed >= shed
+        assert st.completed + shed == len(reqs)
