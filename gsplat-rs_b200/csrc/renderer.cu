@@ -150,12 +150,17 @@ void Renderer::load_scene_path(const std::string &path) {
   scene_changed();
 }
 
+// Image slots only grow (a context that alternates sizes keeps its buffers,
+// and with them the pointers its captured graphs use: a reallocation costs a
+// device synchronisation, a free and an allocation, milliseconds under a
+// loaded allocator); they shrink only when 64 times larger than needed.
 void Renderer::ensure_image() {
   const uint64_t need = 4ull * width_ * height_;
   const uint32_t slots = image_slots();
   bool ok = true;
   for (uint32_t k = 0; k < slots; ++k)
-    ok = ok && image_[k].size() >= need && image_[k].size() <= 2 * need;
+    ok = ok && image_[k].size() >= need &&
+         (image_[k].size() <= 64 * need || image_[k].size() <= (64ull << 20));
   if (!ok) {
     if (deferred_.pending) issue_copy(false);
     sync_all_lanes();
