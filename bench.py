@@ -523,10 +523,11 @@ def measure_served(ffi, rates, seconds, max_requests):
         for rid in warm:
             srv.wait(rid)
             srv.release(rid)
-    # ... and single requests, one at a time, twice for every (scene, size):
-    # a light load runs one-view batches, whose launch graphs the lanes
-    # capture on a layout's second run, as a server in steady state has.
-    for _ in range(2):
+    # ... and single requests, one at a time, four times for every (scene,
+    # size): a light load runs one-view batches, whose launch graphs a lane
+    # captures on a layout's second run on that lane (a capture takes about
+    # 3 ms of the scheduler's time), as a server in steady state has.
+    for _ in range(4):
         for sid in range(len(scenes)):
             for w, h in gsplat_scenes.RESOLUTIONS:
                 rid = srv.submit(sid, cam0, w, h)
