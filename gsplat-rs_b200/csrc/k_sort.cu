@@ -306,8 +306,13 @@ __device__ __forceinline__ void pass_tile(const SortPlan *__restrict__ plan, uin
 // Persistent pass: a fixed grid of blocks takes tiles from an atomic ticket
 // (so look-back only ever waits on tiles already taken by running blocks)
 // until the item count, read on the device, is covered.
-template <int kIpt>
-__global__ void __launch_bounds__(kThreads, kIpt > 8 ? GSR_SORT_MIN_BLOCKS_LARGE : GSR_SORT_MIN_BLOCKS)
+// kMinBlocks: resident blocks per SM the register allocation must allow.
+// Sorts that leave L2 (tens of millions of keys and more) are latency bound
+// on their memory traffic and gain from a fourth resident block, though it
+// costs spills (64 registers); L2-resident sorts (a 1080p frame's 1.9 M tile
+// pairs) are faster with three.
+template <int kIpt, int kMinBlocks = (kIpt > 8 ? GSR_SORT_MIN_BLOCKS_LARGE : GSR_SORT_MIN_BLOCKS)>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
     pass_kernel(const SortPlan *__restrict__ plan, uint32_t pass, uint32_t shift, uint32_t *k0,
                 uint32_t *v0, uint32_t *k1, uint32_t *v1, uint32_t *status, uint32_t *ticket,
                 uint32_t *error) {
@@ -336,6 +341,8 @@ __global__ void __launch_bounds__(kThreads, kIpt > 8 ? GSR_SORT_MIN_BLOCKS_LARGE
 #endif
 constexpr int kIptLarge = GSR_SORT_IPT_LARGE;
 static_assert(kIptLarge > 8, "the large tile must hold more keys per thread than the small one");
+// Sorts sized for this many keys or more run the four-blocks-per-SM pass.
+constexpr uint32_t kHugeSort = 1u << 24;
 inline uint32_t ipt_for(uint32_t capacity) {
   return capacity <= (1u << 21) ? 8u : (uint32_t)kIptLarge;
 }
@@ -367,14 +374,15 @@ int current_device() {
 }
 // Resident pass blocks on the current device (the persistent grid), looked
 // up once per device.
-template <int kIpt>
+template <int kIpt, int kMinBlocks>
 uint32_t resident_pass_blocks() {
   static std::atomic<uint32_t> cache[kMaxDevices];
   const int dev = current_device();
   uint32_t blocks = cache[dev].load(std::memory_order_relaxed);
   if (blocks == 0) {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel<kIpt>, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel<kIpt, kMinBlocks>,
+                                                  kThreads, 0);
     blocks = device_sm_count() * (uint32_t)std::max(per_sm, 1);
     cache[dev].store(blocks, std::memory_order_relaxed);
   }
@@ -419,15 +427,22 @@ void launch_sort(const SortBuffers &b, cudaStream_t stream) {
                                                     b.plan, status, tiles, kThreads * ipt);
   for (uint32_t p = 0; p < b.passes; ++p) {
     uint32_t *st = status + (size_t)p * tiles * 256;
+    constexpr int kSmall = GSR_SORT_MIN_BLOCKS, kLarge = GSR_SORT_MIN_BLOCKS_LARGE;
     if (ipt == 8) {
-      const uint32_t g = std::min(grid, resident_pass_blocks<8>());
-      pass_kernel<8><<<g, kThreads, 0, stream>>>(b.plan, p, b.begin_bit + 8 * p, b.keys0, b.vals0,
-                                                 b.keys1, b.vals1, st, tickets + p, b.error);
-    } else {
-      const uint32_t g = std::min(grid, resident_pass_blocks<kIptLarge>());
-      pass_kernel<kIptLarge><<<g, kThreads, 0, stream>>>(b.plan, p, b.begin_bit + 8 * p, b.keys0,
+      const uint32_t g = std::min(grid, resident_pass_blocks<8, kSmall>());
+      pass_kernel<8, kSmall><<<g, kThreads, 0, stream>>>(b.plan, p, b.begin_bit + 8 * p, b.keys0,
                                                          b.vals0, b.keys1, b.vals1, st,
                                                          tickets + p, b.error);
+    } else if (b.capacity < kHugeSort) {
+      const uint32_t g = std::min(grid, resident_pass_blocks<kIptLarge, kLarge>());
+      pass_kernel<kIptLarge, kLarge><<<g, kThreads, 0, stream>>>(
+          b.plan, p, b.begin_bit + 8 * p, b.keys0, b.vals0, b.keys1, b.vals1, st, tickets + p,
+          b.error);
+    } else {
+      const uint32_t g = std::min(grid, resident_pass_blocks<kIptLarge, 4>());
+      pass_kernel<kIptLarge, 4><<<g, kThreads, 0, stream>>>(b.plan, p, b.begin_bit + 8 * p,
+                                                            b.keys0, b.vals0, b.keys1, b.vals1,
+                                                            st, tickets + p, b.error);
     }
   }
 }

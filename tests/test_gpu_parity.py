@@ -208,8 +208,10 @@ def test_sort_gpu_radix_cases(kats, oracle):
     assert np.array_equal(ffi.sort_values_by_keys(np.full(eq["count"], eq["key"], np.uint32), ids), ids)
 
 
-@pytest.mark.parametrize("n", [3_000_000, 5_000_001])
+@pytest.mark.parametrize("n", [3_000_000, 5_000_001, 17_000_003])
 def test_sort_large_with_ties(oracle, n):
+    """Heavy ties over millions of keys; 17 M keys run the four-blocks-per-SM
+    pass of sorts that leave L2."""
     rng = np.random.default_rng(n)
     keys = rng.integers(0, 1 << 20, n, dtype=np.uint32)  # heavy ties, top byte constant
     vals = rng.permutation(n).astype(np.uint32)
