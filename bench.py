@@ -56,8 +56,8 @@ FALLBACK_HBM_GBS = 6650.0
 # the command): DRAM bytes read + written, warp instructions issued, and
 # executed FP32 thread operations (2 x FFMA + FADD + FMUL). None until
 # captured for the current kernel.
-NCU_RASTER = {"dram_bytes": 18_304_256, "warp_inst": 148_805_815,
-              "thread_flop": 2 * 922_818_785 + 128_638_205 + 270_554_805,
+NCU_RASTER = {"dram_bytes": 18_312_960, "warp_inst": 120_559_340,
+              "thread_flop": 2 * 1_223_868_317 + 202_085_090 + 375_960_460,
               "source": "profiles/frame_279k_sh3_1080p.md (ncu --set full, one launch)"}
 
 

@@ -1,11 +1,13 @@
 // K4: per-tile raster. Built with --fmad=false; every fused multiply-add is
 // an explicit fmaf, so a C++ restatement reproduces each pixel bit for bit.
 //
-// One block per tile, one thread per pixel. The tile's splat list (reference
-// back-to-front order restricted to the tile) is staged into shared memory in
-// chunks of one record per thread with cp.async (16-byte async copies, the
-// record gather is random so tiled TMA does not apply), double-buffered so
-// the next chunk's gather overlaps the current chunk's blending.
+// One block per tile; one thread per pixel, or two pixels of one row per
+// thread for FP32 on 16x16 tiles (GSR_RASTER_PX, default 2). The tile's
+// splat list (reference back-to-front order restricted to the tile) is
+// staged into shared memory in chunks of records with cp.async (16-byte
+// async copies, the record gather is random so tiled TMA does not apply),
+// double-buffered so the next chunk's gather overlaps the current chunk's
+// blending.
 //
 // Per pixel, the fragment rule of the reference shader
 // (crates/gsplat-render-wgpu/shaders/splat_surface_direct.wgsl:336-369):
@@ -25,6 +27,10 @@
 
 #include "device_common.cuh"
 #include "kernels.h"
+
+#ifndef GSR_RASTER_PX
+#define GSR_RASTER_PX 2
+#endif
 
 
 namespace gsr {
@@ -100,17 +106,17 @@ __device__ __forceinline__ uint32_t ellipse_block_mask(float4 ra, float4 rb, flo
   return mask;
 }
 
-// Ordered compaction of the chunk entries whose mask has this warp's bit
-// into list[] (ballots keep the list order); returns their count.
+// Ordered compaction of the chunk entries whose mask meets sel (the warp's
+// blocks) into list[] (ballots keep the list order); returns their count.
 // Entries are stored as k << shift (shift 4: the byte offset of a float4
 // array element).
 __device__ __forceinline__ uint32_t compact_warp_entries(const uint8_t *mask, uint32_t n_in,
-                                                        uint32_t warp, uint32_t lane,
+                                                        uint32_t sel, uint32_t lane,
                                                         uint16_t *list, uint32_t shift = 0) {
   uint32_t n_w = 0;
   for (uint32_t k0 = 0; k0 < n_in; k0 += 32) {
     const uint32_t k = k0 + lane;
-    const bool hit = k < n_in && ((mask[k] >> warp) & 1u);
+    const bool hit = k < n_in && (mask[k] & sel) != 0;
     const uint32_t bal = __ballot_sync(0xffffffffu, hit);
     if (hit) list[n_w + __popc(bal & lanemask_lt())] = (uint16_t)(k << shift);
     n_w += __popc(bal);
@@ -244,7 +250,7 @@ __global__ void __launch_bounds__(kTile *kTile) raster_unorm8_kernel(RasterArgs 
       sm.mask[tid] = (uint8_t)ellipse_block_mask<kTile>(ra, rb, thr, ra.x - ftx, ra.y - fty);
     }
     __syncthreads();
-    const uint32_t n_w = compact_warp_entries(sm.mask, n_in, warp, lane, sm.list[warp], 4);
+    const uint32_t n_w = compact_warp_entries(sm.mask, n_in, 1u << warp, lane, sm.list[warp], 4);
     if (inside) {
       uint32_t i = 0;
       // two entries per step: the second's coverage and weight do not wait
@@ -273,23 +279,32 @@ __global__ void __launch_bounds__(kTile *kTile) raster_unorm8_kernel(RasterArgs 
         (uint32_t)t0 | ((uint32_t)t1 << 8) | ((uint32_t)t2 << 16) | ((uint32_t)t3 << 24);
 }
 
-// FP32 front-to-back mode. Threads map to 8x4-pixel warp blocks (lane l of
-// warp w covers column (w % (kTile/8))*8 + (l & 7), row (w / (kTile/8))*4 +
-// (l >> 3)). Per chunk of kChunk list entries:
+// FP32 front-to-back mode. kPx = 1: threads map to 8x4-pixel warp blocks
+// (lane l of warp w covers column (w % (kTile/8))*8 + (l & 7), row
+// (w / (kTile/8))*4 + (l >> 3)). kPx = 2 (16x16 tiles): warp w covers the
+// 16x4 band of rows 4w..4w+3, lane l the pixels (l & 7, 4w + (l >> 3)) and
+// (8 + (l & 7), 4w + (l >> 3)): both share a row, so the row term of the
+// local coordinates, fma(ay, y, ox), and the entry's three shared loads serve
+// two pixels, and each pixel still evaluates the same expressions as with
+// kPx = 1. Per chunk of kChunk list entries:
 //   1. raw records arrive by cp.async (double-buffered, next chunk in flight);
 //   2. one thread per entry derives, for this tile, the local offsets ox, oy
 //      (local = (ax*lx + ay*ly + ox, bx*lx + by*ly + oy) for pixel coordinates
-//      relative to the 16-pixel grid corner), s^2, and a bit mask of the warp
+//      relative to the 16-pixel grid corner), s^2, and a bit mask of the 8x4
 //      blocks the ellipse |local| <= s reaches (band intervals plus half a
 //      pixel);
-//   3. each warp compacts the entries whose mask has its bit (ballots keep the
-//      list order) and blends only those; a pixel stops at T < 1e-4, a warp
-//      when all 32 pixels have, the block when all pixels have.
+//   3. each warp compacts the entries whose mask meets its blocks (ballots
+//      keep the list order) and blends only those; a pixel stops at
+//      T < 1e-4, a warp when all its pixels have, the block when all pixels
+//      have.
 // Culling is conservative, so results equal the unculled per-pixel walk, and
-// neither the chunk size nor the tile order changes any pixel.
-template <int kTile, int kChunk>
+// neither the chunk size, the pixels per thread nor the tile order changes
+// any pixel.
+template <int kTile, int kChunk, int kPx>
 struct Fp32Smem {
-  static constexpr int kWarps = kTile * kTile / 32;
+  static_assert(kPx == 1 || (kPx == 2 && kTile == 16), "two pixels per thread on 16x16 tiles");
+  static constexpr int kThreads = kTile * kTile / kPx;
+  static constexpr int kWarps = kThreads / 32;
   float4 raw[2][3][kChunk];
   float4 d0[kChunk];  // ax, ay, ox, thr (coverage bound on r^2)
   float4 d1[kChunk];  // bx, by, oy, -
@@ -300,11 +315,11 @@ struct Fp32Smem {
   uint32_t next;
 };
 
-template <int kTile, int kChunk>
+template <int kTile, int kChunk, int kPx>
 __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t tile,
-                                                 Fp32Smem<kTile, kChunk> &sm) {
+                                                 Fp32Smem<kTile, kChunk, kPx> &sm) {
   constexpr int kBlocksX = kTile / 8;
-  constexpr int kWarps = Fp32Smem<kTile, kChunk>::kWarps;
+  constexpr int kThreads = Fp32Smem<kTile, kChunk, kPx>::kThreads;
   if (threadIdx.x == 0)
     sm.view = find_view(a.num_views, tile, [&](uint32_t v) { return a.views[v].tile_base; });
   __syncthreads();
@@ -316,14 +331,23 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
   const uint32_t tx = local_tile % tiles_x, ty = local_tile / tiles_x;
   const uint32_t x0 = tx * kTile, y0 = ty * kTile;
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint32_t bx0 = (warp % kBlocksX) * 8, by0 = (warp / kBlocksX) * 4;
+  const uint32_t bx0 = kPx == 1 ? (warp % kBlocksX) * 8 : 0;
+  const uint32_t by0 = kPx == 1 ? (warp / kBlocksX) * 4 : warp * 4;
+  // the 8x4 blocks this warp's pixels lie in
+  const uint32_t sel = kPx == 1 ? 1u << warp : 3u << (2 * warp);
   const uint32_t lxp = bx0 + (lane & 7), lyp = by0 + (lane >> 3);
   const uint32_t px = x0 + lxp, py = y0 + lyp;
-  const bool inside = px < width && py < height;
   // Local coordinates are taken from the 16-pixel grid corner at or before
   // the tile, so 8x8 and 16x16 tiles evaluate every pixel identically.
   const uint32_t ax0 = x0 & ~15u, ay0 = y0 & ~15u;
-  const float fx = (float)(px - ax0), fy = (float)(py - ay0);
+  const float fy = (float)(py - ay0);
+  float fx[kPx];
+  bool inside[kPx];
+#pragma unroll
+  for (int p = 0; p < kPx; ++p) {
+    fx[p] = (float)(px + 8 * p - ax0);
+    inside[p] = px + 8 * p < width && py < height;
+  }
   const float fax = (float)ax0, fay = (float)ay0;
   const float ftx = (float)x0, fty = (float)y0;
   const uint32_t *__restrict__ ids = a.plan->final_buffer == 0 ? a.ids0 : a.ids1;
@@ -332,18 +356,33 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
   const uint32_t chunks = (count + kChunk - 1) / kChunk;
 
   auto issue = [&](uint32_t c, int buf) {
-    uint32_t k = c * kChunk + tid;
-    if (tid < (uint32_t)kChunk && k < count) {
-      const Record *r = &a.records[ids[range.y - 1 - k]];
-      cp_async16(&sm.raw[buf][0][tid], &r->a);
-      cp_async16(&sm.raw[buf][1][tid], &r->b);
-      cp_async16(&sm.raw[buf][2][tid], &r->c);
+#pragma unroll
+    for (uint32_t t = tid; t < (uint32_t)kChunk; t += kThreads) {
+      const uint32_t k = c * kChunk + t;
+      if (k < count) {
+        const Record *r = &a.records[ids[range.y - 1 - k]];
+        cp_async16(&sm.raw[buf][0][t], &r->a);
+        cp_async16(&sm.raw[buf][1][t], &r->b);
+        cp_async16(&sm.raw[buf][2][t], &r->c);
+      }
     }
     cp_async_commit();
   };
 
-  float T = 1.0f, c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
-  bool done = !inside;
+  float T[kPx], c0[kPx], c1[kPx], c2[kPx];
+  bool done[kPx];
+#pragma unroll
+  for (int p = 0; p < kPx; ++p) {
+    T[p] = 1.0f;
+    c0[p] = c1[p] = c2[p] = 0.0f;
+    done[p] = !inside[p];
+  }
+  auto all_done = [&]() {
+    bool d = true;
+#pragma unroll
+    for (int p = 0; p < kPx; ++p) d = d && done[p];
+    return d;
+  };
   if (chunks > 0) issue(0, 0);
   for (uint32_t c = 0; c < chunks; ++c) {
     const int buf = c & 1;
@@ -351,26 +390,31 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
     else cp_async_commit();
     cp_async_wait_1();
     const uint32_t n_in = min((uint32_t)kChunk, count - c * kChunk);
-    if (tid < n_in) {
-      const float4 ra = sm.raw[buf][0][tid], rb = sm.raw[buf][1][tid], col = sm.raw[buf][2][tid];
-      float cxa = ra.x - fax, cya = ra.y - fay;
-      float ox = -fmaf(ra.z, cxa, ra.w * cya);
-      float oy = -fmaf(rb.x, cxa, rb.y * cya);
-      float cxl = ra.x - ftx, cyl = ra.y - fty;
-      // w > 1/256 exactly when r2 < (log2 alpha + 8) / (4.5 log2 e), so a
-      // pixel is covered when r2 <= thr: the largest float below that bound,
-      // capped at s^2 (nothing is covered when the bound is not positive).
-      const float s2 = rb.z * rb.z;
-      const float wlim = __fdiv_rn(col.w + 8.0f, 6.49212768f);
-      const float thr = wlim > 0.0f ? fminf(s2, __int_as_float(__float_as_int(wlim) - 1)) : -1.0f;
-      sm.d0[tid] = make_float4(ra.z, ra.w, ox, thr);
-      sm.d1[tid] = make_float4(rb.x, rb.y, oy, rb.w);
-      sm.d2[tid] = col;
-      sm.mask[tid] = (uint8_t)ellipse_block_mask<kTile>(ra, rb, thr, cxl, cyl);
+#pragma unroll
+    for (uint32_t t = tid; t < (uint32_t)kChunk; t += kThreads) {
+      if (t < n_in) {
+        const float4 ra = sm.raw[buf][0][t], rb = sm.raw[buf][1][t], col = sm.raw[buf][2][t];
+        float cxa = ra.x - fax, cya = ra.y - fay;
+        float ox = -fmaf(ra.z, cxa, ra.w * cya);
+        float oy = -fmaf(rb.x, cxa, rb.y * cya);
+        float cxl = ra.x - ftx, cyl = ra.y - fty;
+        // w > 1/256 exactly when r2 < (log2 alpha + 8) / (4.5 log2 e), so a
+        // pixel is covered when r2 <= thr: the largest float below that
+        // bound, capped at s^2 (nothing is covered when the bound is not
+        // positive).
+        const float s2 = rb.z * rb.z;
+        const float wlim = __fdiv_rn(col.w + 8.0f, 6.49212768f);
+        const float thr =
+            wlim > 0.0f ? fminf(s2, __int_as_float(__float_as_int(wlim) - 1)) : -1.0f;
+        sm.d0[t] = make_float4(ra.z, ra.w, ox, thr);
+        sm.d1[t] = make_float4(rb.x, rb.y, oy, rb.w);
+        sm.d2[t] = col;
+        sm.mask[t] = (uint8_t)ellipse_block_mask<kTile>(ra, rb, thr, cxl, cyl);
+      }
     }
     __syncthreads();
     // Ordered compaction of this warp's entries (as byte offsets).
-    const uint32_t n_w = compact_warp_entries(sm.mask, n_in, warp, lane, sm.list[warp], 4);
+    const uint32_t n_w = compact_warp_entries(sm.mask, n_in, sel, lane, sm.list[warp], 4);
     // Four list entries per step (one early-out vote, one packed index
     // load); each pixel still takes them strictly in list order.
     // w = alpha e^(-4.5 r2) = 2^(log2 alpha - 4.5 log2(e) r2) (the entry's
@@ -380,74 +424,69 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
     auto at = [&](const float4 *arr, uint32_t j) {
       return *reinterpret_cast<const float4 *>(reinterpret_cast<const char *>(arr) + j);
     };
-    // Branch-free: a lane that does not take the entry (finished, or not
+    // Branch-free: a pixel that does not take the entry (finished, or not
     // covered) blends with wT = 0, which leaves C and T bit for bit as they
     // are (fma(x, 0, c) = c and T - 0 = T for finite x).
-    auto blend = [&](uint32_t j, float r2, float thr) {
-      const bool take = !done && r2 <= thr;
-      const float4 col = at(sm.d2, j);
-      const float w = blend_weight(r2, col.w);
-      const float wT = take ? w * T : 0.0f;
-      c0 = fmaf(col.x, wT, c0);
-      c1 = fmaf(col.y, wT, c1);
-      c2 = fmaf(col.z, wT, c2);
-      T = T - wT;
-      done = done || T < 1e-4f;
-    };
-    auto local_r2 = [&](uint32_t j, float &s2) {
+    auto entry = [&](uint32_t j) {
       const float4 d0 = at(sm.d0, j);
       const float4 d1 = at(sm.d1, j);
-      const float lx = fmaf(d0.x, fx, fmaf(d0.y, fy, d0.z));
-      const float ly = fmaf(d1.x, fx, fmaf(d1.y, fy, d1.z));
-      s2 = d0.w;
-      return fmaf(lx, lx, ly * ly);
+      const float4 col = at(sm.d2, j);
+      const float rx = fmaf(d0.y, fy, d0.z), ry = fmaf(d1.y, fy, d1.z);
+#pragma unroll
+      for (int p = 0; p < kPx; ++p) {
+        const float lx = fmaf(d0.x, fx[p], rx);
+        const float ly = fmaf(d1.x, fx[p], ry);
+        const float r2 = fmaf(lx, lx, ly * ly);
+        const bool take = !done[p] && r2 <= d0.w;
+        const float w = blend_weight(r2, col.w);
+        const float wT = take ? w * T[p] : 0.0f;
+        c0[p] = fmaf(col.x, wT, c0[p]);
+        c1[p] = fmaf(col.y, wT, c1[p]);
+        c2[p] = fmaf(col.z, wT, c2[p]);
+        T[p] = T[p] - wT;
+        done[p] = done[p] || T[p] < 1e-4f;
+      }
     };
     uint32_t i = 0;
     for (; i + 3 < n_w; i += 4) {
-      if (__all_sync(0xffffffffu, done)) break;
+      if (__all_sync(0xffffffffu, all_done())) break;
       const uint2 jj = *reinterpret_cast<const uint2 *>(&sm.list[warp][i]);
-      const uint32_t ja = jj.x & 0xffffu, jb = jj.x >> 16, jc = jj.y & 0xffffu, jd = jj.y >> 16;
-      float sa, sb, sc, sd;
-      const float r2a = local_r2(ja, sa);
-      const float r2b = local_r2(jb, sb);
-      const float r2c = local_r2(jc, sc);
-      const float r2d = local_r2(jd, sd);
-      blend(ja, r2a, sa);
-      blend(jb, r2b, sb);
-      blend(jc, r2c, sc);
-      blend(jd, r2d, sd);
+      entry(jj.x & 0xffffu);
+      entry(jj.x >> 16);
+      entry(jj.y & 0xffffu);
+      entry(jj.y >> 16);
     }
     for (; i < n_w; ++i) {
-      if (__all_sync(0xffffffffu, done)) break;
-      const uint32_t ja = sm.list[warp][i];
-      float sa;
-      const float r2a = local_r2(ja, sa);
-      blend(ja, r2a, sa);
+      if (__all_sync(0xffffffffu, all_done())) break;
+      entry(sm.list[warp][i]);
     }
-    if (__syncthreads_count(done) == kTile * kTile) break;
+    if (__syncthreads_count(all_done()) == kThreads) break;
   }
   cp_async_wait_all();
-  if (inside)
-    image[(size_t)py * width + px] = to_unorm8(c0) | (to_unorm8(c1) << 8) |
-                                       (to_unorm8(c2) << 16) | (to_unorm8(1.0f - T) << 24);
+#pragma unroll
+  for (int p = 0; p < kPx; ++p)
+    if (inside[p])
+      image[(size_t)py * width + px + 8 * p] =
+          to_unorm8(c0[p]) | (to_unorm8(c1[p]) << 8) | (to_unorm8(c2[p]) << 16) |
+          (to_unorm8(1.0f - T[p]) << 24);
 }
 
 // One block per tile (kPersistent false), or a fixed grid of blocks that take
 // tiles from a global queue (an atomic ticket over the batch's tiles) until
 // it is empty.
-template <int kTile, int kChunk, bool kPersistent>
-__global__ void __launch_bounds__(kTile *kTile) raster_fp32_kernel(RasterArgs a) {
-  __shared__ Fp32Smem<kTile, kChunk> sm;
+template <int kTile, int kChunk, int kPx, bool kPersistent>
+__global__ void __launch_bounds__(kTile *kTile / kPx) raster_fp32_kernel(RasterArgs a) {
+  __shared__ Fp32Smem<kTile, kChunk, kPx> sm;
   fold_errors(a);
   if constexpr (!kPersistent) {
-    raster_fp32_tile<kTile, kChunk>(a, blockIdx.x, sm);
+    raster_fp32_tile<kTile, kChunk, kPx>(a, blockIdx.x, sm);
   } else {
     for (;;) {
       if (threadIdx.x == 0) sm.next = atomicAdd(&a.counters->raster_ticket, 1u);
       __syncthreads();
       const uint32_t tile = sm.next;
       if (tile >= a.total_tiles) break;
-      raster_fp32_tile<kTile, kChunk>(a, tile, sm);
+      raster_fp32_tile<kTile, kChunk, kPx>(a, tile, sm);
       __syncthreads();  // shared memory is reused by the next tile
     }
   }
@@ -468,20 +507,20 @@ void launch_raster(const RasterArgs &a, uint32_t tile, uint32_t blend_mode,
   const bool persistent = cfg.blocks_per_sm > 0;
   const uint32_t grid =
       persistent ? std::min<uint32_t>(a.total_tiles, cfg.blocks_per_sm * sm_count) : a.total_tiles;
-#define GSR_FP32(T, C)                                                           \
+#define GSR_FP32(T, C, P)                                                        \
   do {                                                                           \
     if (persistent)                                                              \
-      raster_fp32_kernel<T, C, true><<<grid, T * T, 0, stream>>>(a);             \
+      raster_fp32_kernel<T, C, P, true><<<grid, T * T / P, 0, stream>>>(a);      \
     else                                                                         \
-      raster_fp32_kernel<T, C, false><<<grid, T * T, 0, stream>>>(a);            \
+      raster_fp32_kernel<T, C, P, false><<<grid, T * T / P, 0, stream>>>(a);     \
   } while (0)
   if (tile == 16) {
-    if (cfg.chunk == 64) GSR_FP32(16, 64);
-    else if (cfg.chunk == 128) GSR_FP32(16, 128);
-    else GSR_FP32(16, 256);
+    if (cfg.chunk == 64) GSR_FP32(16, 64, GSR_RASTER_PX);
+    else if (cfg.chunk == 128) GSR_FP32(16, 128, GSR_RASTER_PX);
+    else GSR_FP32(16, 256, GSR_RASTER_PX);
   } else {
-    if (cfg.chunk == 32) GSR_FP32(8, 32);
-    else GSR_FP32(8, 64);
+    if (cfg.chunk == 32) GSR_FP32(8, 32, 1);
+    else GSR_FP32(8, 64, 1);
   }
 #undef GSR_FP32
 }
