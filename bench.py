@@ -29,6 +29,7 @@ import sys
 import tempfile
 import threading
 import time
+import types
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "gsplat-rs_b200"))
@@ -56,7 +57,7 @@ FALLBACK_HBM_GBS = 6650.0
 # the command): DRAM bytes read + written, warp instructions issued, and
 # executed FP32 thread operations (2 x FFMA + FADD + FMUL). None until
 # captured for the current kernel.
-NCU_RASTER = {"dram_bytes": 18_312_960, "warp_inst": 120_559_340,
+NCU_RASTER = {"dram_bytes": 18_312_448, "warp_inst": 119_637_791,
               "thread_flop": 2 * 1_223_868_317 + 202_085_090 + 375_960_460,
               "source": "profiles/frame_279k_sh3_1080p.md (ncu --set full, one launch)"}
 
@@ -198,6 +199,34 @@ def algorithmic_bytes(phase, counts, n, planes, width, height, tile_passes):
     if phase == "raster":
         return k * 52 + width * height * 4
     return 0
+
+
+def batched_preprocess_bytes(specs, stats, scenes, planes, set_views=16):
+    """Preprocess bytes of a batch at minimum: a view set (up to `set_views`
+    consecutive views of one scene in a launch group, in render order: views
+    sorted by scene, stable) reads its scene once: the 16-byte position of
+    every splat, and the 32-byte shape and the SH planes of each splat some
+    view of the set sees or draws (the per-view sums, capped at the scene);
+    every view writes its own keys, ids, rects and records."""
+    order = sorted(range(len(specs)), key=lambda v: specs[v][0])
+    total = 0
+    run = []
+
+    def close(run):
+        if not run:
+            return 0
+        n = scenes[specs[run[0]][0]]["positions"].shape[0]
+        shape = sum(stats[v].visible_count * 32 + stats[v].drawn_count * 16 * planes for v in run)
+        return n * 16 + min(shape, n * (32 + 16 * planes))
+
+    for v in order:
+        if run and (specs[v][0] != specs[run[0]][0] or stats[v].group != stats[run[0]].group
+                    or len(run) == set_views):
+            total += close(run)
+            run = []
+        run.append(v)
+        total += stats[v].visible_count * 16 + stats[v].drawn_count * 48
+    return total + close(run)
 
 
 def image_errors(img, ref):
@@ -404,6 +433,41 @@ def measure_batched(ffi, torch, steps, warmup, cameras_per_scene=64):
         for k in range(len(specs)):
             b.readback_rgba8(k, out[offs[k]:offs[k + 1]])
         e2e.append(time.perf_counter() - t0)
+    # Per-phase device times of the same batch, group by group (a measurement
+    # mode: each group waits for the one before, so no whole-batch graph),
+    # against each phase's algorithmic bytes summed over the views.
+    b.set_phase_timing(True)
+    b.render(arr)
+    b.render(arr)
+    phase_ms = b.phase_times()
+    b.set_phase_timing(False)
+    stats = [b.view_stats(k) for k in range(len(specs))]
+    group_tiles = {}
+    for k, (sid, _, w, h) in enumerate(specs):
+        g = stats[k].group
+        group_tiles[g] = group_tiles.get(g, 0) + ((w + 15) // 16) * ((h + 15) // 16)
+    group_passes = {}
+    for g, tiles in group_tiles.items():
+        p = 1
+        while (1 << (8 * p)) < tiles:
+            p += 1
+        group_passes[g] = p
+    hbm = hbm_peak_gbs()
+    phases = {}
+    for k, ms in phase_ms.items():
+        if k == "preprocess":
+            nbytes = batched_preprocess_bytes(specs, stats, scenes, 12)
+        else:
+            nbytes = 0
+            for v, (sid, _, w, h) in enumerate(specs):
+                st = stats[v]
+                c = types.SimpleNamespace(visible=st.visible_count, drawn=st.drawn_count,
+                                          tile_keys=st.tile_pairs)
+                nbytes += algorithmic_bytes(k, c, scenes[sid]["positions"].shape[0], 12, w, h,
+                                            group_passes[st.group])
+        gbs = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else None
+        phases[k] = {"ms": ms, "bytes": nbytes, "gbs": gbs,
+                     "frac_measured": gbs / hbm[0] if gbs else None}
     per_scene = []
     for sid in range(len(scenes)):
         sub = ffi.Batch.make_views([v for v in specs if v[0] == sid])
@@ -461,6 +525,10 @@ def measure_batched(ffi, torch, steps, warmup, cameras_per_scene=64):
             "plain_wall_views_per_s": n / plain_wall,
             "speedup_vs_plain": (n / (float(np.median(dev)) / 1000.0)) / (n / (plain_dev_total / 1000.0)),
             "per_scene": per_scene,
+            "phases": phases, "phases_hbm_peak_gbs": hbm[0], "phases_hbm_peak_source": hbm[1],
+            "phases_timing": "a separate phase-timed render of the same batch "
+                             "(gsplat_batch_set_phase_timing): per-phase CUDA events of each "
+                             "launch group, summed; groups run one by one",
             "timing": "device ms from CUDA events around all launch groups (batched) and the "
                       "per-phase CUDA events of each plain frame; scenes exceed L2"}
 
@@ -752,6 +820,16 @@ def measure_packed(ffi, torch, frames=60):
 
 
 NOMINAL_HBM_GBS = 8000.0  # B200 HBM3e data-sheet bandwidth, for context beside the measured peak
+
+
+def hbm_peak_gbs():
+    """(HBM copy peak in GB/s, "measured" | "fallback")."""
+    if os.path.exists(PEAKS_FILE):
+        with open(PEAKS_FILE) as f:
+            hbm = json.load(f).get("hbm_gbs")
+        if hbm:
+            return float(hbm), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
 
 
 def measure_config3(ffi, torch, frames=20):

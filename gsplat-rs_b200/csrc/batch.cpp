@@ -169,7 +169,7 @@ Lane::~Lane() {
 
 void Lane::enqueue(const std::vector<ViewSpec> &views, const std::vector<uint64_t> &bases,
                    uint64_t total_pixels, const std::vector<ViewGroup> &groups, uint64_t reserve,
-                   bool one_graph) {
+                   bool one_graph, float *phase_sums) {
   GSR_CUDA(cudaSetDevice(device_));
   const uint64_t need = 4 * std::max<uint64_t>(total_pixels, 1);
   if (images_.size() < need) {
@@ -201,6 +201,12 @@ void Lane::enqueue(const std::vector<ViewSpec> &views, const std::vector<uint64_
       HostSinks sinks{group_counters_.get() + g, view_counters_.get() + gr.first};
       pipe_->enqueue(views.data() + gr.first, gr.count, images_.as<uint32_t>(),
                      bases.data() + gr.first, sinks);
+      if (phase_sums) {
+        GSR_CUDA(cudaStreamSynchronize(stream_));
+        float t[kPhaseCount];
+        pipe_->phase_times(t);
+        for (int k = 0; k < kPhaseCount; ++k) phase_sums[k] += t[k];
+      }
     }
   }
   GSR_CUDA(cudaEventRecord(end_, stream_));
@@ -304,10 +310,13 @@ BatchResult Batch::render(const std::vector<BatchView> &in) {
   groups_ = plan_groups(specs_, predicted, tile_, limits_);
   uint64_t reserve = 0;
   for (const auto &g : groups_) reserve = std::max(reserve, g.predicted_pairs);
-  // the whole batch, every launch group, as one CUDA graph
+  // the whole batch, every launch group, as one CUDA graph (group by group
+  // when phase-timed)
   const uint64_t graphs_before = lane_->pipe().batch_graph_launches();
-  lane_->enqueue(specs_, bases_, pixels, groups_, reserve, true);
   BatchResult r;
+  r.phase_timed = phase_timing_;
+  lane_->enqueue(specs_, bases_, pixels, groups_, reserve, !phase_timing_,
+                 phase_timing_ ? r.phase_ms : nullptr);
   r.reruns = lane_->finish(specs_, bases_, groups_);
   r.device_ms = lane_->device_ms();
   r.groups = (uint32_t)groups_.size();

@@ -90,6 +90,9 @@ struct BatchResult {
   uint32_t groups = 0, reruns = 0, launches = 0;
   uint32_t graph_launches = 0;  // whole-batch graph launches of the first pass (0 or 1)
   uint64_t pairs = 0;      // tile pairs over all views
+  // per-phase device ms summed over the groups (phase-timed renders only)
+  float phase_ms[kPhaseCount] = {};
+  bool phase_timed = false;
 };
 
 // Pinned host array that only grows (pointer stable while the size fits).
@@ -123,9 +126,12 @@ class Lane {
   // in group_counters() once the stream reaches them. one_graph: every group
   // in one CUDA graph (Pipeline::enqueue_groups; for repeated batches), else
   // one graph per group layout (served batches, which rarely repeat whole).
+  // phase_sums (not with one_graph): waits for each group and adds its
+  // per-phase device times there (a measurement mode: the host sees every
+  // group boundary).
   void enqueue(const std::vector<ViewSpec> &views, const std::vector<uint64_t> &bases,
                uint64_t total_pixels, const std::vector<ViewGroup> &groups, uint64_t reserve,
-               bool one_graph = false);
+               bool one_graph = false, float *phase_sums = nullptr);
   // Waits, re-runs groups that overflowed their pair buffers and throws on
   // device errors. Returns the reruns.
   uint32_t finish(const std::vector<ViewSpec> &views, const std::vector<uint64_t> &bases,
@@ -160,6 +166,11 @@ class Batch {
   uint32_t blend_mode() { return lane_->pipe().blend_mode(); }
   int device() const { return device_; }
   void set_limits(const GroupLimits &l);
+  // Phase timing: renders run their groups one by one, waiting after each,
+  // and report per-phase device times (BatchResult::phase_ms) in place of
+  // the whole-batch graph.
+  void set_phase_timing(bool on) { phase_timing_ = on; }
+  bool phase_timing() const { return phase_timing_; }
   const GroupLimits &limits() const { return limits_; }
 
   // Renders every view; blocks until all images are in HBM.
@@ -189,6 +200,7 @@ class Batch {
   std::vector<ViewCounters> stats_;
   BatchResult last_;
   bool has_images_ = false;
+  bool phase_timing_ = false;
 };
 
 // Validates batch views against the store and builds pipeline view specs and

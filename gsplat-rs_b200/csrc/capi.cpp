@@ -830,6 +830,27 @@ int32_t gsplat_batch_get_times(const GsplatBatch *batch, GsplatBatchTimes *out_t
   });
 }
 
+int32_t gsplat_batch_set_phase_timing(GsplatBatch *batch, uint32_t on) {
+  return guarded("gsplat_batch_set_phase_timing", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_set_phase_timing");
+    if (on > 1) return fail(Code::InvalidArgument, "gsplat_batch_set_phase_timing: on must be 0 or 1");
+    batch->batch->set_phase_timing(on != 0);
+    return ok();
+  });
+}
+
+int32_t gsplat_batch_get_phase_times(const GsplatBatch *batch, float *out_ms, uint32_t count) {
+  return guarded("gsplat_batch_get_phase_times", [&]() -> int32_t {
+    GSR_BATCH_CHECK("gsplat_batch_get_phase_times");
+    if (!out_ms && count > 0)
+      return fail(Code::InvalidArgument, "gsplat_batch_get_phase_times: out_ms is null");
+    const gsr::BatchResult &r = batch->batch->last();
+    for (uint32_t k = 0; k < count && k < (uint32_t)gsr::kPhaseCount; ++k)
+      out_ms[k] = r.phase_timed ? r.phase_ms[k] : 0.0f;
+    return ok();
+  });
+}
+
 int32_t gsplat_batch_get_view_stats(const GsplatBatch *batch, uint32_t view,
                                     GsplatBatchViewStats *out_stats) {
   return guarded("gsplat_batch_get_view_stats", [&]() -> int32_t {

@@ -31,6 +31,12 @@
 #ifndef GSR_RASTER_PX
 #define GSR_RASTER_PX 2
 #endif
+// Resident blocks per SM the two-pixel FP32 kernel is compiled for: 8
+// blocks of 4 warps fit 64 registers a thread without spills and 27 KB of
+// shared memory a block (256-entry chunks); 10 or 12 spill and run slower.
+#ifndef GSR_RASTER_MIN_BLOCKS
+#define GSR_RASTER_MIN_BLOCKS 8
+#endif
 
 
 namespace gsr {
@@ -305,10 +311,10 @@ struct Fp32Smem {
   static_assert(kPx == 1 || (kPx == 2 && kTile == 16), "two pixels per thread on 16x16 tiles");
   static constexpr int kThreads = kTile * kTile / kPx;
   static constexpr int kWarps = kThreads / 32;
+  // Chunk records as they arrive (a, b, c), overwritten in place by the
+  // per-tile entry data: [0] = ax, ay, ox, thr (coverage bound on r^2);
+  // [1] = bx, by, oy, -; [2] = r, g, b, log2 alpha (the record's c).
   float4 raw[2][3][kChunk];
-  float4 d0[kChunk];  // ax, ay, ox, thr (coverage bound on r^2)
-  float4 d1[kChunk];  // bx, by, oy, -
-  float4 d2[kChunk];  // r, g, b, log2 alpha
   uint8_t mask[kChunk];
   uint16_t list[kWarps][kChunk];
   uint32_t view;
@@ -406,9 +412,8 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
         const float wlim = __fdiv_rn(col.w + 8.0f, 6.49212768f);
         const float thr =
             wlim > 0.0f ? fminf(s2, __int_as_float(__float_as_int(wlim) - 1)) : -1.0f;
-        sm.d0[t] = make_float4(ra.z, ra.w, ox, thr);
-        sm.d1[t] = make_float4(rb.x, rb.y, oy, rb.w);
-        sm.d2[t] = col;
+        sm.raw[buf][0][t] = make_float4(ra.z, ra.w, ox, thr);
+        sm.raw[buf][1][t] = make_float4(rb.x, rb.y, oy, rb.w);
         sm.mask[t] = (uint8_t)ellipse_block_mask<kTile>(ra, rb, thr, cxl, cyl);
       }
     }
@@ -427,10 +432,11 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
     // Branch-free: a pixel that does not take the entry (finished, or not
     // covered) blends with wT = 0, which leaves C and T bit for bit as they
     // are (fma(x, 0, c) = c and T - 0 = T for finite x).
+    const float4 *e0 = sm.raw[buf][0], *e1 = sm.raw[buf][1], *e2 = sm.raw[buf][2];
     auto entry = [&](uint32_t j) {
-      const float4 d0 = at(sm.d0, j);
-      const float4 d1 = at(sm.d1, j);
-      const float4 col = at(sm.d2, j);
+      const float4 d0 = at(e0, j);
+      const float4 d1 = at(e1, j);
+      const float4 col = at(e2, j);
       const float rx = fmaf(d0.y, fy, d0.z), ry = fmaf(d1.y, fy, d1.z);
 #pragma unroll
       for (int p = 0; p < kPx; ++p) {
@@ -475,7 +481,8 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
 // tiles from a global queue (an atomic ticket over the batch's tiles) until
 // it is empty.
 template <int kTile, int kChunk, int kPx, bool kPersistent>
-__global__ void __launch_bounds__(kTile *kTile / kPx) raster_fp32_kernel(RasterArgs a) {
+__global__ void __launch_bounds__(kTile *kTile / kPx, kPx == 2 ? GSR_RASTER_MIN_BLOCKS : 1)
+    raster_fp32_kernel(RasterArgs a) {
   __shared__ Fp32Smem<kTile, kChunk, kPx> sm;
   fold_errors(a);
   if constexpr (!kPersistent) {

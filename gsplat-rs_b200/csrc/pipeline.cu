@@ -730,6 +730,11 @@ void Pipeline::fetch_counters() {
   last_sinks_ = HostSinks{counters_host_, view_counters_pinned_};
 }
 
+void Pipeline::phase_times(float out[kPhaseCount]) const {
+  for (int k = 0; k < kPhaseCount; ++k)
+    GSR_CUDA(cudaEventElapsedTime(&out[k], ev_[k], ev_[k + 1]));
+}
+
 void Pipeline::collect(RunResult &r) {
   float t[kPhaseCount];
   for (int k = 0; k < kPhaseCount; ++k) GSR_CUDA(cudaEventElapsedTime(&t[k], ev_[k], ev_[k + 1]));

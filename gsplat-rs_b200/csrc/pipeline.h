@@ -191,6 +191,9 @@ class Pipeline {
  public:
   // Recorded, in the last enqueued run, just before its raster launch.
   cudaEvent_t raster_start_event() const { return ev_[kPhaseRaster]; }
+  // Phase times of the last run enqueued without batch mode (its stream
+  // must have reached the run's end).
+  void phase_times(float out[kPhaseCount]) const;
 
  private:
   void collect(RunResult &r);

@@ -262,6 +262,9 @@ _SIGS = [
     ("gsplat_batch_render", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.POINTER(GsplatBatchView), ctypes.c_uint32]),
     ("gsplat_batch_get_times", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(GsplatBatchTimes)]),
+    ("gsplat_batch_set_phase_timing", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
+    ("gsplat_batch_get_phase_times", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_uint32]),
     ("gsplat_batch_get_view_stats", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(GsplatBatchViewStats)]),
     ("gsplat_batch_readback_rgba8", ctypes.c_int32,
@@ -620,6 +623,15 @@ class Batch:
         t = GsplatBatchTimes()
         check(lib().gsplat_batch_get_times(self.ptr, ctypes.byref(t)))
         return t
+
+    def set_phase_timing(self, on):
+        check(lib().gsplat_batch_set_phase_timing(self.ptr, 1 if on else 0))
+
+    def phase_times(self):
+        """Per-phase device ms of the last render (zeros unless phase-timed)."""
+        out = (ctypes.c_float * len(Context.PHASES))()
+        check(lib().gsplat_batch_get_phase_times(self.ptr, out, len(out)))
+        return dict(zip(Context.PHASES, [float(x) for x in out]))
 
     def view_stats(self, view):
         s = GsplatBatchViewStats()

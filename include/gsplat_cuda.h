@@ -311,6 +311,16 @@ int32_t gsplat_batch_autotune(GsplatBatch *batch, const GsplatBatchView *views, 
 /* Renders all `count` views and waits until every image is in device memory. */
 int32_t gsplat_batch_render(GsplatBatch *batch, const GsplatBatchView *views, uint32_t count);
 int32_t gsplat_batch_get_times(const GsplatBatch *batch, GsplatBatchTimes *out_times);
+/* Phase timing (off by default): while on, a render runs its launch groups one
+ * after another, waiting after each, in place of the whole-batch graph, and
+ * records per-phase CUDA-event times summed over the groups. A measurement
+ * mode: the images are the same, the device time is not the production one. */
+int32_t gsplat_batch_set_phase_timing(GsplatBatch *batch, uint32_t on);
+/* Per-phase device ms of the last render, in the order preprocess, depth sort,
+ * emission, tile sort, tile ranges, raster; `count` of them (at most 6) are
+ * written. All zero unless that render was phase-timed. Groups re-run after
+ * outgrowing their pair buffers add their first run only. */
+int32_t gsplat_batch_get_phase_times(const GsplatBatch *batch, float *out_ms, uint32_t count);
 int32_t gsplat_batch_get_view_stats(const GsplatBatch *batch, uint32_t view,
                                     GsplatBatchViewStats *out_stats);
 /* RGBA8 image of view `view` of the last render (row 0 = top, tight rows). */

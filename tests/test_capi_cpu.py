@@ -110,6 +110,10 @@ def test_batch_null_and_no_gpu_errors():
     assert "batch is null" in ffi.last_error()
     t = ffi.GsplatBatchTimes()
     assert L.gsplat_batch_get_times(None, ctypes.byref(t)) == 1
+    assert L.gsplat_batch_set_phase_timing(None, 1) == 1
+    ms = (ctypes.c_float * 6)()
+    assert L.gsplat_batch_get_phase_times(None, ms, 6) == 1
+    assert "batch is null" in ffi.last_error()
     out = ctypes.c_void_p(1)
     rc = L.gsplat_batch_create(ctypes.byref(out))
     if rc == 4:

@@ -108,6 +108,37 @@ def test_batch_grouping_and_pair_reruns():
         _check_against_plain(b, scenes, views, tile=8)
 
 
+def test_batch_phase_timing():
+    """Phase-timed renders run group by group and report per-phase device
+    times summed over the groups; the images stay those of the whole-batch
+    graph."""
+    scenes = _scenes()
+    views = _views(np.random.default_rng(31), 9, len(scenes))
+    with ffi.Batch() as b:
+        for s in scenes:
+            b.add_scene(s)
+        b.set_limits(max_views=4)
+        b.render(views)
+        t = b.render(views)
+        assert t.groups == 3 and t.graph_launches == 1
+        assert all(v == 0.0 for v in b.phase_times().values())
+        ref = [b.readback_rgba8(k).copy() for k in range(len(views))]
+        b.set_phase_timing(True)
+        b.render(views)
+        t = b.render(views)
+        assert t.graph_launches == 0
+        ph = b.phase_times()
+        assert list(ph) == ["preprocess", "depth_sort", "emit", "tile_sort", "ranges", "raster"]
+        assert all(v > 0.0 for v in ph.values()), ph
+        assert sum(ph.values()) <= t.device_ms * 1.01 + 0.05
+        for k in range(len(views)):
+            assert np.array_equal(b.readback_rgba8(k), ref[k]), f"view {k}"
+        b.set_phase_timing(False)
+        t = b.render(views)
+        assert t.graph_launches == 1
+        assert all(v == 0.0 for v in b.phase_times().values())
+
+
 @pytest.mark.parametrize("tile,blend", [(8, 0), (16, 1)])
 def test_batch_tile_size_and_blend_mode(oracle, tile, blend):
     scenes = _scenes()
