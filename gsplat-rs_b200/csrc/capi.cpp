@@ -558,6 +558,17 @@ int32_t gsplat_context_debug_projected(GsplatContext *ctx, GsplatProjectedSplat 
   });
 }
 
+int32_t gsplat_context_debug_coverage(GsplatContext *ctx, float *out, uint64_t capacity,
+                                      uint64_t *out_len) {
+  return guarded("gsplat_context_debug_coverage", [&]() -> int32_t {
+    if (!ctx || !out_len) return fail(Code::InvalidArgument, "gsplat_context_debug_coverage: null argument");
+    auto v = ctx->renderer->debug_coverage();
+    *out_len = v.size();
+    if (out) std::memcpy(out, v.data(), sizeof(float2) * std::min<uint64_t>(capacity, v.size()));
+    return ok();
+  });
+}
+
 int32_t gsplat_context_debug_tile_pairs(GsplatContext *ctx, uint32_t *tiles, uint32_t *ids,
                                         uint64_t capacity, uint64_t *out_len) {
   return guarded("gsplat_context_debug_tile_pairs", [&]() -> int32_t {

@@ -414,6 +414,9 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
             wlim > 0.0f ? fminf(s2, __int_as_float(__float_as_int(wlim) - 1)) : -1.0f;
         sm.raw[buf][0][t] = make_float4(ra.z, ra.w, ox, thr);
         sm.raw[buf][1][t] = make_float4(rb.x, rb.y, oy, rb.w);
+        // debug tap: the inputs and the bound this kernel blends with (every
+        // tile of a splat writes the same pair)
+        if (a.debug_cov) a.debug_cov[ids[range.y - 1 - (c * kChunk + t)]] = make_float2(col.w, thr);
         sm.mask[t] = (uint8_t)ellipse_block_mask<kTile>(ra, rb, thr, cxl, cyl);
       }
     }

@@ -109,6 +109,7 @@ struct RasterArgs {
   uint32_t *images;
   FrameCounters *counters;         // raster_ticket is the persistent tile queue
   uint32_t *sticky;
+  float2 *debug_cov = nullptr;     // debug tap: (log2 alpha, coverage bound) per splat slot
 };
 // Raster launch shape: records staged per step (tile 16: 64/128/256; tile 8:
 // 32/64) and persistent blocks per SM pulling tiles from a global queue

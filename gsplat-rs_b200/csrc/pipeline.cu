@@ -299,6 +299,7 @@ void Pipeline::ensure_workspace(const Layout &l) {
       depth_sort_work_ = splat_ws_.as<uint32_t>(o_work);
       splat_cap_ = ncap;
       projected_.reset(0);
+      debug_cov_.reset(0);
     }
     note_regrowth(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() -
                                                             t_grow).count());
@@ -322,6 +323,11 @@ void Pipeline::ensure_workspace(const Layout &l) {
       GSR_CUDA(cudaStreamSynchronize(stream_));
       drop_graph();
       projected_.reset(need);
+    }
+    if (debug_cov_.size() < 8ull * splat_cap_) {
+      GSR_CUDA(cudaStreamSynchronize(stream_));
+      drop_graph();
+      debug_cov_.reset(8ull * splat_cap_);
     }
     if (debug_pairs_.size() < 8 * key_cap_) {
       GSR_CUDA(cudaStreamSynchronize(stream_));
@@ -428,6 +434,11 @@ void Pipeline::launch_all(const Layout &l, uint32_t *images, const HostSinks &si
   record(5);
   RasterArgs ra{views_dev,  l.views,  l.total_tiles, ranges_,   tile_plan_,
                 tile_vals0_, tile_vals1_, records_,  images, counters_, sticky_};
+  if (debug_) {
+    GSR_CUDA(cudaMemsetAsync(debug_cov_.get(), 0xff, 8ull * std::max<uint32_t>(l.total_splats, 1),
+                             stream_));
+    ra.debug_cov = debug_cov_.as<float2>();
+  }
   launch_raster(ra, tile_, blend_mode_, raster_cfg_, sm_count_, stream_);
   record(6);
   // Runs with host sinks copy their counters there; the others leave them in
@@ -830,6 +841,17 @@ std::vector<ProjectedDev> Pipeline::debug_projected(uint32_t count) {
   std::vector<ProjectedDev> out(count);
   if (count)
     GSR_CUDA(cudaMemcpy(out.data(), projected_.get(), sizeof(ProjectedDev) * count,
+                        cudaMemcpyDeviceToHost));
+  return out;
+}
+
+std::vector<float2> Pipeline::debug_coverage(uint32_t count) {
+  if (!debug_ || !debug_cov_.get())
+    throw Error(Code::InvalidArgument, "debug taps were not enabled for the last frame");
+  GSR_CUDA(cudaSetDevice(device_));
+  std::vector<float2> out(count);
+  if (count)
+    GSR_CUDA(cudaMemcpy(out.data(), debug_cov_.get(), sizeof(float2) * count,
                         cudaMemcpyDeviceToHost));
   return out;
 }

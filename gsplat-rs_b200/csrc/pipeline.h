@@ -167,6 +167,9 @@ class Pipeline {
   // Debug taps of the last run (valid until the next run).
   std::vector<uint32_t> debug_order();
   std::vector<ProjectedDev> debug_projected(uint32_t count);
+  // (log2 alpha, coverage bound) the FP32 raster used per splat slot; NaN for
+  // splats in no tile list (or frames in the UNORM8 mode).
+  std::vector<float2> debug_coverage(uint32_t count);
   void debug_tile_pairs(std::vector<uint32_t> &tiles, std::vector<uint32_t> &ids);
   void debug_tile_ranges(uint32_t num_tiles, std::vector<uint32_t> &ranges,
                          std::vector<uint32_t> &ids);
@@ -269,6 +272,7 @@ class Pipeline {
   uint32_t *tile_keys0_ = nullptr, *tile_vals0_ = nullptr, *tile_keys1_ = nullptr,
            *tile_vals1_ = nullptr, *tile_sort_work_ = nullptr;
   DeviceBuffer debug_pairs_;
+  DeviceBuffer debug_cov_;
   ViewCounters *view_counters_pinned_ = nullptr;
   uint32_t view_counters_pinned_cap_ = 0;
   // Pinned staging ring for the view table: slot s is rewritten only after

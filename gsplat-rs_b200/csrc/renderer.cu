@@ -360,6 +360,11 @@ std::vector<ProjectedDev> Renderer::debug_projected() {
   return front_pipe().debug_projected(scene_->n);
 }
 
+std::vector<float2> Renderer::debug_coverage() {
+  if (!has_frame_) throw Error(Code::InvalidArgument, "debug taps were not enabled for the last frame");
+  return front_pipe().debug_coverage(scene_->n);
+}
+
 void Renderer::debug_tile_pairs(std::vector<uint32_t> &tiles, std::vector<uint32_t> &ids) {
   if (!has_frame_) throw Error(Code::InvalidArgument, "debug taps were not enabled for the last frame");
   front_pipe().debug_tile_pairs(tiles, ids);

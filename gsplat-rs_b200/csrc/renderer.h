@@ -92,6 +92,7 @@ class Renderer {
   void readback_rgba8_async(uint8_t *out, uint64_t len);
   std::vector<uint32_t> debug_order();
   std::vector<ProjectedDev> debug_projected();
+  std::vector<float2> debug_coverage();
   void debug_tile_pairs(std::vector<uint32_t> &tiles, std::vector<uint32_t> &ids);
   void debug_tile_ranges(std::vector<uint32_t> &ranges, std::vector<uint32_t> &ids);
 

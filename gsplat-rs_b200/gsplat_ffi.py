@@ -233,6 +233,8 @@ _SIGS = [
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32)]),
     ("gsplat_server_add_scene_packed", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32)]),
+    ("gsplat_context_debug_coverage", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
     ("gsplat_context_debug_projected", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
     ("gsplat_context_debug_tile_pairs", ctypes.c_int32,
@@ -514,6 +516,16 @@ class Context:
         out = np.zeros(max(n.value, 1), PROJECTED_DTYPE)
         check(lib().gsplat_context_debug_projected(self.ptr, out.ctypes.data, n.value,
                                                    ctypes.byref(n)))
+        return out[:n.value]
+
+    def debug_coverage(self):
+        """(n, 2) float32: log2 alpha and the coverage bound the FP32 raster
+        used per splat (NaN for splats in no tile list)."""
+        n = ctypes.c_uint64()
+        check(lib().gsplat_context_debug_coverage(self.ptr, None, 0, ctypes.byref(n)))
+        out = np.zeros((max(n.value, 1), 2), np.float32)
+        check(lib().gsplat_context_debug_coverage(self.ptr, out.ctypes.data, n.value,
+                                                  ctypes.byref(n)))
         return out[:n.value]
 
     def debug_tile_pairs(self):

@@ -172,6 +172,13 @@ int32_t gsplat_context_debug_order(GsplatContext *ctx, uint32_t *out, uint64_t c
 /* Per splat id (needs gsplat_context_set_debug_taps(ctx, 1) before the frame). */
 int32_t gsplat_context_debug_projected(GsplatContext *ctx, GsplatProjectedSplat *out,
                                        uint64_t capacity, uint64_t *out_len);
+/* Per splat id, two floats: the log2(alpha) and the coverage bound on r^2
+ * (the largest float below (log2 alpha + 8) / (4.5 log2 e), capped at s^2;
+ * -1 when that bound is not positive) the FP32 raster blended the splat with;
+ * NaN for splats in no tile list and for UNORM8-mode frames. `capacity` and
+ * `out_len` count splats. */
+int32_t gsplat_context_debug_coverage(GsplatContext *ctx, float *out, uint64_t capacity,
+                                      uint64_t *out_len);
 /* (tile, splat id) pairs in emission order (depth order, rect rows outer). */
 int32_t gsplat_context_debug_tile_pairs(GsplatContext *ctx, uint32_t *tiles, uint32_t *ids,
                                         uint64_t capacity, uint64_t *out_len);

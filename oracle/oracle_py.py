@@ -414,6 +414,22 @@ def render_reference_frame(sv, cam, width, height, threads=8, rows=0):
     return out.reshape(height, width, 4), t
 
 
+def coverage_bound(s, log2a):
+    """FP32-mode coverage bound on r^2 per splat, in float32 (each operation
+    rounded like the tile model in oracle_render.cpp, orc_raster_tiles_fp32):
+    the reference's fragment rule (crates/gsplat-render-wgpu/shaders/
+    splat_surface_direct.wgsl:336-369) keeps w = alpha e^(-4.5 r^2) > 1/256
+    and |local| <= s, i.e. r^2 < (log2 alpha + 8) / (4.5 log2 e) and
+    r^2 <= s^2; the bound is the largest float below the first, capped at the
+    second, and -1 when the first is not positive."""
+    s = np.asarray(s, np.float32)
+    log2a = np.asarray(log2a, np.float32)
+    s2 = s * s
+    wlim = (log2a + np.float32(8.0)) / np.float32(6.49212768)
+    below = np.nextafter(wlim, np.float32(0.0))
+    return np.where(wlim > np.float32(0.0), np.fmin(s2, below), np.float32(-1.0)).astype(np.float32)
+
+
 def exp_neg(x):
     return lib().orc_exp_neg(float(x))
 

@@ -106,6 +106,38 @@ def test_frame_parity_stages_and_images(oracle, cfg):
     ctx.close()
 
 
+@pytest.mark.parametrize("cfg", ["config1", "config2_small"])
+def test_raster_coverage_bound_tap(oracle, cfg):
+    """The FP32 raster's own per-splat coverage bound, read through the debug
+    tap, equals the oracle's bound of the same inputs bit for bit; its
+    log2 alpha (the hardware logarithm) is within 4e-6 of numpy's; only splats
+    in some tile list carry a value (not all of them: a tile stops staging
+    chunks once every pixel is opaque)."""
+    if cfg == "config1":
+        scene, cam, w, h = gsplat_scenes.config1(seed=0)
+    else:
+        scene, cam, w, h = gsplat_scenes.config2(seed=11, n=40000)
+        w, h = 960, 540
+    ctx = _render(scene, cam, w, h, blend=0)
+    cov = ctx.debug_coverage()
+    proj = ctx.debug_projected()
+    _, ids = ctx.debug_tile_pairs()
+    listed = np.zeros(len(cov), bool)
+    listed[np.unique(ids)] = True
+    has = ~np.isnan(cov[:, 1])
+    assert not (has & ~listed).any()
+    assert has.sum() > 0.5 * listed.sum() and has.sum() > 100
+    want = oracle.coverage_bound(proj["extent_scale"][has], cov[has, 0])
+    assert np.array_equal(cov[has, 1].view(np.uint32), want.view(np.uint32))
+    alpha = proj["color"][has, 3].astype(np.float64)
+    assert np.abs(cov[has, 0] - np.log2(alpha)).max() <= 4e-6
+    # the UNORM8 mode leaves the tap empty
+    ctx.set_blend_mode(1)
+    ctx.render_frame()
+    assert np.isnan(ctx.debug_coverage()[:, 1]).all()
+    ctx.close()
+
+
 def test_full_config2_parity(oracle):
     """279,199 splats, SH3, 1920x1080: every stage bit-exact at full size (the
     FP32 image within its tolerance)."""
