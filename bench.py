@@ -57,7 +57,11 @@ FALLBACK_HBM_GBS = 6650.0
 # the command): DRAM bytes read + written, warp instructions issued, and
 # executed FP32 thread operations (2 x FFMA + FADD + FMUL). None until
 # captured for the current kernel.
-NCU_RASTER = {"dram_bytes": 18_312_448, "warp_inst": 119_637_791,
+# thread_flop: FP32 operations of one launch from the scalar build of the
+# same arithmetic (-D GSR_RASTER_F32X2=0; ncu's per-op counters do not count
+# the paired f32x2 instructions of the default build, which performs exactly
+# the same operations).
+NCU_RASTER = {"dram_bytes": 18_311_168, "warp_inst": 95_671_016,
               "thread_flop": 2 * 1_223_868_317 + 202_085_090 + 375_960_460,
               "source": "profiles/frame_279k_sh3_1080p.md (ncu --set full, one launch)"}
 

@@ -176,10 +176,14 @@ __device__ __forceinline__ float exp_neg(float x) {
 // polynomial instead; the two images agree to the last UNORM8 step except
 // where a weight sits on the 1/256 threshold or a channel on a rounding
 // boundary.
-__device__ __forceinline__ float blend_weight(float r2, float log2_alpha) {
+__device__ __forceinline__ float ex2_approx(float x) {
   float w;
-  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(w) : "f"(fmaf(r2, -6.49212768f, log2_alpha)));
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(w) : "f"(x));
   return w;
+}
+
+__device__ __forceinline__ float blend_weight(float r2, float log2_alpha) {
+  return ex2_approx(fmaf(r2, -6.49212768f, log2_alpha));
 }
 
 __device__ __forceinline__ uint32_t to_unorm8(float x) {

@@ -31,6 +31,10 @@
 #ifndef GSR_RASTER_PX
 #define GSR_RASTER_PX 2
 #endif
+// Paired FP32 arithmetic for the two pixels of a thread (f32x2).
+#ifndef GSR_RASTER_F32X2
+#define GSR_RASTER_F32X2 1
+#endif
 // Resident blocks per SM the two-pixel FP32 kernel is compiled for: 8
 // blocks of 4 warps fit 64 registers a thread without spills and 27 KB of
 // shared memory a block (256-entry chunks); 10 or 12 spill and run slower.
@@ -441,19 +445,45 @@ __device__ __forceinline__ void raster_fp32_tile(const RasterArgs &a, uint32_t t
       const float4 d1 = at(e1, j);
       const float4 col = at(e2, j);
       const float rx = fmaf(d0.y, fy, d0.z), ry = fmaf(d1.y, fy, d1.z);
+      if constexpr (kPx == 2 && GSR_RASTER_F32X2) {
+        // The two pixels' arithmetic as paired FP32 instructions (sm_100
+        // f32x2: each component rounds exactly as the scalar operation, and
+        // T - wT is fma(wT, -1, T), the same single rounding).
+        const float2 fxp = make_float2(fx[0], fx[1]);
+        const float2 lx = __ffma2_rn(make_float2(d0.x, d0.x), fxp, make_float2(rx, rx));
+        const float2 ly = __ffma2_rn(make_float2(d1.x, d1.x), fxp, make_float2(ry, ry));
+        const float2 r2 = __ffma2_rn(lx, lx, __fmul2_rn(ly, ly));
+        const float2 arg =
+            __ffma2_rn(r2, make_float2(-6.49212768f, -6.49212768f), make_float2(col.w, col.w));
+        const float2 wt = __fmul2_rn(make_float2(ex2_approx(arg.x), ex2_approx(arg.y)),
+                                     make_float2(T[0], T[1]));
+        const bool take0 = !done[0] && r2.x <= d0.w, take1 = !done[1] && r2.y <= d0.w;
+        const float2 wT = make_float2(take0 ? wt.x : 0.0f, take1 ? wt.y : 0.0f);
+        const float2 n0 = __ffma2_rn(make_float2(col.x, col.x), wT, make_float2(c0[0], c0[1]));
+        const float2 n1 = __ffma2_rn(make_float2(col.y, col.y), wT, make_float2(c1[0], c1[1]));
+        const float2 n2 = __ffma2_rn(make_float2(col.z, col.z), wT, make_float2(c2[0], c2[1]));
+        const float2 nt = __ffma2_rn(wT, make_float2(-1.0f, -1.0f), make_float2(T[0], T[1]));
+        c0[0] = n0.x, c0[1] = n0.y;
+        c1[0] = n1.x, c1[1] = n1.y;
+        c2[0] = n2.x, c2[1] = n2.y;
+        T[0] = nt.x, T[1] = nt.y;
+        done[0] = done[0] || T[0] < 1e-4f;
+        done[1] = done[1] || T[1] < 1e-4f;
+      } else {
 #pragma unroll
-      for (int p = 0; p < kPx; ++p) {
-        const float lx = fmaf(d0.x, fx[p], rx);
-        const float ly = fmaf(d1.x, fx[p], ry);
-        const float r2 = fmaf(lx, lx, ly * ly);
-        const bool take = !done[p] && r2 <= d0.w;
-        const float w = blend_weight(r2, col.w);
-        const float wT = take ? w * T[p] : 0.0f;
-        c0[p] = fmaf(col.x, wT, c0[p]);
-        c1[p] = fmaf(col.y, wT, c1[p]);
-        c2[p] = fmaf(col.z, wT, c2[p]);
-        T[p] = T[p] - wT;
-        done[p] = done[p] || T[p] < 1e-4f;
+        for (int p = 0; p < kPx; ++p) {
+          const float lx = fmaf(d0.x, fx[p], rx);
+          const float ly = fmaf(d1.x, fx[p], ry);
+          const float r2 = fmaf(lx, lx, ly * ly);
+          const bool take = !done[p] && r2 <= d0.w;
+          const float w = blend_weight(r2, col.w);
+          const float wT = take ? w * T[p] : 0.0f;
+          c0[p] = fmaf(col.x, wT, c0[p]);
+          c1[p] = fmaf(col.y, wT, c1[p]);
+          c2[p] = fmaf(col.z, wT, c2[p]);
+          T[p] = T[p] - wT;
+          done[p] = done[p] || T[p] < 1e-4f;
+        }
       }
     };
     uint32_t i = 0;
