@@ -1148,7 +1148,7 @@ def main():
     ap.add_argument("--no-ingest", action="store_true")
     ap.add_argument("--no-packed", action="store_true")
     ap.add_argument("--no-config3", action="store_true")
-    ap.add_argument("--frame-lanes", type=int, default=3,
+    ap.add_argument("--frame-lanes", type=int, default=8,
                     help="frame lanes of the e2e loop (gsplat_context_set_frame_lanes)")
     ap.add_argument("--ingest-splats", type=int, default=279_199,
                     help="splats of the PLY ingestion workload")

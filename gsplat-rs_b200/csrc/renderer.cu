@@ -69,7 +69,7 @@ void Renderer::sync_all_lanes() {
 // smaller than the frames it will take over).
 void Renderer::set_frame_lanes(uint32_t lanes) {
   if (lanes < 1 || lanes > kMaxLanes)
-    throw Error(Code::InvalidArgument, "frame lanes must be 1 to 4");
+    throw Error(Code::InvalidArgument, "frame lanes must be 1 to 8");
   GSR_CUDA(cudaSetDevice(device_));
   if (deferred_.pending) issue_copy(false);
   sync_all_lanes();

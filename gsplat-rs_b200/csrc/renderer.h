@@ -46,7 +46,7 @@ class Renderer {
   // independent and each image is exactly the single-lane image. A sort
   // interval other than 0 runs on one lane (its reused order lives in that
   // lane's workspace).
-  static constexpr uint32_t kMaxLanes = 4;
+  static constexpr uint32_t kMaxLanes = 8;
   void set_frame_lanes(uint32_t lanes);
   uint32_t frame_lanes() const { return lane_count_; }
   // Depth-order refresh cadence. 0 (the default): every frame sorts, as the

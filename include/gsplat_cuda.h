@@ -111,7 +111,7 @@ int32_t gsplat_context_set_raster_config(GsplatContext *ctx, uint32_t chunk, uin
  * order, in that order (stale-order frames, as in the reference). */
 int32_t gsplat_context_set_sort_interval(GsplatContext *ctx, uint32_t interval);
 
-/* No counterpart in the reference: frame lanes (1 to 4, default 1).
+/* No counterpart in the reference: frame lanes (1 to 8, default 1).
  * Frames enqueued with gsplat_context_render_frame_async rotate over `lanes`
  * independent pipelines, each on its own CUDA stream with its own workspace
  * and image, so consecutive frames overlap on the device (one frame's sorts

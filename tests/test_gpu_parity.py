@@ -651,7 +651,7 @@ def test_async_readback_pipeline_equals_synchronous_frames():
         assert np.array_equal(ctx.readback_rgba8().reshape(-1), big)
 
 
-@pytest.mark.parametrize("lanes", [2, 3, 4])
+@pytest.mark.parametrize("lanes", [2, 3, 4, 8])
 def test_frame_lanes_equal_single_lane_frames(lanes):
     """Frames that overlap on the device over `lanes` pipelines (one stream,
     workspace and image each) give, frame by frame, the single-lane images:
