@@ -546,7 +546,7 @@ def _spin_until(t):
             time.sleep(d - 0.001)
 
 
-def measure_served(ffi, rates, seconds, max_requests):
+def measure_served(ffi, rates, seconds, max_requests, lanes=2):
     """Served stream: 8 resident scenes (sizes log-uniform in [50k, 3M], SH
     degree 0-3 mixed), Poisson arrivals at each offered rate, each request a
     random scene, orbit camera and resolution from {512^2, 720p, 1080p}.
@@ -565,11 +565,12 @@ def measure_served(ffi, rates, seconds, max_requests):
     # overload the requests that run keep a bounded queueing delay
     max_queue_ms = 50
     try:
-        srv = ffi.Server(lanes=2, max_views=256, work_budget=64 << 30, result_pool_mib=reserve_mib,
-                         max_queue_ms=max_queue_ms)
+        srv = ffi.Server(lanes=lanes, max_views=256, work_budget=64 << 30,
+                         result_pool_mib=reserve_mib, max_queue_ms=max_queue_ms)
     except ffi.GsplatError:
         reserve_mib = 0
-        srv = ffi.Server(lanes=2, max_views=256, work_budget=64 << 30, max_queue_ms=max_queue_ms)
+        srv = ffi.Server(lanes=lanes, max_views=256, work_budget=64 << 30,
+                         max_queue_ms=max_queue_ms)
     for sc in scenes:
         srv.add_scene(sc)
     # The plain call gets its best case: one context per (scene, size), so no
@@ -673,7 +674,7 @@ def measure_served(ffi, rates, seconds, max_requests):
         c.close()
     return {"workload": "8 resident scenes, sizes log-uniform in [50k, 3M] splats, SH degree 0-3 "
                         "mixed; Poisson arrivals; each request a random scene, orbit camera and "
-                        "resolution from 512^2/720p/1080p; 2 lanes, <=256 views per batch, "
+                        f"resolution from 512^2/720p/1080p; {lanes} lanes, <=256 views per batch, "
                         "64 GiB work budget",
             "result_pool_mib": reserve_mib, "max_queue_ms": max_queue_ms,
             "latency": "submit -> RGBA8 image in pinned host memory (host clock)",
@@ -903,7 +904,7 @@ def run_sections_only(args, ffi, torch):
                                          args.cameras_per_scene)
     if "served" in args.only:
         out["served"] = measure_served(ffi, [float(x) for x in args.serve_rates.split(",")],
-                                       args.serve_seconds, 4000)
+                                       args.serve_seconds, 4000, args.serve_lanes)
     if "ingest" in args.only:
         out["ingest"] = measure_ingest(ffi, args.ingest_splats)
     if "packed" in args.only:
@@ -1115,7 +1116,7 @@ def run_cuda(args, world, rank, local):
         line["batched"] = measure_batched(ffi, torch, args.batch_steps, 2)
     if not args.no_served and world == 1:
         line["served"] = measure_served(ffi, [float(x) for x in args.serve_rates.split(",")],
-                                        args.serve_seconds, 4000)
+                                        args.serve_seconds, 4000, args.serve_lanes)
     if not args.no_ingest and world == 1:
         line["ingest"] = measure_ingest(ffi, args.ingest_splats)
     if not args.no_packed and world == 1:
@@ -1143,6 +1144,8 @@ def main():
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--serve-rates", default="500,2000,8000,20000")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
+    ap.add_argument("--serve-lanes", type=int, default=2,
+                    help="server lanes (gsplat_server_create's lanes)")
     ap.add_argument("--artifact", default="",
                     help="also write the plain frames as a v1 benchmark artifact into this folder")
     ap.add_argument("--no-ingest", action="store_true")
