@@ -546,6 +546,12 @@ def _spin_until(t):
             time.sleep(d - 0.001)
 
 
+# Pipeline workspace the served section's lanes may admit per batch (over all
+# lanes): batches stay a few dozen views, and the warm-up's extreme bursts take
+# every lane to its largest workspace before any rate is timed.
+SERVE_WORK_BUDGET = 16 << 30
+
+
 def measure_served(ffi, rates, seconds, max_requests, lanes=2):
     """Served stream: 8 resident scenes (sizes log-uniform in [50k, 3M], SH
     degree 0-3 mixed), Poisson arrivals at each offered rate, each request a
@@ -565,11 +571,11 @@ def measure_served(ffi, rates, seconds, max_requests, lanes=2):
     # overload the requests that run keep a bounded queueing delay
     max_queue_ms = 50
     try:
-        srv = ffi.Server(lanes=lanes, max_views=256, work_budget=64 << 30,
+        srv = ffi.Server(lanes=lanes, max_views=256, work_budget=SERVE_WORK_BUDGET,
                          result_pool_mib=reserve_mib, max_queue_ms=max_queue_ms)
     except ffi.GsplatError:
         reserve_mib = 0
-        srv = ffi.Server(lanes=lanes, max_views=256, work_budget=64 << 30,
+        srv = ffi.Server(lanes=lanes, max_views=256, work_budget=SERVE_WORK_BUDGET,
                          max_queue_ms=max_queue_ms)
     for sc in scenes:
         srv.add_scene(sc)
@@ -596,6 +602,22 @@ def measure_served(ffi, rates, seconds, max_requests, lanes=2):
         for rid in warm:
             srv.wait(rid)
             srv.release(rid)
+    # Then the extremes an overloaded queue can hand a lane, twice each (the
+    # lanes take batches in turn): full batches of the largest scene at
+    # 1080p (splats, pairs), of the smallest at 1080p (tiles) and of the
+    # largest at 512^2 (splats per pixel), so no workspace has to grow while
+    # a rate is timed (growing maps gigabytes of device memory in the middle
+    # of the request stream).
+    sizes = [int(s["positions"].shape[0]) for s in scenes]
+    big, small = sizes.index(max(sizes)), sizes.index(min(sizes))
+    rng = np.random.default_rng(905)
+    for sid, (w, h) in ((big, (1920, 1080)), (small, (1920, 1080)), (big, (512, 512))):
+        for _ in range(2):
+            warm = [srv.submit(sid, gsplat_scenes.orbit_camera(rng), w, h)
+                    for _ in range(256)]
+            for rid in warm:
+                srv.wait(rid)
+                srv.release(rid)
     # ... and single requests, one at a time, four times for every (scene,
     # size): a light load runs one-view batches, whose launch graphs a lane
     # captures on a layout's second run on that lane (a capture takes about
@@ -675,7 +697,7 @@ def measure_served(ffi, rates, seconds, max_requests, lanes=2):
     return {"workload": "8 resident scenes, sizes log-uniform in [50k, 3M] splats, SH degree 0-3 "
                         "mixed; Poisson arrivals; each request a random scene, orbit camera and "
                         f"resolution from 512^2/720p/1080p; {lanes} lanes, <=256 views per batch, "
-                        "64 GiB work budget",
+                        "16 GiB work budget",
             "result_pool_mib": reserve_mib, "max_queue_ms": max_queue_ms,
             "latency": "submit -> RGBA8 image in pinned host memory (host clock)",
             "rates": out}

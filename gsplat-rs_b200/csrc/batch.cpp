@@ -155,6 +155,10 @@ Lane::Lane(int device) : device_(device) {
   GSR_CUDA(cudaEventCreate(&start_));
   GSR_CUDA(cudaEventCreate(&end_));
   pipe_ = std::make_unique<Pipeline>(device_, stream_);
+  // pinned once for a full launch of views (growing them later frees pinned
+  // memory, which waits for the whole device)
+  view_counters_.ensure(kMaxViewsPerLaunch);
+  group_counters_.ensure(kMaxViewsPerLaunch);
 }
 
 Lane::~Lane() {
@@ -175,7 +179,7 @@ void Lane::enqueue(const std::vector<ViewSpec> &views, const std::vector<uint64_
   if (images_.size() < need) {
     const auto t_grow = std::chrono::steady_clock::now();
     GSR_CUDA(cudaStreamSynchronize(stream_));
-    images_.reset(need + need / 4);
+    images_.reset(need + need / 4, stream_);  // stream order: no device-wide wait
     pipe_->note_regrowth(std::chrono::duration<double, std::milli>(
                              std::chrono::steady_clock::now() - t_grow).count());
   }

@@ -18,16 +18,36 @@ constexpr uint64_t kMaxSortItems = (1u << 30) - 1;
 constexpr uint64_t kInitialPairsPerSplat = 16;
 }  // namespace
 
-DeviceBuffer::~DeviceBuffer() {
-  if (ptr_) cudaFree(ptr_);
+DeviceBuffer::~DeviceBuffer() { release(); }
+
+void DeviceBuffer::release() {
+  if (ptr_) {
+    if (ordered_) cudaFreeAsync(ptr_, stream_);
+    else cudaFree(ptr_);
+  }
+  ptr_ = nullptr;
+  bytes_ = 0;
+  ordered_ = false;
+  stream_ = nullptr;
+}
+
+void DeviceBuffer::reset(uint64_t bytes, cudaStream_t stream) {
+  release();
+  if (bytes == 0) return;
+  cudaError_t e = cudaMallocAsync(&ptr_, bytes, stream);
+  if (e != cudaSuccess) {
+    ptr_ = nullptr;
+    cudaGetLastError();
+    throw Error(Code::Internal, "device allocation of " + std::to_string(bytes) +
+                                    " bytes failed: " + cudaGetErrorString(e));
+  }
+  bytes_ = bytes;
+  stream_ = stream;
+  ordered_ = true;
 }
 
 void DeviceBuffer::reset(uint64_t bytes) {
-  if (ptr_) {
-    cudaFree(ptr_);
-    ptr_ = nullptr;
-    bytes_ = 0;
-  }
+  release();
   if (bytes == 0) return;
   cudaError_t e = cudaMalloc(&ptr_, bytes);
   if (e != cudaSuccess) {
@@ -252,28 +272,27 @@ void Pipeline::ensure_workspace(const Layout &l) {
     const uint64_t o_k1 = off; off += align256(8 * k1_total);
     const uint64_t o_em = off; off += align256(8 * emit_words);
     view_zero_bytes_ = off;
-    // the table: view sets, then views (one host-to-device copy per run)
-    const uint64_t o_sets = off; off += align256(sizeof(ViewSetDev) * vcap);
+    // the table: view sets, then views (one host-to-device copy per run);
+    // the sets region is sized for the largest launch, so the table's layout
+    // (and the pinned staging slots that mirror it) never changes
+    const uint64_t o_sets = off; off += align256(sizeof(ViewSetDev) * kMaxViewsPerLaunch);
     const uint64_t o_tab = off; off += align256(sizeof(ViewDev) * vcap);
-    view_ws_.reset(off);
+    view_ws_.reset(off, stream_);
     sets_dev_ = view_ws_.as<ViewSetDev>(o_sets);
     view_counters_ = view_ws_.as<ViewCounters>(o_vc);
     k1_status_ = view_ws_.as<unsigned long long>(o_k1);
     emit_status_ = view_ws_.as<unsigned long long>(o_em);
     views_dev_ = view_ws_.as<ViewDev>(o_tab);
     view_cap_ = vcap;
-    // a staging slot has the device table's layout (sets, then views at o_tab)
-    const uint64_t slot_bytes = off - o_sets;
-    if (view_counters_pinned_cap_ < vcap || table_slot_bytes_ != slot_bytes) {
-      // in-flight runs may still read or write the pinned host arrays
-      GSR_CUDA(cudaStreamSynchronize(stream_));
-      if (view_counters_pinned_) cudaFreeHost(view_counters_pinned_);
-      if (table_pinned_) cudaFreeHost(table_pinned_);
-      view_counters_pinned_ = nullptr;
-      table_pinned_ = nullptr;
-      GSR_CUDA(cudaMallocHost(&view_counters_pinned_, sizeof(ViewCounters) * vcap));
+    // A staging slot has the device table's layout (sets, then views at
+    // o_tab). The pinned host arrays are pinned once, for the largest launch
+    // (freeing pinned memory waits for the whole device, which would stall
+    // a growing lane behind every other stream's work).
+    if (!table_pinned_) {
+      const uint64_t slot_bytes = (o_tab - o_sets) + align256(sizeof(ViewDev) * kMaxViewsPerLaunch);
+      GSR_CUDA(cudaMallocHost(&view_counters_pinned_, sizeof(ViewCounters) * kMaxViewsPerLaunch));
       GSR_CUDA(cudaMallocHost((void **)&table_pinned_, slot_bytes * kViewSlots));
-      view_counters_pinned_cap_ = vcap;
+      view_counters_pinned_cap_ = kMaxViewsPerLaunch;
       table_slot_bytes_ = slot_bytes;
     }
     table_sets_bytes_ = o_tab - o_sets;
@@ -287,8 +306,7 @@ void Pipeline::ensure_workspace(const Layout &l) {
       uint64_t o_rect = off; off += align256(8ull * ncap);
       uint64_t o_rec = off; off += align256(sizeof(Record) * (uint64_t)ncap);
       uint64_t o_work = off; off += align256(4 * words);
-      splat_ws_.reset(0);
-      splat_ws_.reset(off);
+      splat_ws_.reset(off, stream_);
       sorted_valid_ = false;  // the sorted ids lived in the old buffers
       vis_keys0_ = splat_ws_.as<uint32_t>(o_k0);
       vis_vals0_ = splat_ws_.as<uint32_t>(o_v0);
@@ -298,8 +316,8 @@ void Pipeline::ensure_workspace(const Layout &l) {
       records_ = splat_ws_.as<Record>(o_rec);
       depth_sort_work_ = splat_ws_.as<uint32_t>(o_work);
       splat_cap_ = ncap;
-      projected_.reset(0);
-      debug_cov_.reset(0);
+      projected_.reset(0, stream_);
+      debug_cov_.reset(0, stream_);
     }
     note_regrowth(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() -
                                                             t_grow).count());
@@ -309,7 +327,7 @@ void Pipeline::ensure_workspace(const Layout &l) {
     GSR_CUDA(cudaStreamSynchronize(stream_));
     drop_graph();
     tile_cap_ = std::max(l.total_tiles, tile_cap_ + tile_cap_ / 2);
-    tile_ws_.reset(align256(8ull * std::max<uint32_t>(tile_cap_, 1)));
+    tile_ws_.reset(align256(8ull * std::max<uint32_t>(tile_cap_, 1)), stream_);
     ranges_ = tile_ws_.as<uint2>();
     note_regrowth(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() -
                                                             t_grow).count());
@@ -322,17 +340,17 @@ void Pipeline::ensure_workspace(const Layout &l) {
     if (projected_.size() < need) {
       GSR_CUDA(cudaStreamSynchronize(stream_));
       drop_graph();
-      projected_.reset(need);
+      projected_.reset(need, stream_);
     }
     if (debug_cov_.size() < 8ull * splat_cap_) {
       GSR_CUDA(cudaStreamSynchronize(stream_));
       drop_graph();
-      debug_cov_.reset(8ull * splat_cap_);
+      debug_cov_.reset(8ull * splat_cap_, stream_);
     }
     if (debug_pairs_.size() < 8 * key_cap_) {
       GSR_CUDA(cudaStreamSynchronize(stream_));
       drop_graph();
-      debug_pairs_.reset(8 * key_cap_);
+      debug_pairs_.reset(8 * key_cap_, stream_);
     }
   }
 }
@@ -356,15 +374,14 @@ void Pipeline::ensure_key_workspace(uint64_t capacity) {
   uint64_t o_k1 = off; off += align256(4ull * cap);
   uint64_t o_v1 = off; off += align256(4ull * cap);
   uint64_t o_work = off; off += align256(4 * words);
-  key_ws_.reset(0);
-  key_ws_.reset(off);
+  key_ws_.reset(off, stream_);
   tile_keys0_ = key_ws_.as<uint32_t>(o_k0);
   tile_vals0_ = key_ws_.as<uint32_t>(o_v0);
   tile_keys1_ = key_ws_.as<uint32_t>(o_k1);
   tile_vals1_ = key_ws_.as<uint32_t>(o_v1);
   tile_sort_work_ = key_ws_.as<uint32_t>(o_work);
   key_cap_ = cap;
-  debug_pairs_.reset(0);
+  debug_pairs_.reset(0, stream_);
   note_regrowth(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() -
                                                           t_grow).count());
 }
@@ -778,7 +795,7 @@ RunResult Pipeline::run(const ViewSpec *views, uint32_t count, uint32_t *images,
       throw Error(Code::Unsupported, "tile pair count " + std::to_string(need) +
                                          " exceeds the renderer's limit of 2^30 - 1");
     ensure_key_workspace(std::min<uint64_t>(need + need / 4 + 1024, kMaxSortItems));
-    if (debug_) debug_pairs_.reset(8 * key_cap_);
+    if (debug_) debug_pairs_.reset(8 * key_cap_, stream_);
     ++r.reruns;
   }
   GSR_CUDA(cudaMemsetAsync(sticky_, 0, 4, stream_));

@@ -25,6 +25,12 @@ class DeviceBuffer {
   DeviceBuffer(const DeviceBuffer &) = delete;
   DeviceBuffer &operator=(const DeviceBuffer &) = delete;
   void reset(uint64_t bytes);  // frees, then allocates `bytes` (0 = free only)
+  // The same in stream order on `stream` (cudaFreeAsync / cudaMallocAsync):
+  // no host or device-wide wait, so a workspace can grow while other streams
+  // run. The buffer must then only be used on `stream` (or after it), and
+  // it is freed in stream order there when destroyed, so the stream must
+  // outlive it.
+  void reset(uint64_t bytes, cudaStream_t stream);
   void *get() const { return ptr_; }
   uint64_t size() const { return bytes_; }
   template <typename T>
@@ -33,8 +39,11 @@ class DeviceBuffer {
   }
 
  private:
+  void release();
   void *ptr_ = nullptr;
   uint64_t bytes_ = 0;
+  cudaStream_t stream_ = nullptr;  // set when allocated in stream order
+  bool ordered_ = false;
 };
 
 // Scene resident in HBM (SoA float4 planes, see device_types.h SceneDev).
